@@ -1,0 +1,570 @@
+// hype_api.cu -- the C ABI of include/hype_gpu.h: solver objects, device
+// buffers, TMA descriptors, the RHSFunctionPrim drop-in and the device-resident
+// SSP-RK time loop (captured once per solver as a CUDA graph and replayed).
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <new>
+#include <vector>
+#include "../../include/hype_gpu.h"
+#include "hype_internal.h"
+
+using namespace hype;
+
+struct hype_solver {
+    hype_config cfg;
+    int nv = 0;
+    int pitch = 0;
+    long long plane = 0;
+    double h = 0.0, r1_h = 0.0, cfl_h = 0.0;
+    double *dU = nullptr, *dS0 = nullptr, *dS1 = nullptr, *dS2 = nullptr;
+    double *dAosIn = nullptr, *dAosOut = nullptr, *dInlet = nullptr;
+    double *dRed = nullptr;           // reduction scratch
+    DevScalars *dSc = nullptr;
+    DevScalars *hSc = nullptr;        // pinned mirror
+    CUtensorMap tmU, tmS0, tmS1;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaGraphExec_t step_exec = nullptr;
+    dim3 grid;
+    int bps = 0;                      // stage blocks per SM
+    bool began = false;
+    double last_ms = 0.0;
+    char err[512] = {0};
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static int fail(hype_solver *s, int code, const char *fmt, ...)
+{
+    if (s) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(s->err, sizeof(s->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+#define CUDA_TRY(s, expr)                                                                                  \
+    do {                                                                                                   \
+        cudaError_t e_ = (expr);                                                                           \
+        if (e_ != cudaSuccess) return fail((s), HYPE_ERR_CUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+typedef CUresult (*PFN_tmapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                         const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                         CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_tmapEncodeTiled get_encode()
+{
+    static PFN_tmapEncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_tmapEncodeTiled>(p);
+    }
+    return fn;
+}
+
+// 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (STAGE_BW, 1, nvar).
+static int make_tmap(hype_solver *s, CUtensorMap *m, double *base)
+{
+    PFN_tmapEncodeTiled enc = get_encode();
+    if (!enc) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    cuuint64_t dims[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, (cuuint64_t)s->nv};
+    cuuint64_t strides[2] = {(cuuint64_t)s->pitch * 8ull, (cuuint64_t)s->plane * 8ull};
+    cuuint32_t box[3] = {(cuuint32_t)STAGE_BW, 1u, (cuuint32_t)s->nv};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return HYPE_OK;
+}
+
+// kapila_5eqn.c:485-513 evaluated once on the host (the profile does not depend
+// on t) for the three left ghost columns of every ghost-extended row.
+static void fill_inlet(const hype_solver *s, std::vector<double> &tab)
+{
+    const hype_config &c = s->cfg;
+    const int ny = c.ny, nv = s->nv;
+    tab.assign((size_t)3 * (ny + 6) * nv, 0.0);
+    for (int g = -3; g < 0; ++g)
+        for (int j = -3; j < ny + 3; ++j) {
+            const double y = c.y_min + ((double)j + 0.5) * s->h;
+            const double M = 2.0, rho_air = 1.0, rho_water = 1000.0, P = 1.013;
+            const double U_avg = M * std::sqrt(c.gamma2 * P / rho_air);
+            const double phi_R = 1.0 - 1.0e-6, phi_L = 1.0e-6;
+            const double PHI = 0.5 * (phi_R + phi_L);
+            const double dif_phi = (phi_L - phi_R) / 2.0;
+            const double hh = 30.0 / 500.0;
+            const double epsilon = 3.0 * hh;
+            const double r_0 = 1.0;
+            const double r = std::fabs(y);
+            double *V = &tab[((size_t)(g + 3) * (ny + 6) + (j + 3)) * nv];
+            V[0] = rho_water;
+            V[1] = rho_air;
+            V[2] = (r < 1.0) ? 2.0 * U_avg * (1.0 - y * y) : 0.0;
+            V[3] = 0.0;
+            V[4] = P;
+            V[5] = PHI + dif_phi * std::tanh(-(r - r_0) / epsilon);
+        }
+}
+
+static StageParams base_params(const hype_solver *s)
+{
+    StageParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.nx = s->cfg.nx; p.ny = s->cfg.ny; p.pitch = s->pitch; p.plane = s->plane;
+    p.ow_max = STAGE_OW;
+    p.bc[0] = s->cfg.bc_left; p.bc[1] = s->cfg.bc_right; p.bc[2] = s->cfg.bc_bottom; p.bc[3] = s->cfg.bc_top;
+    p.eos.g1 = s->cfg.gamma1; p.eos.g2 = s->cfg.gamma2; p.eos.pi1 = s->cfg.pi1; p.eos.pi2 = s->cfg.pi2;
+    p.eos.fix_p2 = (s->cfg.flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
+    p.r1_h = s->r1_h;
+    p.cfl_h = s->cfl_h;
+    p.sc = s->dSc;
+    p.inlet = s->dInlet;
+    p.kb = 1.0;
+    return p;
+}
+
+static const CUtensorMap &tmap_for(const hype_solver *s, const double *buf)
+{
+    return buf == s->dU ? s->tmU : buf == s->dS0 ? s->tmS0 : s->tmS1;
+}
+
+static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode, double ka, double kb, double kc,
+                         const double *xn, double *out2, int reduce, int out_aos = 0)
+{
+    StageParams p = base_params(s);
+    p.in = in; p.out = out; p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc; p.xn = xn; p.out2 = out2;
+    p.reduce_smax = reduce;
+    p.out_aos = out_aos;
+    return launch_stage(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->grid, s->stream);
+}
+
+// One SSP-RK step on the device state (hype.c:362-382 schemes, petsc TSSSP forms).
+static cudaError_t enqueue_step(hype_solver *s)
+{
+    cudaError_t e;
+    const double cfl_h = s->cfl_h;
+    if ((e = launch_begin_step(s->dSc, s->stream)) != cudaSuccess) return e;
+    switch (s->cfg.order) {
+    case 0:   // TSEULER: u += dt F(u)
+        if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, 1.0, 0, nullptr, nullptr, 1)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(s->dU, s->dS0, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream)) != cudaSuccess) return e;
+        break;
+    case 1: { // SSPRKS2, s = 2: w = u + (dt/1) F(u); u = ((1/2) w + (dt/2) F(w)) + (1/2) u
+        const int ns = 2;
+        if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, (ns - 1.), 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
+        if ((e = stage(s, s->dS0, s->dU, OUT_ZSX, (ns - 1.) / ns, (double)ns, 1. / ns, s->dU, nullptr, 1)) != cudaSuccess) return e;
+        break;
+    }
+    case 2: { // SSPRKS3, s = 4, n = 2, r = 2
+        const int n = 2, ns = 4, r = ns - n;
+        if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, (double)r, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
+        if ((e = stage(s, s->dS0, s->dS1, OUT_AXPY, 0, (double)r, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
+        // VecAXPBYPCZ(w0, n/(2n-1), (n-1) dt/(r(2n-1)), (n-1)/(2n-1), w1 = u^n, F)
+        if ((e = stage(s, s->dS1, s->dS0, OUT_ZXS, 1. * n / (2 * n - 1.), (double)(r * (2 * n - 1)), (n - 1.) / (2 * n - 1.),
+                       s->dU, nullptr, 0)) != cudaSuccess) return e;
+        if ((e = stage(s, s->dS0, s->dU, OUT_AXPY, 0, (double)r, 0, nullptr, nullptr, 1)) != cudaSuccess) return e;
+        break;
+    }
+    default: { // SSPRK(10,4)
+        const double *in = s->dU;
+        double *bufs[2] = {s->dS0, s->dS1};
+        int k = 0;
+        for (int i = 0; i < 4; ++i) {
+            if ((e = stage(s, in, bufs[k], OUT_AXPY, 0, 6.0, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
+            in = bufs[k]; k ^= 1;
+        }
+        // fifth stage + w1 = u/25 + 9 w/25 (into S2) + w = 15 w1 - 5 w
+        if ((e = stage(s, in, bufs[k], OUT_RK104_5, 0, 6.0, 0, s->dU, s->dS2, 0)) != cudaSuccess) return e;
+        in = bufs[k]; k ^= 1;
+        for (int i = 5; i < 9; ++i) {
+            if ((e = stage(s, in, bufs[k], OUT_AXPY, 0, 6.0, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
+            in = bufs[k]; k ^= 1;
+        }
+        // VecAXPBYPCZ(w1, 3/5, dt/10, 1, w0, F); sol = w1
+        if ((e = stage(s, in, s->dU, OUT_ZSX, 3. / 5, 10.0, 1.0, s->dS2, nullptr, 1)) != cudaSuccess) return e;
+        break;
+    }
+    }
+    return launch_end_step(s->dSc, cfl_h, s->stream);
+}
+
+static int check_config(const hype_config *c, hype_solver *s)
+{
+    if (!c) return fail(s, HYPE_ERR_INVALID, "null config");
+    if (hype_nvar(c->system) == 0) return fail(s, HYPE_ERR_INVALID, "unknown system %d", c->system);
+    if (c->order < 0 || c->order > 3) return fail(s, HYPE_ERR_INVALID, "order must be 0..3 (got %d)", c->order);
+    if (c->nx < 3 || c->ny < 3) return fail(s, HYPE_ERR_INVALID, "grid must be at least 3x3 (got %dx%d)", c->nx, c->ny);
+    if ((long long)c->nx * c->ny > (1LL << 31) - 1) return fail(s, HYPE_ERR_INVALID, "grid too large");
+    if (!(c->x_max > c->x_min) || !(c->y_max > c->y_min)) return fail(s, HYPE_ERR_INVALID, "empty domain");
+    if (!(c->cfl > 0.0)) return fail(s, HYPE_ERR_INVALID, "CFL must be positive");
+    const int bcs[4] = {c->bc_left, c->bc_right, c->bc_bottom, c->bc_top};
+    for (int k = 0; k < 4; ++k) {
+        if (bcs[k] < 0 || bcs[k] > 4) return fail(s, HYPE_ERR_INVALID, "unknown boundary type %d", bcs[k]);
+        if (bcs[k] == HYPE_BC_WALL)
+            return fail(s, HYPE_ERR_INVALID, "wall boundaries are not supported (the reference never fills their ghost cells)");
+        if (bcs[k] == HYPE_BC_INLET && (k != 0 || c->system != HYPE_KAPILA_5EQN))
+            return fail(s, HYPE_ERR_INVALID, "inlet boundary exists only on the left for the Kapila system (InletBCPrim)");
+    }
+    if ((c->bc_left == HYPE_BC_PERIODIC) != (c->bc_right == HYPE_BC_PERIODIC) ||
+        (c->bc_bottom == HYPE_BC_PERIODIC) != (c->bc_top == HYPE_BC_PERIODIC))
+        return fail(s, HYPE_ERR_INVALID, "periodic boundaries must be set on both sides of an axis");
+    if (c->precision != HYPE_PREC_FP64 && c->precision != HYPE_PREC_MIXED)
+        return fail(s, HYPE_ERR_INVALID, "unknown precision %d", c->precision);
+    if (c->precision == HYPE_PREC_MIXED && c->system != HYPE_KAPILA_5EQN)
+        return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for the Kapila system");
+    return HYPE_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+void hype_config_default(hype_config *c)
+{
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->system = HYPE_KAPILA_5EQN;       // hype.h:35
+    c->order = 1;                       // hype.c:32
+    c->nx = 128; c->ny = 128;           // hype.c:37-38
+    c->x_min = 0.0; c->x_max = 12.0;    // hype.c:33-36
+    c->y_min = 0.0; c->y_max = 12.0;
+    c->cfl = 0.9;                       // hype.c:39
+    c->bc_left = HYPE_BC_TRANSMISSIVE; c->bc_right = HYPE_BC_TRANSMISSIVE;   // hype.c:46-49
+    c->bc_bottom = HYPE_BC_REFLECTIVE; c->bc_top = HYPE_BC_REFLECTIVE;
+    c->gamma1 = 4.4; c->gamma2 = 1.4; c->pi1 = 6000.0; c->pi2 = 0.0;         // hype.h:42-45
+    c->precision = HYPE_PREC_FP64;
+    c->flags = 0;
+    c->device = 0;
+}
+
+int hype_nvar(int system)
+{
+    switch (system) {
+    case HYPE_EULER: return 4;
+    case HYPE_KAPILA_5EQN: return 6;
+    case HYPE_BAER_NUNZIATO: return 9;
+    default: return 0;
+    }
+}
+
+const char *hype_status_string(int st)
+{
+    switch (st) {
+    case HYPE_OK: return "ok";
+    case HYPE_ERR_INVALID: return "invalid argument or configuration";
+    case HYPE_ERR_CUDA: return "CUDA error";
+    case HYPE_ERR_INADMISSIBLE: return "inadmissible face state (the reference aborts here)";
+    case HYPE_ERR_TIMEOUT: return "device wait timed out";
+    case HYPE_ERR_NOMEM: return "out of device memory";
+    case HYPE_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    case HYPE_ERR_BUSY: return "solver busy";
+    default: return "unknown status";
+    }
+}
+
+const char *hype_last_error(const hype_solver *s) { return s ? s->err : "null solver"; }
+
+int hype_destroy(hype_solver *s)
+{
+    if (!s) return HYPE_OK;
+    int dev = s->cfg.device;
+    cudaSetDevice(dev);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
+    double *bufs[] = {s->dU, s->dS0, s->dS1, s->dS2, s->dAosIn, s->dAosOut, s->dInlet, s->dRed};
+    for (double *b : bufs) if (b) cudaFree(b);
+    if (s->dSc) cudaFree(s->dSc);
+    if (s->hSc) cudaFreeHost(s->hSc);
+    if (s->ev0) cudaEventDestroy(s->ev0);
+    if (s->ev1) cudaEventDestroy(s->ev1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return HYPE_OK;
+}
+
+int hype_create(const hype_config *cfg, hype_solver **out)
+{
+    if (!out) return HYPE_ERR_INVALID;
+    *out = nullptr;
+    hype_solver *s = new (std::nothrow) hype_solver();
+    if (!s) return HYPE_ERR_NOMEM;
+    int rc = check_config(cfg, s);
+    if (rc) { *out = s; return rc; }   // caller reads hype_last_error, then destroys
+    s->cfg = *cfg;
+    *out = s;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
+        return fail(s, HYPE_ERR_NO_DEVICE, "CUDA device %d not available", cfg->device);
+    CUDA_TRY(s, cudaSetDevice(cfg->device));
+    cudaDeviceProp prop;
+    CUDA_TRY(s, cudaGetDeviceProperties(&prop, cfg->device));
+    if (prop.major != 10) return fail(s, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", cfg->device, prop.major, prop.minor);
+    if (cfg->precision != HYPE_PREC_FP64) return fail(s, HYPE_ERR_INVALID, "mixed precision solver objects are created with hype_batch_*");
+
+    s->nv = hype_nvar(cfg->system);
+    s->pitch = (cfg->nx + 15) & ~15;                 // 128-byte rows
+    s->plane = (long long)s->pitch * cfg->ny;
+    s->h = (cfg->x_max - cfg->x_min) / (double)cfg->nx;   // hype.c:57
+    s->r1_h = 1. / s->h;                                  // rhs_function_prim.c:26
+    s->cfl_h = cfg->cfl * s->h;                           // rhs_function_prim.c:620
+    const size_t state_bytes = sizeof(double) * (size_t)s->plane * s->nv;
+    const size_t aos_bytes = sizeof(double) * (size_t)cfg->nx * cfg->ny * s->nv;
+    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CUDA_TRY(s, cudaEventCreate(&s->ev0));
+    CUDA_TRY(s, cudaEventCreate(&s->ev1));
+    double **bufs[] = {&s->dU, &s->dS0, &s->dS1};
+    for (double **b : bufs) {
+        if (cudaMalloc(b, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", state_bytes);
+        CUDA_TRY(s, cudaMemset(*b, 0, state_bytes));
+    }
+    if (cfg->order == 3) {
+        if (cudaMalloc(&s->dS2, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc failed");
+        CUDA_TRY(s, cudaMemset(s->dS2, 0, state_bytes));
+    }
+    if (cudaMalloc(&s->dAosIn, aos_bytes) != cudaSuccess || cudaMalloc(&s->dAosOut, aos_bytes) != cudaSuccess)
+        return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", aos_bytes);
+    CUDA_TRY(s, cudaMalloc(&s->dRed, sizeof(double) * TOTALS_SCRATCH));
+    CUDA_TRY(s, cudaMalloc(&s->dSc, sizeof(DevScalars)));
+    CUDA_TRY(s, cudaMemset(s->dSc, 0, sizeof(DevScalars)));
+    CUDA_TRY(s, cudaMallocHost(&s->hSc, sizeof(DevScalars)));
+    if (cfg->bc_left == HYPE_BC_INLET) {
+        std::vector<double> tab;
+        fill_inlet(s, tab);
+        CUDA_TRY(s, cudaMalloc(&s->dInlet, sizeof(double) * tab.size()));
+        CUDA_TRY(s, cudaMemcpy(s->dInlet, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
+    }
+    if ((rc = make_tmap(s, &s->tmU, s->dU)) || (rc = make_tmap(s, &s->tmS0, s->dS0)) || (rc = make_tmap(s, &s->tmS1, s->dS1))) return rc;
+
+    CUDA_TRY(s, stage_configure(cfg->system, cfg->order));
+    s->bps = stage_blocks_per_sm(cfg->system, cfg->order);
+    if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "stage kernel does not fit on an SM");
+    // One wave: strips x row-runs <= SMs x resident blocks, rows >= 8 per run.
+    const int strips = stage_strips(cfg->nx);
+    const int slots = prop.multiProcessorCount * s->bps;
+    int runs = slots / strips;
+    if (runs < 1) runs = 1;
+    if (runs > cfg->ny / 8) runs = cfg->ny / 8 > 0 ? cfg->ny / 8 : 1;
+    s->grid = dim3((unsigned)strips, (unsigned)runs, 1);
+    return HYPE_OK;
+}
+
+static int read_scalars(hype_solver *s)
+{
+    CUDA_TRY(s, cudaMemcpyAsync(s->hSc, s->dSc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (s->hSc->err & ERR_TMA_TIMEOUT) return fail(s, HYPE_ERR_TIMEOUT, "TMA row load did not complete");
+    if (s->hSc->err & ERR_BAD_LAUNCH) return fail(s, HYPE_ERR_CUDA, "stage kernel launched with a geometry it does not cover");
+    if (s->hSc->err & ERR_INADMISSIBLE_FACE) {
+        const unsigned cell = s->hSc->err_cell;
+        return fail(s, HYPE_ERR_INADMISSIBLE, "inadmissible face state near cell (i=%u, j=%u)",
+                    cell % (unsigned)s->cfg.nx, cell / (unsigned)s->cfg.nx);
+    }
+    return HYPE_OK;
+}
+
+static int reset_scalars(hype_solver *s)
+{
+    std::memset(s->hSc, 0, sizeof(DevScalars));
+    s->hSc->err_cell = 0xffffffffu;
+    CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
+    return HYPE_OK;
+}
+
+static int rhs_common(hype_solver *s, double *dRHS_aos, double *dt)
+{
+    int rc;
+    if ((rc = reset_scalars(s))) return rc;
+    CUDA_TRY(s, stage(s, s->dS0, dRHS_aos, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
+    if ((rc = read_scalars(s))) return rc;
+    if (dt) {
+        double smax;
+        const unsigned long long bits = s->hSc->smax;
+        std::memcpy(&smax, &bits, sizeof(smax));
+        *dt = (s->cfg.cfl * s->h) / (2.0 * smax);   // rhs_function_prim.c:620
+    }
+    return HYPE_OK;
+}
+
+int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double *dt)
+{
+    (void)t;
+    if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
+    if (!s->dU) return fail(s, HYPE_ERR_INVALID, "solver not created");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
+    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, launch_aos_to_planes(s->dAosIn, s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    int rc = rhs_common(s, s->dAosOut, dt);
+    if (rc && rc != HYPE_ERR_INADMISSIBLE) return rc;
+    CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return rc;
+}
+
+int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRHS, double *dt)
+{
+    (void)t;
+    if (!s || !dU || !dRHS) return fail(s, HYPE_ERR_INVALID, "null argument");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    CUDA_TRY(s, launch_aos_to_planes(dU, s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    return rhs_common(s, dRHS, dt);
+}
+
+int hype_set_state(hype_solver *s, const double *U)
+{
+    if (!s || !U) return fail(s, HYPE_ERR_INVALID, "null argument");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
+    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, launch_aos_to_planes(s->dAosIn, s->dU, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return HYPE_OK;
+}
+
+int hype_get_state(hype_solver *s, double *U)
+{
+    if (!s || !U) return fail(s, HYPE_ERR_INVALID, "null argument");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
+    CUDA_TRY(s, launch_planes_to_aos(s->dU, s->dAosOut, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(U, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return HYPE_OK;
+}
+
+int hype_begin(hype_solver *s, double t0, double t_final, int max_steps)
+{
+    if (!s) return HYPE_ERR_INVALID;
+    if (max_steps < 0) return fail(s, HYPE_ERR_INVALID, "max_steps < 0");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    int rc;
+    if ((rc = reset_scalars(s))) return rc;
+    s->hSc->t = t0; s->hSc->t_final = t_final; s->hSc->max_steps = max_steps;
+    CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
+    // hype.c:343: one RHS evaluation of the initial state seeds Ctx.dt
+    CUDA_TRY(s, stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1));
+    CUDA_TRY(s, launch_seed_dt(s->dSc, s->cfl_h, s->stream));
+    if (!s->step_exec) {
+        cudaGraph_t g;
+        CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue_step(s);
+        cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+        if (e != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+        if (e2 != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "step capture end: %s", cudaGetErrorString(e2));
+        e = cudaGraphInstantiate(&s->step_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    }
+    s->began = true;
+    return HYPE_OK;
+}
+
+int hype_advance(hype_solver *s, int nsteps)
+{
+    if (!s) return HYPE_ERR_INVALID;
+    if (!s->began) return fail(s, HYPE_ERR_INVALID, "hype_begin not called");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
+    for (int k = 0; k < nsteps; ++k) CUDA_TRY(s, cudaGraphLaunch(s->step_exec, s->stream));
+    CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
+    return HYPE_OK;
+}
+
+int hype_wait(hype_solver *s, int *steps_done, double *t_end, double *dt_next)
+{
+    if (!s) return HYPE_ERR_INVALID;
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    int rc = read_scalars(s);
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s->ev0, s->ev1) == cudaSuccess) s->last_ms = ms;
+    if (steps_done) *steps_done = s->hSc->steps;
+    if (t_end) *t_end = s->hSc->t;
+    if (dt_next) *dt_next = s->hSc->time_step;
+    return rc;
+}
+
+int hype_solve(hype_solver *s, double t0, double t_final, int max_steps, int *steps_done, double *t_end, double *dt_next)
+{
+    int rc = hype_begin(s, t0, t_final, max_steps);
+    if (rc) return rc;
+    // Each replay checks the stop condition on the device; replays after the
+    // end return at once.  Poll between chunks so a t_final stop costs little.
+    int launched = 0;
+    const int chunk = 64;
+    for (;;) {
+        const int n = (max_steps - launched) < chunk ? (max_steps - launched) : chunk;
+        if (n > 0) { if ((rc = hype_advance(s, n))) return rc; launched += n; }
+        if ((rc = hype_wait(s, steps_done, t_end, dt_next))) return rc;
+        if (s->hSc->done || launched >= max_steps) break;
+    }
+    // the loop above leaves done unset when it stopped exactly at max_steps
+    return HYPE_OK;
+}
+
+int hype_totals(hype_solver *s, int scaled, double *totals, double *amin, double *amax)
+{
+    if (!s || !totals) return fail(s, HYPE_ERR_INVALID, "null argument");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    std::vector<double> h((size_t)s->nv + 2);
+    CUDA_TRY(s, launch_totals(s->dU, s->dRed, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane,
+                              s->cfg.system == HYPE_EULER ? -1 : (s->cfg.system == HYPE_KAPILA_5EQN ? 5 : 8), s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(h.data(), s->dRed, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    const double area = scaled ? s->h * s->h : 1.0;
+    for (int c = 0; c < s->nv; ++c) totals[c] = h[c] * area;
+    if (amin) *amin = h[s->nv];
+    if (amax) *amax = h[s->nv + 1];
+    return HYPE_OK;
+}
+
+int hype_launch_info(const hype_solver *s, int *gx, int *gy, int *threads, size_t *smem, int *bps)
+{
+    if (!s) return HYPE_ERR_INVALID;
+    if (gx) *gx = (int)s->grid.x;
+    if (gy) *gy = (int)s->grid.y;
+    if (threads) *threads = STAGE_NT;
+    if (smem) *smem = stage_smem_bytes(s->cfg.system, s->cfg.order);
+    if (bps) *bps = s->bps;
+    return HYPE_OK;
+}
+
+int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
+{
+    if (!s || reps < 1 || !ms_per_launch) return fail(s, HYPE_ERR_INVALID, "bad argument");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    int rc;
+    if ((rc = reset_scalars(s))) return rc;
+    s->hSc->dt = 1e-30;   // a representative AXPY stage S0 -> S1 with a negligible step
+    CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->dS0, s->dU, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream));
+    CUDA_TRY(s, stage(s, s->dS0, s->dS1, OUT_AXPY, 0, 2.0, 0, nullptr, nullptr, 1));   // warm
+    CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
+    for (int k = 0; k < reps; ++k) CUDA_TRY(s, stage(s, s->dS0, s->dS1, OUT_AXPY, 0, 2.0, 0, nullptr, nullptr, 1));
+    CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
+    if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
+    float ms = 0.f;
+    CUDA_TRY(s, cudaEventElapsedTime(&ms, s->ev0, s->ev1));
+    *ms_per_launch = (double)ms / reps;
+    return HYPE_OK;
+}
+
+int hype_last_elapsed_ms(const hype_solver *s, double *ms)
+{
+    if (!s || !ms) return HYPE_ERR_INVALID;
+    *ms = s->last_ms;
+    return HYPE_OK;
+}
+
+}  // extern "C"

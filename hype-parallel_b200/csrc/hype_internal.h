@@ -1,0 +1,82 @@
+// hype_internal.h -- host/device interface between the C ABI (hype_api.cu) and
+// the kernels (hype_stage.cu, hype_aux.cu).  Not installed; not part of the ABI.
+#pragma once
+#include <cstdint>
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include "hype_physics.cuh"
+
+namespace hype {
+
+// What a stage kernel writes for each owned cell, with F = L(S) the right-hand
+// side of the stage input S and X a second state (u^n):
+//   OUT_RHS      out = F
+//   OUT_AXPY     out = S + ((dt/kb) * F)                          PETSc VecAXPY(S, dt/kb, F)
+//   OUT_ZXS      out = ((ka*X) + ((dt/kb)*F)) + (kc*S)             VecAXPBYPCZ(S, ka, dt/kb, kc, X, F)
+//   OUT_ZSX      out = ((ka*S) + ((dt/kb)*F)) + (kc*X)             VecAXPBYPCZ(X, ka, dt/kb, kc, S, F)
+//   OUT_RK104_5  w  = S + ((dt/6)*F); out2 = (1/25)X + (9/25)w;     fifth stage of SSPRK(10,4) and the
+//                out = 15*out2 + (-5)*w                             two vector updates that follow it
+enum : int { OUT_RHS = 0, OUT_AXPY = 1, OUT_ZXS = 2, OUT_ZSX = 3, OUT_RK104_5 = 4 };
+
+// Device-resident scalars of one solve (one per instance).
+struct DevScalars {
+    double dt;                 // time step of the step in progress
+    double t;                  // time at the start of the step in progress
+    double t_final;
+    double time_step;          // dt proposed by the last RHS (MonitorFunction / Ctx->dt)
+    unsigned long long smax;   // bit pattern of max wave speed of the RHS being reduced
+    unsigned int err;          // ERR_* bits
+    unsigned int err_cell;     // linear index of the first cell that raised an error
+    int steps, max_steps;
+    int done;                  // set when the run reached t_final or max_steps
+    int pad_;
+};
+
+struct StageParams {
+    int nx, ny, pitch;          // row stride of a field plane, in elements (even)
+    long long plane;            // elements per field plane
+    int ow_max;                 // grid.x is chosen so that no strip exceeds this many columns
+    int bc[4];                  // left, right, bottom, top (BC_*)
+    Eos eos;
+    double r1_h;                // 1/h
+    double cfl_h;               // CFL*h
+    const double *in;           // stage input planes (also behind the tensor map)
+    const double *xn;           // second state X (u^n) for OUT_ZXS/OUT_ZSX/OUT_RK104_5
+    double *out;                // output planes (or AoS when out_aos)
+    double *out2;               // OUT_RK104_5 second output
+    int out_aos;                // 1: write `out` interleaved (cell-major, NV per cell)
+    int mode;
+    double ka, kb, kc;
+    DevScalars *sc;             // dt source, smax/err target, early-exit flag
+    int reduce_smax;            // 1: fold this stage's max wave speed into sc->smax
+    const double *inlet;        // [3][ny+6][NV] primitive ghost values for a left inlet (or null)
+};
+
+// Tile geometry of the stage kernel.
+constexpr int STAGE_NT = 128;               // threads per block = reconstruction columns
+constexpr int STAGE_OW = STAGE_NT - 2;      // owned columns per strip
+constexpr int STAGE_BW = STAGE_NT + 6;      // TMA box width (columns x0-4 .. x0+NT+1)
+constexpr int STAGE_SLOTS = 6;              // prim row ring
+
+size_t stage_smem_bytes(int sys, int order);
+cudaError_t stage_configure(int sys, int order);   // raises the dynamic smem limit once
+cudaError_t launch_stage(int sys, int order, const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s);
+int stage_blocks_per_sm(int sys, int order);
+// grid.x: with S = ceil(nx/124) strips and even origins 2*floor(s*nx/(2S)),
+// every strip has at most 2*ceil(nx/(2S)) <= 124 columns and the last one at
+// most nx/S + 2 <= 126 = STAGE_OW.
+inline int stage_strips(int nx) { return (nx + (STAGE_OW - 2) - 1) / (STAGE_OW - 2); }
+
+// hype_aux.cu
+cudaError_t launch_aos_to_planes(const double *aos, double *planes, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s);
+cudaError_t launch_planes_to_aos(const double *planes, double *aos, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s);
+cudaError_t launch_begin_step(DevScalars *sc, cudaStream_t s);
+cudaError_t launch_end_step(DevScalars *sc, double cfl_h, cudaStream_t s);
+cudaError_t launch_seed_dt(DevScalars *sc, double cfl_h, cudaStream_t s);
+// writes nv sums then min/max of field acomp (acomp < 0: zeros) to red[0..nv+1];
+// red must hold 64 + (512 + 1) * (nv + 2) doubles
+cudaError_t launch_totals(const double *planes, double *red, int nx, int ny, int nv, int pitch, long long plane, int acomp,
+                          cudaStream_t s);
+constexpr size_t TOTALS_SCRATCH = 64 + 513 * 11;
+
+}  // namespace hype

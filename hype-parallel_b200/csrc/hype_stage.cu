@@ -1,0 +1,600 @@
+// hype_stage.cu -- the fused FP64 stage kernel: one launch evaluates HyPE-2D's
+// primitive-variable right-hand side L(S) (RHSFunctionPrim, rhs_function_prim.c:12-626)
+// on the stage input S and writes one SSP-RK stage combination of it, folding
+// the CFL wave-speed maximum (rhs_function_prim.c:617-623) into a device scalar.
+//
+// Tiling.  A block of STAGE_NT threads owns a strip of STAGE_OW columns and a
+// run of `rows` rows.  It marches up its rows; at row r every thread t
+// reconstructs the cell in column x0-1+t (the strip plus one ring column each
+// side), so only two of STAGE_NT reconstructions per row are repeated by the
+// neighbouring strip.  Rows of the conserved state arrive by one TMA 3-D box
+// load per row (all fields, columns x0-4 .. x0+NT+1) into a ring of
+// STAGE_SLOTS shared-memory rows, are patched at domain edges with the
+// boundary-condition copies, and are converted to primitive variables in place.
+// Reconstruction coefficients go to shared memory, the x-face Riemann problem
+// at the left of each column is solved by that column's thread from its own
+// and its left neighbour's coefficients, the y-face problem below each cell by
+// the cell's thread from its coefficients and the top-face values it kept
+// from the row below.  Row r-1 is completed (y-flux difference, volume
+// non-conservative term, RK combination) while row r is processed.
+//
+// Built with --fmad=false: arithmetic rounds exactly as the reference's C does.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdio>
+#include "hype_internal.h"
+
+namespace hype {
+
+// ---------------------------------------------------------------------------
+// TMA / mbarrier helpers (inline PTX, sm_90+ forms, valid on sm_100a)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                 ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+// Ghost source index along one axis (rhs_function_prim.c:75-315 and the DMDA
+// periodic wrap): transmissive copies the edge cell, reflective mirrors.
+__device__ __forceinline__ int map_axis(int g, int n, int bc_lo, int bc_hi)
+{
+    if (g < 0) {
+        if (bc_lo == BC_PERIODIC || bc_hi == BC_PERIODIC) return g + n;
+        if (bc_lo == BC_REFLECTIVE) return -1 - g;
+        return 0;   // transmissive (inlet columns are replaced after conversion)
+    }
+    if (g >= n) {
+        if (bc_lo == BC_PERIODIC || bc_hi == BC_PERIODIC) return g - n;
+        if (bc_hi == BC_REFLECTIVE) return 2 * (n - 1) - g + 1;
+        return n - 1;
+    }
+    return g;
+}
+
+__device__ __forceinline__ void raise_error(DevScalars *sc, unsigned bits, unsigned cell)
+{
+    atomicOr(&sc->err, bits);
+    atomicMin(&sc->err_cell, cell);
+}
+
+template <int SYS, int N>
+struct StageKernel {
+    using S = System<SYS>;
+    using QD = Quad<N>;
+    static constexpr int NV = S::NV;
+    static constexpr int NT = STAGE_NT;
+    static constexpr int BW = STAGE_BW;
+    static constexpr int SLOTS = STAGE_SLOTS;
+    static constexpr int NDOF = QD::NDOF;
+    static constexpr int NC = NDOF - 1;                    // stored coefficients (k >= 1)
+    static constexpr int ROW_ELEMS = BW * NV;
+    static constexpr int ROW_BYTES = ROW_ELEMS * 8;
+    static constexpr int SLOT_STRIDE = ((ROW_BYTES + 127) / 128) * 128 / 8;   // doubles
+    // per-thread arrays, [k][c][t] so consecutive threads hit consecutive banks
+    static constexpr int COEF_ELEMS = (NC > 2 ? NC : 2) * NV * NT;             // also the flux exchange (2 NV)
+    static constexpr int YT_ELEMS = QD::NFGP * NV * NT;
+    static constexpr size_t smem_bytes()
+    {
+        return 128 /* barriers */ + (size_t)SLOTS * SLOT_STRIDE * 8 + (size_t)COEF_ELEMS * 8 + (size_t)YT_ELEMS * 8 + 64;
+    }
+};
+
+template <int SYS, int N>
+__global__ void __launch_bounds__(STAGE_NT, 1)
+stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
+{
+    using K = StageKernel<SYS, N>;
+    using S = typename K::S;
+    using QD = typename K::QD;
+    constexpr int NV = K::NV, NT = K::NT, BW = K::BW, SLOTS = K::SLOTS, NDOF = K::NDOF;
+    constexpr int NFGP = QD::NFGP;
+
+    if (p.sc->done) return;
+
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
+    double *rows_s = reinterpret_cast<double *>(smem_raw + 128);
+    double *coef_s = rows_s + (size_t)SLOTS * K::SLOT_STRIDE;
+    double *yt_s = coef_s + K::COEF_ELEMS;
+    __shared__ double red_s[NT / 32];
+
+    const int t = threadIdx.x;
+    // strips split the columns evenly on even boundaries (TMA x origin alignment);
+    // row runs split the rows evenly
+    const int x0 = 2 * (int)(((long long)blockIdx.x * p.nx) / (2LL * gridDim.x));
+    const int x1 = (blockIdx.x + 1 == gridDim.x) ? p.nx : 2 * (int)(((long long)(blockIdx.x + 1) * p.nx) / (2LL * gridDim.x));
+    const int owc = x1 - x0;
+    const int y0 = (int)(((long long)blockIdx.y * p.ny) / gridDim.y);
+    const int H = (int)(((long long)(blockIdx.y + 1) * p.ny) / gridDim.y) - y0;
+    if (owc > NT - 2 || owc < 1 || H < 1) {   // launch geometry outside what the tiling covers
+        if (threadIdx.x == 0) raise_error(p.sc, ERR_BAD_LAUNCH, 0u);
+        return;
+    }
+    const int xs = x0 - 4;                    // TMA box origin (even: x0 is even)
+    const int i = x0 - 1 + t;                 // this thread's reconstruction column
+    const bool active = t <= owc + 1;
+    const bool owned = t >= 1 && t <= owc;
+    const bool xface = t >= 1 && t <= owc + 1;
+    const bool touches_x = (x0 == 0) || (x0 + owc >= p.nx);
+    const int bcL = p.bc[0], bcR = p.bc[1], bcB = p.bc[2], bcT = p.bc[3];
+    const bool py = (bcB == BC_PERIODIC || bcT == BC_PERIODIC);
+    const double dt = (p.mode == OUT_RHS) ? 0.0 : p.sc->dt;
+    const Eos eos = p.eos;
+    const double r1_h = p.r1_h;
+
+    if (t == 0) {
+        for (int s = 0; s < SLOTS; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+
+    const int row_lo = y0 - 3, row_hi = y0 + H + 2;   // rows of state this block reads
+    int next_issue = row_lo, next_conv = row_lo;
+    auto slot_of = [&](int row) { return (row - row_lo) % SLOTS; };
+    auto row_ptr = [&](int row) { return rows_s + (size_t)slot_of(row) * K::SLOT_STRIDE; };   // [c][BW]
+
+    double smax_loc = 0.0;
+    bool bad = false;
+    unsigned bad_cell = 0xffffffffu;
+    // carries for the row being completed (row r-1)
+    double ncp_c[NV], t1_c[NV], gb_c[NV], eb_c[NV];
+#pragma unroll
+    for (int c = 0; c < NV; ++c) { ncp_c[c] = 0.0; t1_c[c] = 0.0; gb_c[c] = 0.0; eb_c[c] = 0.0; }
+
+    for (int r = y0 - 1; r <= y0 + H; ++r) {
+        // ---------------- A. bring rows up to r+2 into the ring --------------
+        if (t == 0) {
+            fence_proxy_async();   // earlier generic accesses to the slots precede the TMA writes
+            for (; next_issue <= min(r + 3, row_hi); ++next_issue) {
+                const int row = next_issue;
+                const int src = map_axis(row, p.ny, bcB, bcT);
+                uint64_t *bar = &bars[slot_of(row)];
+                mbar_expect_tx(bar, K::ROW_BYTES);
+                tma_load_3d(row_ptr(row), &tmap, xs, src, 0, bar);
+            }
+        }
+        for (; next_conv <= r + 2; ++next_conv) {
+            const int row = next_conv;
+            const unsigned parity = (unsigned)(((row - row_lo) / SLOTS) & 1);
+            bool ok = false;
+            for (long it = 0; it < (1L << 24); ++it) {
+                if (mbar_try_wait(&bars[slot_of(row)], parity)) { ok = true; break; }
+            }
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                return;   // block-uniform exit; no copy of this block is left unwaited except the failed one
+            }
+            double *rp = row_ptr(row);
+            const int src = map_axis(row, p.ny, bcB, bcT);
+            const bool yg = row < 0 || row >= p.ny;
+            const bool yrefl = yg && ((row < 0 ? bcB : bcT) == BC_REFLECTIVE);
+            // columns cc in [1, owc+6] are the ones the stencils read
+            const int ncols = owc + 6;
+            // Phase 1: ghost columns fetch their conserved source values
+            double qg[2][NV];
+            bool isg[2] = {false, false};
+            int ccs[2] = {1 + t, 1 + NT + t};
+            if (touches_x) {
+#pragma unroll
+                for (int k = 0; k < 2; ++k) {
+                    const int cc = ccs[k];
+                    if (cc > ncols) continue;
+                    const int g = xs + cc;
+                    if (g >= 0 && g < p.nx) continue;
+                    isg[k] = true;
+                    const int gm = map_axis(g, p.nx, bcL, bcR);
+                    if (gm - xs >= 0 && gm - xs < BW) {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) qg[k][c] = rp[c * BW + (gm - xs)];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) qg[k][c] = p.in[(size_t)c * p.plane + (size_t)src * p.pitch + gm];
+                    }
+                }
+                __syncthreads();
+            }
+            // Phase 2: convert in place, apply reflections / inlet values
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int cc = ccs[k];
+                if (cc > ncols) continue;
+                const int g = xs + cc;
+                double Q[NV], V[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) Q[c] = isg[k] ? qg[k][c] : rp[c * BW + cc];
+                S::cons2prim(eos, Q, V);
+                if (isg[k]) {
+                    const int side_bc = g < 0 ? bcL : bcR;
+                    if (side_bc == BC_INLET && p.inlet) {
+                        const int jr = py ? row : map_axis(row, p.ny, bcB, bcT);
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) V[c] = p.inlet[((size_t)(g + 3) * (p.ny + 6) + (jr + 3)) * NV + c];
+                    } else if (side_bc == BC_REFLECTIVE) {
+                        if (S::RX0 >= 0) V[S::RX0] = -V[S::RX0];
+                        if (S::RX1 >= 0) V[S::RX1] = -V[S::RX1];
+                    }
+                }
+                if (yrefl) {
+                    if (S::RY0 >= 0) V[S::RY0] = -V[S::RY0];
+                    if (S::RY1 >= 0) V[S::RY1] = -V[S::RY1];
+                }
+#pragma unroll
+                for (int c = 0; c < NV; ++c) rp[c * BW + cc] = V[c];
+            }
+        }
+        __syncthreads();   // S1: prim rows r-2 .. r+2 ready
+
+        // ---------------- B. reconstruction of cell (r, i) --------------------
+        const int cc = t + 3;                                     // column of i in the ring rows
+        const double *w_m2 = row_ptr(r - 2), *w_m1 = row_ptr(r - 1), *w_0 = row_ptr(r), *w_p1 = row_ptr(r + 1), *w_p2 = row_ptr(r + 2);
+        if (active) {
+#pragma unroll 1
+            for (int c = 0; c < NV; ++c) {
+                Stencil st;
+                const double *a0 = w_0 + c * BW + cc;
+                st.c = a0[0];
+                st.xm2 = a0[-2]; st.xm1 = a0[-1]; st.xp1 = a0[1]; st.xp2 = a0[2];
+                st.ym2 = w_m2[c * BW + cc]; st.ym1 = w_m1[c * BW + cc]; st.yp1 = w_p1[c * BW + cc]; st.yp2 = w_p2[c * BW + cc];
+                st.pp = w_p1[c * BW + cc + 1]; st.pm = w_m1[c * BW + cc + 1]; st.mp = w_p1[c * BW + cc - 1]; st.mm = w_m1[c * BW + cc - 1];
+                double cf[NDOF];
+                Recon<N>::run(st, cf);
+#pragma unroll
+                for (int k = 1; k < NDOF; ++k) coef_s[((k - 1) * NV + c) * NT + t] = cf[k];
+            }
+            // admissibility at the nodes (rhs_function_prim.c:382-421)
+            bool ok = true;
+            static_for<QD::NNODE>([&](auto q) {
+                if (!ok) return;
+                double V[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    double cf[NDOF];
+                    cf[0] = w_0[c * BW + cc];
+#pragma unroll
+                    for (int k = 1; k < NDOF; ++k) cf[k] = coef_s[((k - 1) * NV + c) * NT + t];
+                    V[c] = poly_eval<NDOF>(cf, PhiNode<N, decltype(q)::value>{});
+                }
+                ok = S::pad(eos, V);
+            });
+            if (!ok && N >= 2) {
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    const double w0 = w_0[c * BW + cc];
+                    coef_s[(0 * NV + c) * NT + t] = minmod(w_0[c * BW + cc + 1] - w0, w0 - w_0[c * BW + cc - 1]);
+                    coef_s[(1 * NV + c) * NT + t] = minmod(w_p1[c * BW + cc] - w0, w0 - w_m1[c * BW + cc]);
+#pragma unroll
+                    for (int k = 3; k < NDOF; ++k) coef_s[((k - 1) * NV + c) * NT + t] = 0.0;
+                }
+            }
+        }
+        // own coefficients of one variable, k = 0 from the ring row
+        auto load_cf = [&](int c, int tt, double *cf) {
+            cf[0] = w_0[c * BW + tt + 3];
+#pragma unroll
+            for (int k = 1; k < NDOF; ++k) cf[k] = coef_s[((k - 1) * NV + c) * NT + tt];
+        };
+
+        // ---------------- C. y-face below (r, i); complete row r-1 ------------
+        const bool in_rows = r >= y0 && r <= y0 + H;
+        if (owned && in_rows) {
+            double G[NV], E[NV];
+#pragma unroll
+            for (int c = 0; c < NV; ++c) { G[c] = 0.0; E[c] = 0.0; }
+            static_for<NFGP>([&](auto q) {
+                double VL[NV], VR[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    double cf[NDOF];
+                    load_cf(c, t, cf);
+                    VR[c] = poly_eval<NDOF>(cf, PhiFace<N, 2, decltype(q)::value>{});
+                    VL[c] = yt_s[(decltype(q)::value * NV + c) * NT + t];
+                }
+                // riemann.c:112-140
+                double QL[NV], QR[NV], FL[NV], FR[NV];
+                S::prim2cons(eos, VL, QL);
+                S::prim2cons(eos, VR, QR);
+                const double sl = S::template flux<1>(eos, VL, FL, bad);
+                const double sr = S::template flux<1>(eos, VR, FR, bad);
+                const double s = (sl < sr) ? sr : sl;
+                double Vav[NV], gx[NV], gy[NV], D[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    Vav[c] = 0.5 * (VR[c] + VL[c]);
+                    gx[c] = 0.0 * (VR[c] - VL[c]);
+                    gy[c] = 1.0 * (VR[c] - VL[c]);
+                }
+                S::ncp(eos, Vav, gx, gy, D);
+                smax_loc = fmax(smax_loc, s);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    const double Fc = 0.5 * (FR[c] + FL[c] - s * (QR[c] - QL[c]));
+                    G[c] += QD::wf(decltype(q)::value) * Fc;
+                    E[c] += QD::wf(decltype(q)::value) * D[c];
+                }
+            });
+            if (bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);
+            if (r > y0) {
+                // row r-1: rhs = ncp + ((-1/h) X - (1/h) Y) (rhs_function_prim.c:589-602), then the RK combination
+                const int jo = r - 1;
+                const size_t gidx = (size_t)jo * p.pitch + i;
+                double out_v[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    const double Y = G[c] - gb_c[c] + 0.5 * (E[c] + eb_c[c]);
+                    const double ty = r1_h * Y;
+                    const double rhs = ncp_c[c] + (t1_c[c] - ty);
+                    out_v[c] = rhs;
+                }
+                if (p.mode == OUT_RHS) {
+                    if (p.out_aos) {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) p.out[((size_t)jo * p.nx + i) * NV + c] = out_v[c];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NV; ++c) p.out[(size_t)c * p.plane + gidx] = out_v[c];
+                    }
+                } else {
+                    const double b = dt / p.kb;
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) {
+                        const double Sv = p.in[(size_t)c * p.plane + gidx];
+                        const double bF = b * out_v[c];
+                        double o;
+                        if (p.mode == OUT_AXPY) {
+                            o = Sv + bF;
+                        } else if (p.mode == OUT_ZXS) {
+                            const double Xv = p.xn[(size_t)c * p.plane + gidx];
+                            const double s0 = p.ka * Xv + bF;
+                            o = s0 + p.kc * Sv;
+                        } else if (p.mode == OUT_ZSX) {
+                            const double Xv = p.xn[(size_t)c * p.plane + gidx];
+                            const double s0 = p.ka * Sv + bF;
+                            o = s0 + p.kc * Xv;
+                        } else {   // OUT_RK104_5
+                            const double Xv = p.xn[(size_t)c * p.plane + gidx];
+                            const double w = Sv + bF;
+                            const double w1 = (1. / 25) * Xv + (9. / 25) * w;
+                            p.out2[(size_t)c * p.plane + gidx] = w1;
+                            o = 15.0 * w1 + (-5.0) * w;
+                        }
+                        p.out[(size_t)c * p.plane + gidx] = o;
+                    }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NV; ++c) { gb_c[c] = G[c]; eb_c[c] = E[c]; }
+        }
+
+        // ---------------- D. keep the top-face values for row r+1 -------------
+        if (owned && r >= y0 - 1 && r < y0 + H) {
+#pragma unroll
+            for (int c = 0; c < NV; ++c) {
+                double cf[NDOF];
+                load_cf(c, t, cf);
+                static_for<NFGP>([&](auto q) {
+                    yt_s[(decltype(q)::value * NV + c) * NT + t] = poly_eval<NDOF>(cf, PhiFace<N, 3, decltype(q)::value>{});
+                });
+            }
+        }
+
+        // ---------------- E. volume non-conservative term (rhs_function_prim.c:459-479)
+        const bool full_row = r >= y0 && r < y0 + H;
+        if (owned && full_row) {
+#pragma unroll
+            for (int c = 0; c < NV; ++c) ncp_c[c] = 0.0;
+            static_for<QD::NVGP>([&](auto q) {
+                constexpr int Q = decltype(q)::value;
+                double V[NV], gx[NV], gy[NV], B[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    double cf[NDOF];
+                    load_cf(c, t, cf);
+                    V[c] = poly_eval<NDOF>(cf, PhiVol<N, Q>{});
+                    gx[c] = r1_h * poly_eval<NDOF>(cf, DPhiVolX<N, Q>{});
+                    gy[c] = r1_h * poly_eval<NDOF>(cf, DPhiVolY<N, Q>{});
+                }
+                S::ncp(eos, V, gx, gy, B);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) ncp_c[c] += -QD::wv(Q) * B[c];
+            });
+        }
+        __syncthreads();   // S2: every column's coefficients of row r visible
+
+        // ---------------- F. x-face at the left of column i -------------------
+        double Fx[NV], Dx[NV];
+#pragma unroll
+        for (int c = 0; c < NV; ++c) { Fx[c] = 0.0; Dx[c] = 0.0; }
+        if (xface && full_row) {
+            static_for<NFGP>([&](auto q) {
+                double VL[NV], VR[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    double cl[NDOF], cr[NDOF];
+                    load_cf(c, t - 1, cl);
+                    load_cf(c, t, cr);
+                    VL[c] = poly_eval<NDOF>(cl, PhiFace<N, 1, decltype(q)::value>{});
+                    VR[c] = poly_eval<NDOF>(cr, PhiFace<N, 0, decltype(q)::value>{});
+                }
+                double QL[NV], QR[NV], FL[NV], FR[NV];
+                S::prim2cons(eos, VL, QL);
+                S::prim2cons(eos, VR, QR);
+                const double sl = S::template flux<0>(eos, VL, FL, bad);
+                const double sr = S::template flux<0>(eos, VR, FR, bad);
+                const double s = (sl < sr) ? sr : sl;
+                double Vav[NV], gx[NV], gy[NV], D[NV];
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    Vav[c] = 0.5 * (VR[c] + VL[c]);
+                    gx[c] = 1.0 * (VR[c] - VL[c]);
+                    gy[c] = 0.0 * (VR[c] - VL[c]);
+                }
+                S::ncp(eos, Vav, gx, gy, D);
+                smax_loc = fmax(smax_loc, s);
+#pragma unroll
+                for (int c = 0; c < NV; ++c) {
+                    const double Fc = 0.5 * (FR[c] + FL[c] - s * (QR[c] - QL[c]));
+                    Fx[c] += QD::wf(decltype(q)::value) * Fc;
+                    Dx[c] += QD::wf(decltype(q)::value) * D[c];
+                }
+            });
+            if (bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);
+        }
+        __syncthreads();   // S3: coefficient reads done; the buffer now carries face fluxes
+        if (xface && full_row) {
+#pragma unroll
+            for (int c = 0; c < NV; ++c) { coef_s[c * NT + t] = Fx[c]; coef_s[(NV + c) * NT + t] = Dx[c]; }
+        }
+        __syncthreads();   // S4
+        if (owned && full_row) {
+#pragma unroll
+            for (int c = 0; c < NV; ++c) {
+                const double F1 = coef_s[c * NT + t + 1], D1 = coef_s[(NV + c) * NT + t + 1];
+                const double X = F1 - Fx[c] + 0.5 * (D1 + Dx[c]);
+                t1_c[c] = -r1_h * X;
+            }
+        }
+    }
+
+    // ---------------- CFL maximum: warp shuffle, block, one atomic ------------
+    if (bad) raise_error(p.sc, ERR_INADMISSIBLE_FACE, bad_cell);
+    if (p.reduce_smax) {
+        double m = smax_loc;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if ((t & 31) == 0) red_s[t >> 5] = m;
+        __syncthreads();
+        if (t == 0) {
+            double b = red_s[0];
+#pragma unroll
+            for (int w = 1; w < NT / 32; ++w) b = fmax(b, red_s[w]);
+            if (b > 0.0) atomicMax(&p.sc->smax, (unsigned long long)__double_as_longlong(b));
+        }
+    }
+}
+
+template <int SYS, int N>
+static cudaError_t configure_one()
+{
+    return cudaFuncSetAttribute(stage_kernel<SYS, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)StageKernel<SYS, N>::smem_bytes());
+}
+
+template <int SYS>
+static size_t smem_sys(int order)
+{
+    switch (order) {
+    case 0: return StageKernel<SYS, 0>::smem_bytes();
+    case 1: return StageKernel<SYS, 1>::smem_bytes();
+    case 2: return StageKernel<SYS, 2>::smem_bytes();
+    default: return StageKernel<SYS, 3>::smem_bytes();
+    }
+}
+
+size_t stage_smem_bytes(int sys, int order)
+{
+    switch (sys) {
+    case SYS_EULER: return smem_sys<SYS_EULER>(order);
+    case SYS_KAPILA: return smem_sys<SYS_KAPILA>(order);
+    default: return smem_sys<SYS_BN>(order);
+    }
+}
+
+template <int SYS>
+static cudaError_t configure_sys(int order)
+{
+    switch (order) {
+    case 0: return configure_one<SYS, 0>();
+    case 1: return configure_one<SYS, 1>();
+    case 2: return configure_one<SYS, 2>();
+    default: return configure_one<SYS, 3>();
+    }
+}
+
+cudaError_t stage_configure(int sys, int order)
+{
+    switch (sys) {
+    case SYS_EULER: return configure_sys<SYS_EULER>(order);
+    case SYS_KAPILA: return configure_sys<SYS_KAPILA>(order);
+    default: return configure_sys<SYS_BN>(order);
+    }
+}
+
+template <int SYS, int N>
+static int bps_one()
+{
+    int nb = 0;
+    if (configure_one<SYS, N>() != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage_kernel<SYS, N>, STAGE_NT, StageKernel<SYS, N>::smem_bytes()) != cudaSuccess)
+        return 0;
+    return nb;
+}
+template <int SYS>
+static int bps_sys(int order)
+{
+    switch (order) {
+    case 0: return bps_one<SYS, 0>();
+    case 1: return bps_one<SYS, 1>();
+    case 2: return bps_one<SYS, 2>();
+    default: return bps_one<SYS, 3>();
+    }
+}
+int stage_blocks_per_sm(int sys, int order)
+{
+    switch (sys) {
+    case SYS_EULER: return bps_sys<SYS_EULER>(order);
+    case SYS_KAPILA: return bps_sys<SYS_KAPILA>(order);
+    default: return bps_sys<SYS_BN>(order);
+    }
+}
+
+template <int SYS, int N>
+static cudaError_t launch_one(const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s)
+{
+    stage_kernel<SYS, N><<<grid, STAGE_NT, StageKernel<SYS, N>::smem_bytes(), s>>>(tmap, p);
+    return cudaGetLastError();
+}
+
+template <int SYS>
+static cudaError_t launch_sys(int order, const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s)
+{
+    switch (order) {
+    case 0: return launch_one<SYS, 0>(tmap, p, grid, s);
+    case 1: return launch_one<SYS, 1>(tmap, p, grid, s);
+    case 2: return launch_one<SYS, 2>(tmap, p, grid, s);
+    default: return launch_one<SYS, 3>(tmap, p, grid, s);
+    }
+}
+
+cudaError_t launch_stage(int sys, int order, const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s)
+{
+    switch (sys) {
+    case SYS_EULER: return launch_sys<SYS_EULER>(order, tmap, p, grid, s);
+    case SYS_KAPILA: return launch_sys<SYS_KAPILA>(order, tmap, p, grid, s);
+    default: return launch_sys<SYS_BN>(order, tmap, p, grid, s);
+    }
+}
+
+}  // namespace hype

@@ -1,0 +1,169 @@
+/*
+ * hype_gpu.h -- C ABI of hype-parallel_b200, a B200 (sm_100a) implementation of
+ * HyPE-2D's right-hand-side evaluation and explicit SSP-RK time step for the
+ * Euler, Kapila five-equation and Baer-Nunziato systems.
+ *
+ * Plain C: pointers, sizes and status codes only; no PETSc and no CUDA types.
+ * Every entry point returns HYPE_OK (0) or a HYPE_ERR_* code; hype_last_error()
+ * gives the message of the last failure on a solver.
+ *
+ * State arrays crossing this boundary have the layout of the reference's
+ * global Vec (HyPE-2D/hype.h:68-70, Field{comp[nVar]} indexed u[j][i]):
+ * nx*ny cells, row-major (i fastest), nvar doubles interleaved per cell.
+ * Component orders are the reference's:
+ *   Euler   [rho, rho u, rho v, E]                                  euler.c:14-38
+ *   Kapila  [a1 rho1, a2 rho2, rho u, rho v, E, a1]                  kapila_5eqn.c:14-61
+ *   BN      [a1 r1, a1 r1 u1, a1 r1 v1, a1 E1, a2 r2, a2 r2 u2,
+ *            a2 r2 v2, a2 E2, a1]                                    baer_nunziato.c:14-60
+ */
+#ifndef HYPE_GPU_H
+#define HYPE_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define HYPE_API __attribute__((visibility("default")))
+#else
+#define HYPE_API
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define HYPE_OK                0
+#define HYPE_ERR_INVALID       1   /* bad argument or unsupported configuration            */
+#define HYPE_ERR_CUDA          2   /* CUDA runtime or driver error                          */
+#define HYPE_ERR_INADMISSIBLE  3   /* a face state failed the flux admissibility test; the
+                                      reference calls MPI_Abort there (kapila_5eqn.c:353-357,
+                                      baer_nunziato.c:281-303, euler.c:212-222)              */
+#define HYPE_ERR_TIMEOUT       4   /* a bounded device wait expired                          */
+#define HYPE_ERR_NOMEM         5   /* device memory (or the admission budget) exhausted      */
+#define HYPE_ERR_NO_DEVICE     6   /* no CUDA device / not an sm_100 device                  */
+#define HYPE_ERR_BUSY          7   /* operation needs the solver idle                        */
+
+/* ---- PDE systems: the compile-time #define of HyPE-2D/hype.h:33-35 --------- */
+#define HYPE_EULER          0
+#define HYPE_KAPILA_5EQN    1
+#define HYPE_BAER_NUNZIATO  2
+
+/* ---- boundary types: values of HyPE-2D/hype.h:76 enum bndry_type ------------ */
+#define HYPE_BC_WALL          0   /* rejected: the reference never fills its ghosts      */
+#define HYPE_BC_INLET         1   /* left boundary, Kapila only (InletBCPrim)            */
+#define HYPE_BC_PERIODIC      2
+#define HYPE_BC_REFLECTIVE    3
+#define HYPE_BC_TRANSMISSIVE  4
+
+/* ---- arithmetic ---------------------------------------------------------- */
+#define HYPE_PREC_FP64   0    /* bit-compatible with the reference's C          */
+#define HYPE_PREC_MIXED  1    /* FP32 state/reconstruction/flux, FP64 EOS and totals */
+
+/* ---- flags --------------------------------------------------------------- */
+#define HYPE_FLAG_BN_FIX_P2   1u  /* Baer-Nunziato: take the phase-2 flux pressure from V[7]
+                                     instead of V[8] (baer_nunziato.c:271 reads alpha_1)   */
+
+/*
+ * Run-time form of the reference's compile-time and AppCtx parameters:
+ *   system                 hype.h:33-35 (#define KAPILA_5EQN ...)
+ *   order                  AppCtx.N (hype.c:32): 0..3; selects WENO degree,
+ *                          quadrature and SSP scheme (hype.c:59-68, 362-382)
+ *   nx, ny, x/y min/max    AppCtx.N_x, N_y, x_min ... (hype.c:33-38); h = (x_max-x_min)/nx
+ *   cfl                    AppCtx.CFL
+ *   bc_*                   AppCtx.LeftBoundary ... (hype.c:46-49)
+ *   gamma1..pi2            GAMMA_1, GAMMA_2, PI_1, PI_2 (hype.h:42-45)
+ */
+typedef struct {
+    int system;
+    int order;
+    int nx, ny;
+    double x_min, x_max, y_min, y_max;
+    double cfl;
+    int bc_left, bc_right, bc_bottom, bc_top;
+    double gamma1, gamma2, pi1, pi2;
+    int precision;
+    unsigned flags;
+    int device;           /* CUDA device ordinal */
+} hype_config;
+
+typedef struct hype_solver hype_solver;
+
+/* Fills *cfg with the defaults of HyPE-2D/hype.c:32-50 and hype.h:42-45. */
+HYPE_API void hype_config_default(hype_config *cfg);
+
+/* Number of conserved variables of a system (nVar, hype.h:37): 4, 6 or 9; 0 if unknown. */
+HYPE_API int hype_nvar(int system);
+
+/* Human-readable name of a status code. */
+HYPE_API const char *hype_status_string(int status);
+
+/*
+ * Creates a solver: validates cfg, allocates the device state (three stage
+ * buffers of nx*ny*nvar doubles plus staging), builds the TMA descriptors.
+ * Replaces the set-up half of HyPE-2D/hype.c:56-309 (DMDA, work Vecs, scratch
+ * arrays u_bnd/F/G/D/E, quadrature and basis tables).
+ */
+HYPE_API int hype_create(const hype_config *cfg, hype_solver **out);
+HYPE_API int hype_destroy(hype_solver *s);
+HYPE_API const char *hype_last_error(const hype_solver *s);
+
+/*
+ * Drop-in for RHSFunctionPrim (HyPE-2D/rhs_function_prim.c:12-626, declared at
+ * hype.h:306): RHS = L(U) over all cells and *dt = CFL*h/(2*s_max), the value
+ * the reference leaves in Ctx->dt (rhs_function_prim.c:620-623).  U and RHS are
+ * host arrays in the Vec layout above.  t is accepted for the TS signature (the
+ * inlet profile is time independent).  Thread-compatible, not reentrant on one
+ * solver (as the reference, which shares AppCtx scratch).
+ */
+HYPE_API int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double *dt);
+
+/* Same with U and RHS in device memory of the solver's device (e.g. a PETSc
+ * VECCUDA array); the call is synchronous. */
+HYPE_API int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRHS, double *dt);
+
+/* Device-resident state: copy in / out (Vec layout, host memory).  Setting the
+ * state keeps the time-loop scalars (t, dt, step count) of hype_begin; call
+ * hype_begin again to restart the loop from a new initial state. */
+HYPE_API int hype_set_state(hype_solver *s, const double *U);
+HYPE_API int hype_get_state(hype_solver *s, double *U);
+
+/*
+ * The time loop of HyPE-2D/hype.c:337-384 on the device-resident state: one
+ * RHS call at t0 seeds dt (hype.c:343, 356), then SSP-RK steps (N=0 forward
+ * Euler, N=1 SSPRKS2 two stages, N=2 SSPRKS3 four stages, N=3 SSPRK(10,4);
+ * hype.c:362-382) until t_final (last step clipped, TS_EXACTFINALTIME_MATCHSTEP)
+ * or max_steps; each step's dt is the CFL dt of the previous step's last RHS
+ * call (MonitorFunction, post_process.c:19).  Outputs may be NULL.
+ */
+HYPE_API int hype_solve(hype_solver *s, double t0, double t_final, int max_steps,
+               int *steps_done, double *t_end, double *dt_next);
+
+/* Split form of hype_solve for callers that overlap host work:
+ * hype_begin seeds dt; hype_advance enqueues up to nsteps steps (CUDA graph
+ * replays, asynchronous); hype_wait blocks and reports progress and errors. */
+HYPE_API int hype_begin(hype_solver *s, double t0, double t_final, int max_steps);
+HYPE_API int hype_advance(hype_solver *s, int nsteps);
+HYPE_API int hype_wait(hype_solver *s, int *steps_done, double *t_end, double *dt_next);
+
+/* Sums of each conserved variable over the cells (times h^2 when scaled != 0),
+ * computed on the device in FP64 with a fixed reduction order; totals has nvar
+ * entries.  Also reports min/max of the volume fraction (Kapila, BN). */
+HYPE_API int hype_totals(hype_solver *s, int scaled, double *totals, double *alpha_min, double *alpha_max);
+
+/* Launch geometry of the stage kernel chosen for this grid (for reports). */
+HYPE_API int hype_launch_info(const hype_solver *s, int *grid_x, int *grid_y, int *threads, size_t *smem_bytes,
+                     int *blocks_per_sm);
+
+/* Average device time of one stage-kernel launch (an SSP-RK stage u + dt/2 L(u)
+ * over the device state, dt negligible so the state is unchanged to rounding),
+ * over `reps` launches timed with CUDA events on the solver's stream. */
+HYPE_API int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch);
+
+/* Device time of the last hype_solve/hype_wait interval, in milliseconds
+ * (CUDA events around the step replays). */
+HYPE_API int hype_last_elapsed_ms(const hype_solver *s, double *ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HYPE_GPU_H */

@@ -1,0 +1,187 @@
+"""GPU parity of the FP64 sm_100a path against the reference's bits.
+
+The FP64 kernels are built with --fmad=false and keep the reference's operand
+order, so the bar here is bit-exactness: the SHA-256 of every RHS and final
+state must equal the one the reference's own sources produced (golden file),
+and dt / step count / final time must be identical doubles.  Where a test
+cannot use the golden file (fresh seeds, full-size grids) it compares with the
+CPU oracle, which the CPU suite pins to the same bits.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.json")))
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+def describe_diff(a, b, nv):
+    d = np.abs(a - b).reshape(-1, nv)
+    k = int(np.argmax(d.max(axis=1)))
+    return f"max |diff| {d.max():.3e} at cell {k} comp {int(np.argmax(d[k]))}; ref scale {np.abs(b).max():.3e}"
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN["rhs"]))
+def test_rhs_prim_bitwise(name, hp, orc):
+    g = GOLDEN["rhs"][name]
+    _, cfg, kind, seed = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        R, dt, st = s.rhs_function_prim(0.0, U)
+    if sha(R) != g["sha_RHS"]:
+        Ro, _, _ = orc.rhs(cfg, U)
+        pytest.fail(f"RHS differs from the reference: {describe_diff(R, Ro, cfg.nvar)}")
+    assert st == hp.OK
+    assert float(dt).hex() == g["dt"]
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN["solve"]))
+def test_solve_bitwise(name, hp, orc):
+    g = GOLDEN["solve"][name]
+    (_, cfg, kind, seed), t0, tf, nmax = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        s.set_state(U)
+        steps, te, dtn, st = s.solve(t0, tf, nmax)
+        Ue = s.get_state()
+    if g["status"] != 0:
+        assert st == hp.ERR_INADMISSIBLE
+        return
+    assert st == hp.OK
+    assert steps == g["steps"]
+    assert float(te).hex() == g["t_end"]
+    assert float(dtn).hex() == g["dt_next"]
+    if sha(Ue) != g["sha_U_end"]:
+        Uo, *_ = orc.solve(cfg, U, t0, tf, nmax)
+        pytest.fail(f"final state differs: {describe_diff(Ue, Uo, cfg.nvar)}")
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_rhs_fresh_seeds_vs_oracle(seed, hp, orc):
+    rng = np.random.default_rng(1000 + seed)
+    for system, kind in ((O.KAPILA, "rough"), (O.KAPILA, "bubble"), (O.BN, "discs"), (O.EULER, "quadrants")):
+        nx, ny = int(rng.integers(3, 300)), int(rng.integers(3, 40))
+        order = int(rng.integers(0, 4))
+        bcs = [int(b) for b in rng.choice([O.TRANSMISSIVE, O.REFLECTIVE], 4)]
+        if rng.uniform() < 0.3:
+            bcs[2] = bcs[3] = O.PERIODIC
+        eos = cases.EULER_EOS if system == O.EULER else cases.KAPILA_EOS
+        cfg = O.Config(system=system, order=order, nx=nx, ny=ny, bc_left=bcs[0], bc_right=bcs[1], bc_bottom=bcs[2],
+                       bc_top=bcs[3], **eos)
+        U = cases.state(cfg, kind, seed)
+        Ro, dto, sto = orc.rhs(cfg, U)
+        with hp.Solver(cases.to_pkg(cfg)) as s:
+            R, dt, st = s.rhs_function_prim(0.0, U)
+        assert (st == hp.OK) == (sto == O.OK), (nx, ny, order, bcs)
+        if sto == O.OK:
+            assert dt == dto
+            assert R.tobytes() == Ro.tobytes(), describe_diff(R, Ro, cfg.nvar)
+
+
+def test_rhs_device_pointers(hp, orc):
+    import torch
+    _, cfg, kind, seed = cases.case_by_name("kapila_37x23_rough_mixed_bc")
+    U = cases.state(cfg, kind, seed)
+    Ro, dto, _ = orc.rhs(cfg, U)
+    dU = torch.from_numpy(U).cuda()
+    dR = torch.empty_like(dU)
+    torch.cuda.synchronize()
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        dt, st = s.rhs_function_prim_device(0.0, dU.data_ptr(), dR.data_ptr())
+    assert st == hp.OK and dt == dto
+    assert dR.cpu().numpy().tobytes() == Ro.tobytes()
+
+
+def test_inadmissible_state_reported_not_aborted(hp):
+    """The reference MPI_Aborts on a negative squared sound speed; the GPU path
+    returns HYPE_ERR_INADMISSIBLE and the solver stays usable."""
+    _, cfg, kind, seed = cases.case_by_name("kapila_16x16_bubble")
+    U = cases.state(cfg, kind, seed).reshape(-1, 6).copy()
+    U[100, 4] = -1e12          # energy far below the stiffened-gas floor: p + pi < 0
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        R, dt, st = s.rhs_function_prim(0.0, U.reshape(-1))
+        assert st == hp.ERR_INADMISSIBLE
+        U2 = cases.state(cfg, kind, seed)
+        R2, dt2, st2 = s.rhs_function_prim(0.0, U2)
+        assert st2 == hp.OK
+        assert sha(R2) == GOLDEN["rhs"]["kapila_16x16_bubble"]["sha_RHS"]
+
+
+def test_repeated_calls_identical(hp):
+    _, cfg, kind, seed = cases.case_by_name("bn_16x16")
+    U = cases.state(cfg, kind, seed)
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        outs = [s.rhs_function_prim(0.0, U)[0].tobytes() for _ in range(3)]
+    assert outs[0] == outs[1] == outs[2]
+
+
+def test_conservation_and_alpha_bounds_periodic(hp):
+    """Periodic Kapila run: the conservative totals (partial masses, momentum,
+    energy) change only by rounding (relative 1e-12) and alpha_1 stays in [0, 1]."""
+    cfg = O.Config(system=O.KAPILA, order=2, nx=192, ny=160, bc_left=O.PERIODIC, bc_right=O.PERIODIC,
+                   bc_bottom=O.PERIODIC, bc_top=O.PERIODIC, **cases.KAPILA_EOS)
+    U = cases.state(cfg, "bubble", 21)
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        s.set_state(U)
+        tot0, amin0, amax0 = s.totals()
+        steps, te, dtn, st = s.solve(0.0, 1.0, 40)
+        assert st == hp.OK and steps == 40
+        tot1, amin1, amax1 = s.totals()
+    scale = np.abs(U.reshape(-1, 6)).sum(axis=0)
+    for c in (0, 1, 4):                     # partial masses, energy
+        assert abs(tot1[c] - tot0[c]) <= 1e-12 * scale[c], (c, tot0[c], tot1[c])
+    for c in (2, 3):                        # momentum (starts near zero): relative to the momentum-flux scale
+        assert abs(tot1[c] - tot0[c]) <= 1e-12 * max(scale[c], 1.0) * 10, (c, tot0[c], tot1[c])
+    assert amin1 >= 0.0 and amax1 <= 1.0
+
+
+def _window_check(hp, orc, cfg, U, R_full, dt_full, wins, rng):
+    """Interior windows of a large RHS against the oracle on window + 3-cell halo."""
+    nv = cfg.nvar
+    Ug = U.reshape(cfg.ny, cfg.nx, nv)
+    Rg = R_full.reshape(cfg.ny, cfg.nx, nv)
+    w = 48
+    for _ in range(wins):
+        j0 = int(rng.integers(3, cfg.ny - w - 3))
+        i0 = int(rng.integers(3, cfg.nx - w - 3))
+        sub = np.ascontiguousarray(Ug[j0 - 3:j0 + w + 3, i0 - 3:i0 + w + 3]).reshape(-1)
+        c2 = O.Config(**{**cases.config_to_dict(cfg), "nx": w + 6, "ny": w + 6})
+        c2.x_max = c2.x_min + (cfg.x_max - cfg.x_min) / cfg.nx * (w + 6)   # same h
+        assert (c2.x_max - c2.x_min) / c2.nx == (cfg.x_max - cfg.x_min) / cfg.nx
+        Rs, _, st = orc.rhs(c2, sub)
+        Rs = Rs.reshape(w + 6, w + 6, nv)[3:-3, 3:-3]
+        got = Rg[j0:j0 + w, i0:i0 + w]
+        assert Rs.tobytes() == np.ascontiguousarray(got).tobytes(), describe_diff(got, Rs, nv)
+
+
+@pytest.mark.parametrize("system,n,kind", [(O.KAPILA, 2048, "bubble"), (O.BN, 1024, "discs")])
+def test_full_size_rhs_windows_and_shift_invariance(system, n, kind, hp, orc):
+    """Full-size grids of the benchmark workloads: random interior windows are
+    bit-identical to the oracle, and on a periodic grid shifting the state by
+    (dx, dy) cells shifts the RHS bit for bit and leaves dt unchanged."""
+    cfg = O.Config(system=system, order=2, nx=n, ny=n, **cases.KAPILA_EOS)
+    U = cases.state(cfg, kind, 5)
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        R, dt, st = s.rhs_function_prim(0.0, U)
+    assert st == hp.OK
+    _window_check(hp, orc, cfg, U, R, dt, 3, np.random.default_rng(9))
+    cp = O.Config(**{**cases.config_to_dict(cfg), "bc_left": O.PERIODIC, "bc_right": O.PERIODIC,
+                     "bc_bottom": O.PERIODIC, "bc_top": O.PERIODIC})
+    Ug = U.reshape(n, n, cfg.nvar)
+    Us = np.ascontiguousarray(np.roll(Ug, (37, 101), axis=(0, 1))).reshape(-1)
+    with hp.Solver(cases.to_pkg(cp)) as s:
+        R0, dt0, st0 = s.rhs_function_prim(0.0, U)
+        R1, dt1, st1 = s.rhs_function_prim(0.0, Us)
+    assert st0 == st1 == hp.OK and dt0 == dt1
+    assert np.roll(R0.reshape(n, n, cfg.nvar), (37, 101), axis=(0, 1)).tobytes() == R1.reshape(n, n, cfg.nvar).tobytes()
