@@ -121,6 +121,29 @@ HYPE_API int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RH
  * VECCUDA array); the call is synchronous. */
 HYPE_API int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRHS, double *dt);
 
+/*
+ * RHSFunctionPrim for callers that cannot allocate device memory -- for
+ * example a plug-in running inside an application or framework whose memory
+ * pool already owns the GPU, or a time loop that must not pay the device-wide
+ * synchronisation of cudaMalloc/cudaFree.  No counterpart in the reference
+ * (HyPE-2D allocates its scratch in main, hype.c:237-251); it has the meaning
+ * of hype_rhs_prim_device but needs no solver object and calls no allocator.
+ *
+ * dU and dRHS are device arrays in the Vec layout (caller-owned).  All working
+ * memory is one static device array of HYPE_NOALLOC_MAX_BYTES, held by every
+ * GPU that loads this library until the process exits: the grid must satisfy
+ * 256 + ceil16(nx) * ny * nvar * 8 <= HYPE_NOALLOC_MAX_BYTES (Kapila up to
+ * about 590 x 590 cells), else HYPE_ERR_NOMEM is returned before any device
+ * work.  FP64 only; periodic, reflective and transmissive boundaries only
+ * (HYPE_ERR_INVALID otherwise).  Runs on the legacy default stream and returns
+ * when the result is in dRHS.  The first call on a device sets up (looks up
+ * the array's device address) and should come before any stream capture.
+ * Calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.
+ */
+#define HYPE_NOALLOC_MAX_BYTES (16u * 1024u * 1024u)
+HYPE_API int hype_rhs_prim_noalloc(const hype_config *cfg, double t, const double *dU, double *dRHS, double *dt);
+
 /* Device-resident state: copy in / out (Vec layout, host memory).  Setting the
  * state keeps the time-loop scalars (t, dt, step count) of hype_begin; call
  * hype_begin again to restart the loop from a new initial state. */
