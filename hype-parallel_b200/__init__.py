@@ -218,8 +218,10 @@ class Solver:
             raise ValueError("U has the wrong size")
         self._check(lib().hype_set_state(self._h, _ptr(U)))
 
-    def get_state(self) -> np.ndarray:
-        U = np.empty(self.n, dtype=np.float64)
+    def get_state(self, out: np.ndarray | None = None) -> np.ndarray:
+        U = np.empty(self.n, dtype=np.float64) if out is None else out
+        if U.size != self.n or U.dtype != np.float64 or not U.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of the state size")
         self._check(lib().hype_get_state(self._h, _ptr(U)))
         return U
 

@@ -545,6 +545,10 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
     if (!s || reps < 1 || !ms_per_launch) return fail(s, HYPE_ERR_INVALID, "bad argument");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     int rc;
+    // keep the time loop's scalars (t, dt, step count) for the caller
+    DevScalars saved;
+    CUDA_TRY(s, cudaMemcpyAsync(&saved, s->dSc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if ((rc = reset_scalars(s))) return rc;
     s->hSc->dt = 1e-30;   // a representative AXPY stage S0 -> S1 with a negligible step
     CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
@@ -557,6 +561,9 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
     float ms = 0.f;
     CUDA_TRY(s, cudaEventElapsedTime(&ms, s->ev0, s->ev1));
     *ms_per_launch = (double)ms / reps;
+    *s->hSc = saved;
+    CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return HYPE_OK;
 }
 

@@ -53,9 +53,10 @@ struct StageParams {
 };
 
 // Tile geometry of the stage kernel.
-constexpr int STAGE_NT = 128;               // threads per block = reconstruction columns
-constexpr int STAGE_OW = STAGE_NT - 2;      // owned columns per strip
-constexpr int STAGE_BW = STAGE_NT + 6;      // TMA box width (columns x0-4 .. x0+NT+1)
+constexpr int STAGE_CELLS = 128;            // reconstruction columns per block
+constexpr int STAGE_NT = 2 * STAGE_CELLS;   // threads per block: two per column
+constexpr int STAGE_OW = STAGE_CELLS - 2;   // owned columns per strip
+constexpr int STAGE_BW = STAGE_CELLS + 6;   // TMA box width (columns x0-4 .. x0+CELLS+1)
 constexpr int STAGE_SLOTS = 6;              // prim row ring
 
 size_t stage_smem_bytes(int sys, int order);
