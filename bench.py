@@ -191,6 +191,7 @@ def run_gpu(args, rank, world, local_rank):
     U0 = hp.initial_state(cfg, "shock_bubble", seed=SEED + rank, nbubbles=NBUB)
     solver = hp.Solver(cfg)
     solver.set_state(U0)
+    tile = solver.autotune(3) if not args.no_autotune else None
     solver.begin(0.0, 1e30, 1 << 30)
 
     def barrier():
@@ -265,7 +266,7 @@ def run_gpu(args, rank, world, local_rank):
                          "traffic": None, "peak_source": peak_src,
                          "note": "stage kernel alone: 96 B/cell algorithmic (one FP64 state read + one write) per launch; "
                                  "the kernel is FP64-pipe bound, see profiles/"},
-            "stage_kernel": {"ms_per_launch": ms_stage, "launch": info},
+            "stage_kernel": {"ms_per_launch": ms_stage, "launch": info, "autotuned_tile": tile},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps * 6,
@@ -283,6 +284,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default stage tile shape")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -114,6 +114,7 @@ def lib() -> ctypes.CDLL:
         L.hype_launch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3 + [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
         L.hype_last_elapsed_ms.argtypes = [vp, _DP]
         L.hype_time_stage.argtypes = [vp, ctypes.c_int, _DP]
+        L.hype_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.hype_config_default.argtypes = [ctypes.POINTER(_Cfg)]
         for name in ("hype_ic_shock_bubble",):
             getattr(L, name).argtypes = [ctypes.POINTER(_Cfg), ctypes.c_uint64, ctypes.c_int, _DP]
@@ -267,6 +268,12 @@ class Solver:
         ms = ctypes.c_double(0.0)
         self._check(lib().hype_time_stage(self._h, reps, ctypes.byref(ms)))
         return ms.value
+
+    def autotune(self, reps: int = 3):
+        """Pick the fastest stage-kernel tile shape; returns (tile width, waves)."""
+        c, w = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().hype_autotune(self._h, reps, ctypes.byref(c), ctypes.byref(w)))
+        return c.value, w.value
 
     def last_elapsed_ms(self) -> float:
         ms = ctypes.c_double(0.0)

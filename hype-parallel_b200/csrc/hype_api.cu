@@ -30,7 +30,10 @@ struct hype_solver {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t step_exec = nullptr;
-    dim3 grid;
+    int cells = STAGE_CELLS;          // tile width of the stage kernel
+    int waves = 1;                    // row runs per strip = waves x (SM slots / strips)
+    int sms = 0;
+    int strips = 1, runs = 1;         // tile decomposition of the grid
     int bps = 0;                      // stage blocks per SM
     bool began = false;
     double last_ms = 0.0;
@@ -73,14 +76,14 @@ static PFN_tmapEncodeTiled get_encode()
     return fn;
 }
 
-// 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (STAGE_BW, 1, nvar).
+// 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (cells + 6, 1, nvar).
 static int make_tmap(hype_solver *s, CUtensorMap *m, double *base)
 {
     PFN_tmapEncodeTiled enc = get_encode();
     if (!enc) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
     cuuint64_t dims[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, (cuuint64_t)s->nv};
     cuuint64_t strides[2] = {(cuuint64_t)s->pitch * 8ull, (cuuint64_t)s->plane * 8ull};
-    cuuint32_t box[3] = {(cuuint32_t)STAGE_BW, 1u, (cuuint32_t)s->nv};
+    cuuint32_t box[3] = {(cuuint32_t)stage_box_width(s->cells), 1u, (cuuint32_t)s->nv};
     cuuint32_t estr[3] = {1u, 1u, 1u};
     CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                      CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -122,7 +125,7 @@ static StageParams base_params(const hype_solver *s)
     StageParams p;
     std::memset(&p, 0, sizeof(p));
     p.nx = s->cfg.nx; p.ny = s->cfg.ny; p.pitch = s->pitch; p.plane = s->plane;
-    p.ow_max = STAGE_OW;
+    p.strips = s->strips; p.runs = s->runs;
     p.bc[0] = s->cfg.bc_left; p.bc[1] = s->cfg.bc_right; p.bc[2] = s->cfg.bc_bottom; p.bc[3] = s->cfg.bc_top;
     p.eos.g1 = s->cfg.gamma1; p.eos.g2 = s->cfg.gamma2; p.eos.pi1 = s->cfg.pi1; p.eos.pi2 = s->cfg.pi2;
     p.eos.fix_p2 = (s->cfg.flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
@@ -133,6 +136,31 @@ static StageParams base_params(const hype_solver *s)
     p.kb = 1.0;
     return p;
 }
+
+// Tile width and decomposition: `waves` waves of strips x row runs (<= SMs x
+// resident blocks each), at least 8 rows per run.  Rebuilds the TMA
+// descriptors, whose box width follows the tile width, and drops the captured
+// step graph (recaptured on the next hype_begin / hype_advance).
+static int set_tiling(hype_solver *s, int cells, int waves = 1)
+{
+    const hype_config *cfg = &s->cfg;
+    int rc;
+    s->cells = cells;
+    CUDA_TRY(s, stage_configure(cfg->system, cfg->order, cells));
+    s->bps = stage_blocks_per_sm(cfg->system, cfg->order, cells);
+    if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "stage kernel does not fit on an SM");
+    s->strips = stage_strips(cfg->nx, cells);
+    const int slots = s->sms * s->bps * (waves > 0 ? waves : 1);
+    s->waves = waves > 0 ? waves : 1;
+    int runs = slots / s->strips;
+    if (runs < 1) runs = 1;
+    if (runs > cfg->ny / 8) runs = cfg->ny / 8 > 0 ? cfg->ny / 8 : 1;
+    s->runs = runs;
+    if ((rc = make_tmap(s, &s->tmU, s->dU)) || (rc = make_tmap(s, &s->tmS0, s->dS0)) || (rc = make_tmap(s, &s->tmS1, s->dS1))) return rc;
+    if (s->step_exec) { cudaGraphExecDestroy(s->step_exec); s->step_exec = nullptr; }
+    return HYPE_OK;
+}
+
 
 static const CUtensorMap &tmap_for(const hype_solver *s, const double *buf)
 {
@@ -146,7 +174,7 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
     p.in = in; p.out = out; p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc; p.xn = xn; p.out2 = out2;
     p.reduce_smax = reduce;
     p.out_aos = out_aos;
-    return launch_stage(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->grid, s->stream);
+    return launch_stage(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
 }
 
 // One SSP-RK step on the device state (hype.c:362-382 schemes, petsc TSSSP forms).
@@ -345,19 +373,9 @@ int hype_create(const hype_config *cfg, hype_solver **out)
         CUDA_TRY(s, cudaMalloc(&s->dInlet, sizeof(double) * tab.size()));
         CUDA_TRY(s, cudaMemcpy(s->dInlet, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
     }
-    if ((rc = make_tmap(s, &s->tmU, s->dU)) || (rc = make_tmap(s, &s->tmS0, s->dS0)) || (rc = make_tmap(s, &s->tmS1, s->dS1))) return rc;
 
-    CUDA_TRY(s, stage_configure(cfg->system, cfg->order));
-    s->bps = stage_blocks_per_sm(cfg->system, cfg->order);
-    if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "stage kernel does not fit on an SM");
-    // One wave: strips x row-runs <= SMs x resident blocks, rows >= 8 per run.
-    const int strips = stage_strips(cfg->nx);
-    const int slots = prop.multiProcessorCount * s->bps;
-    int runs = slots / strips;
-    if (runs < 1) runs = 1;
-    if (runs > cfg->ny / 8) runs = cfg->ny / 8 > 0 ? cfg->ny / 8 : 1;
-    s->grid = dim3((unsigned)strips, (unsigned)runs, 1);
-    return HYPE_OK;
+    s->sms = prop.multiProcessorCount;
+    return set_tiling(s, STAGE_CELLS);
 }
 
 static int read_scalars(hype_solver *s)
@@ -444,6 +462,23 @@ int hype_get_state(hype_solver *s, double *U)
     return HYPE_OK;
 }
 
+// One SSP-RK step (begin_step, the stages, end_step) captured once as a CUDA
+// graph and replayed by hype_advance.
+static int ensure_step_graph(hype_solver *s)
+{
+    if (s->step_exec) return HYPE_OK;
+    cudaGraph_t g;
+    CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_step(s);
+    cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
+    if (e != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
+    if (e2 != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "step capture end: %s", cudaGetErrorString(e2));
+    e = cudaGraphInstantiate(&s->step_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    return HYPE_OK;
+}
+
 int hype_begin(hype_solver *s, double t0, double t_final, int max_steps)
 {
     if (!s) return HYPE_ERR_INVALID;
@@ -456,17 +491,7 @@ int hype_begin(hype_solver *s, double t0, double t_final, int max_steps)
     // hype.c:343: one RHS evaluation of the initial state seeds Ctx.dt
     CUDA_TRY(s, stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1));
     CUDA_TRY(s, launch_seed_dt(s->dSc, s->cfl_h, s->stream));
-    if (!s->step_exec) {
-        cudaGraph_t g;
-        CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-        cudaError_t e = enqueue_step(s);
-        cudaError_t e2 = cudaStreamEndCapture(s->stream, &g);
-        if (e != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "step capture: %s", cudaGetErrorString(e));
-        if (e2 != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "step capture end: %s", cudaGetErrorString(e2));
-        e = cudaGraphInstantiate(&s->step_exec, g, 0);
-        cudaGraphDestroy(g);
-        if (e != cudaSuccess) return fail(s, HYPE_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
-    }
+    if ((rc = ensure_step_graph(s))) return rc;
     s->began = true;
     return HYPE_OK;
 }
@@ -476,6 +501,8 @@ int hype_advance(hype_solver *s, int nsteps)
     if (!s) return HYPE_ERR_INVALID;
     if (!s->began) return fail(s, HYPE_ERR_INVALID, "hype_begin not called");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    int rc;
+    if ((rc = ensure_step_graph(s))) return rc;
     CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
     for (int k = 0; k < nsteps; ++k) CUDA_TRY(s, cudaGraphLaunch(s->step_exec, s->stream));
     CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
@@ -532,10 +559,10 @@ int hype_totals(hype_solver *s, int scaled, double *totals, double *amin, double
 int hype_launch_info(const hype_solver *s, int *gx, int *gy, int *threads, size_t *smem, int *bps)
 {
     if (!s) return HYPE_ERR_INVALID;
-    if (gx) *gx = (int)s->grid.x;
-    if (gy) *gy = (int)s->grid.y;
-    if (threads) *threads = STAGE_NT;
-    if (smem) *smem = stage_smem_bytes(s->cfg.system, s->cfg.order);
+    if (gx) *gx = s->strips;
+    if (gy) *gy = s->runs;
+    if (threads) *threads = stage_threads(s->cells);
+    if (smem) *smem = stage_smem_bytes(s->cfg.system, s->cfg.order, s->cells);
     if (bps) *bps = s->bps;
     return HYPE_OK;
 }
@@ -564,6 +591,28 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
     *s->hSc = saved;
     CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return HYPE_OK;
+}
+
+int hype_autotune(hype_solver *s, int reps, int *cells_out, int *waves_out)
+{
+    if (!s) return HYPE_ERR_INVALID;
+    if (reps < 1) reps = 3;
+    static const int cand_cells[2] = {64, 128};
+    static const int cand_waves[3] = {1, 2, 4};
+    int best_c = s->cells, best_w = s->waves, rc;
+    double best = 1e300;
+    for (int c : cand_cells)
+        for (int w : cand_waves) {
+            if ((rc = set_tiling(s, c, w))) return rc;
+            if (stage_strips(s->cfg.nx, c) * s->runs < 1) continue;
+            double ms = 0.0;
+            if ((rc = hype_time_stage(s, reps, &ms))) return rc;
+            if (ms < best) { best = ms; best_c = c; best_w = w; }
+        }
+    if ((rc = set_tiling(s, best_c, best_w))) return rc;
+    if (cells_out) *cells_out = best_c;
+    if (waves_out) *waves_out = best_w;
     return HYPE_OK;
 }
 

@@ -35,7 +35,6 @@ struct DevScalars {
 struct StageParams {
     int nx, ny, pitch;          // row stride of a field plane, in elements (even)
     long long plane;            // elements per field plane
-    int ow_max;                 // grid.x is chosen so that no strip exceeds this many columns
     int bc[4];                  // left, right, bottom, top (BC_*)
     Eos eos;
     double r1_h;                // 1/h
@@ -50,23 +49,27 @@ struct StageParams {
     DevScalars *sc;             // dt source, smax/err target, early-exit flag
     int reduce_smax;            // 1: fold this stage's max wave speed into sc->smax
     const double *inlet;        // [3][ny+6][NV] primitive ghost values for a left inlet (or null)
+    int strips, runs;           // tile decomposition: column strips x row runs
 };
 
-// Tile geometry of the stage kernel.
-constexpr int STAGE_CELLS = 128;            // reconstruction columns per block
-constexpr int STAGE_NT = 2 * STAGE_CELLS;   // threads per block: two per column
-constexpr int STAGE_OW = STAGE_CELLS - 2;   // owned columns per strip
-constexpr int STAGE_BW = STAGE_CELLS + 6;   // TMA box width (columns x0-4 .. x0+CELLS+1)
+// Tile geometry of the stage kernel: a tile is CELLS reconstruction columns
+// (CELLS - 2 owned) of one strip, processed by 2*CELLS threads; CELLS is 64 or
+// 128 (chosen per grid by the autotuner, 128 by default).
+constexpr int STAGE_CELLS = 128;
 constexpr int STAGE_SLOTS = 6;              // prim row ring
+inline int stage_box_width(int cells) { return cells + 6; }   // TMA box: columns x0-4 .. x0+cells+1
 
-size_t stage_smem_bytes(int sys, int order);
-cudaError_t stage_configure(int sys, int order);   // raises the dynamic smem limit once
-cudaError_t launch_stage(int sys, int order, const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s);
-int stage_blocks_per_sm(int sys, int order);
-// grid.x: with S = ceil(nx/124) strips and even origins 2*floor(s*nx/(2S)),
-// every strip has at most 2*ceil(nx/(2S)) <= 124 columns and the last one at
-// most nx/S + 2 <= 126 = STAGE_OW.
-inline int stage_strips(int nx) { return (nx + (STAGE_OW - 2) - 1) / (STAGE_OW - 2); }
+size_t stage_smem_bytes(int sys, int order, int cells);
+int stage_threads(int cells);
+cudaError_t stage_configure(int sys, int order, int cells);   // raises the dynamic smem limit
+int stage_blocks_per_sm(int sys, int order, int cells);
+cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
+cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
+                               const int2 *work, int nwork, int blocks, cudaStream_t s);
+// Strips of a grid: with S = ceil(nx/(cells-4)) strips and even origins
+// 2*floor(s*nx/(2S)), every strip has at most 2*ceil(nx/(2S)) <= cells-4
+// columns and the last one at most nx/S + 2 <= cells-2.
+inline int stage_strips(int nx, int cells) { return (nx + (cells - 4) - 1) / (cells - 4); }
 
 // hype_aux.cu
 cudaError_t launch_aos_to_planes(const double *aos, double *planes, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s);

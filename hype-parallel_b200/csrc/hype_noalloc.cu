@@ -114,26 +114,26 @@ extern "C" HYPE_API int hype_rhs_prim_noalloc(const hype_config *cfg, double t, 
     CUtensorMap tm;
     cuuint64_t dims[3] = {(cuuint64_t)cfg->nx, (cuuint64_t)cfg->ny, (cuuint64_t)nv};
     cuuint64_t strides[2] = {(cuuint64_t)pitch * 8ull, (cuuint64_t)plane * 8ull};
-    cuuint32_t box[3] = {(cuuint32_t)STAGE_BW, 1u, (cuuint32_t)nv};
+    cuuint32_t box[3] = {(cuuint32_t)stage_box_width(STAGE_CELLS), 1u, (cuuint32_t)nv};
     cuuint32_t estr[3] = {1u, 1u, 1u};
     if (reinterpret_cast<PFN_encodeTiled>(fn)(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box, estr,
                                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return HYPE_ERR_CUDA;
 
-    if (stage_configure(cfg->system, cfg->order) != cudaSuccess) return HYPE_ERR_CUDA;
+    if (stage_configure(cfg->system, cfg->order, STAGE_CELLS) != cudaSuccess) return HYPE_ERR_CUDA;
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, cfg->device) != cudaSuccess) return HYPE_ERR_CUDA;
-    const int bps = stage_blocks_per_sm(cfg->system, cfg->order);
+    const int bps = stage_blocks_per_sm(cfg->system, cfg->order, STAGE_CELLS);
     if (bps < 1) return HYPE_ERR_CUDA;
-    const int strips = stage_strips(cfg->nx);
+    const int strips = stage_strips(cfg->nx, STAGE_CELLS);
     int runs = sms * bps / strips;
     if (runs < 1) runs = 1;
     if (runs > cfg->ny / 8) runs = cfg->ny / 8 > 0 ? cfg->ny / 8 : 1;
 
     StageParams p;
     std::memset(&p, 0, sizeof(p));
-    p.nx = cfg->nx; p.ny = cfg->ny; p.pitch = pitch; p.plane = plane; p.ow_max = STAGE_OW;
+    p.nx = cfg->nx; p.ny = cfg->ny; p.pitch = pitch; p.plane = plane; p.strips = strips; p.runs = runs;
     p.bc[0] = cfg->bc_left; p.bc[1] = cfg->bc_right; p.bc[2] = cfg->bc_bottom; p.bc[3] = cfg->bc_top;
     p.eos.g1 = cfg->gamma1; p.eos.g2 = cfg->gamma2; p.eos.pi1 = cfg->pi1; p.eos.pi2 = cfg->pi2;
     p.eos.fix_p2 = (cfg->flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
@@ -146,7 +146,7 @@ extern "C" HYPE_API int hype_rhs_prim_noalloc(const hype_config *cfg, double t, 
     noalloc_reset_kernel<<<1, 1, 0, 0>>>(sc);
     if (cudaGetLastError() != cudaSuccess) return HYPE_ERR_CUDA;
     if (launch_aos_to_planes(dU, planes, cfg->nx, cfg->ny, nv, pitch, plane, 0) != cudaSuccess) return HYPE_ERR_CUDA;
-    if (launch_stage(cfg->system, cfg->order, tm, p, dim3((unsigned)strips, (unsigned)runs, 1), 0) != cudaSuccess) return HYPE_ERR_CUDA;
+    if (launch_stage(cfg->system, cfg->order, STAGE_CELLS, tm, p, 0) != cudaSuccess) return HYPE_ERR_CUDA;
     DevScalars h_sc;
     if (cudaMemcpy(&h_sc, sc, sizeof(h_sc), cudaMemcpyDeviceToHost) != cudaSuccess) return HYPE_ERR_CUDA;
     if (h_sc.err & ERR_TMA_TIMEOUT) return HYPE_ERR_TIMEOUT;

@@ -3,11 +3,11 @@
 // on the stage input S and writes one SSP-RK stage combination of it, folding
 // the CFL wave-speed maximum (rhs_function_prim.c:617-623) into a device scalar.
 //
-// Tiling.  A block of STAGE_NT threads owns a strip of STAGE_OW columns and a
-// run of `rows` rows.  It marches up its rows; at row r every thread t
-// reconstructs the cell in column x0-1+t (the strip plus one ring column each
-// side), so only two of STAGE_NT reconstructions per row are repeated by the
-// neighbouring strip.  Rows of the conserved state arrive by one TMA 3-D box
+// Tiling.  A tile is a strip of up to CELLS-2 columns and a run of rows of one
+// grid, processed by a block of 2*CELLS threads, two per column.  The block
+// marches up its rows; at row r the thread pair m reconstructs the cell in
+// column x0-1+m (the strip plus one ring column each side), so only two of
+// CELLS reconstructions per row are repeated by the neighbouring strip.  Rows of the conserved state arrive by one TMA 3-D box
 // load per row (all fields, columns x0-4 .. x0+NT+1) into a ring of
 // STAGE_SLOTS shared-memory rows, are patched at domain edges with the
 // boundary-condition copies, and are converted to primitive variables in place.
@@ -56,6 +56,10 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 }
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 
 // Ghost source index along one axis (rhs_function_prim.c:75-315 and the DMDA
 // periodic wrap): transmissive copies the edge cell, reflective mirrors.
@@ -80,14 +84,14 @@ __device__ __forceinline__ void raise_error(DevScalars *sc, unsigned bits, unsig
     atomicMin(&sc->err_cell, cell);
 }
 
-template <int SYS, int N>
+template <int SYS, int N, int CELLS_>
 struct StageKernel {
     using S = System<SYS>;
     using QD = Quad<N>;
     static constexpr int NV = S::NV;
-    static constexpr int NT = STAGE_NT;          // two threads per cell
-    static constexpr int CELLS = STAGE_CELLS;    // reconstruction columns per block
-    static constexpr int BW = STAGE_BW;
+    static constexpr int CELLS = CELLS_;         // reconstruction columns per tile
+    static constexpr int NT = 2 * CELLS;         // two threads per cell
+    static constexpr int BW = CELLS + 6;         // TMA box width
     static constexpr int SLOTS = STAGE_SLOTS;
     static constexpr int NDOF = QD::NDOF;
     static constexpr int NC = NDOF - 1;                    // stored coefficients (k >= 1)
@@ -98,7 +102,7 @@ struct StageKernel {
     static constexpr int COEF_ELEMS = (NC > 2 ? NC : 2) * NV * CELLS;         // also the x-flux exchange (2 NV)
     static constexpr int YT_ELEMS = 2 * NV * CELLS;                            // top-face values, by Gauss point
     static constexpr int CARRY_ELEMS = 4 * NV * CELLS;                         // ncp, t1, G below, E below
-    static constexpr int MIN_BLOCKS = NV <= 6 ? 2 : 1;
+    static constexpr int MIN_BLOCKS = (NV <= 6 ? 2 : 1) * (128 / CELLS);
     static constexpr size_t smem_bytes()
     {
         return 128 /* barriers */ + (size_t)SLOTS * SLOT_STRIDE * 8 + (size_t)(COEF_ELEMS + YT_ELEMS + CARRY_ELEMS) * 8 + 64;
@@ -156,11 +160,13 @@ __device__ __forceinline__ double riemann_gp(const Eos &eos, const double *VL, c
     return s;
 }
 
-template <int SYS, int N>
-__global__ void __launch_bounds__(STAGE_NT, (StageKernel<SYS, N>::MIN_BLOCKS))
-stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
+// One tile of one grid: columns of strip `strip` (of p.strips) and rows of run
+// `run` (of p.runs).  Called by every thread of a block of K::NT threads.
+template <int SYS, int N, int CELLS_>
+__device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorMap *tmap, int strip, int run,
+                                           unsigned char *smem_raw, double *red_s)
 {
-    using K = StageKernel<SYS, N>;
+    using K = StageKernel<SYS, N, CELLS_>;
     using S = typename K::S;
     using QD = typename K::QD;
     constexpr int NV = K::NV, CELLS = K::CELLS, BW = K::BW, SLOTS = K::SLOTS, NDOF = K::NDOF;
@@ -170,24 +176,22 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 
     if (p.sc->done) return;
 
-    extern __shared__ __align__(128) unsigned char smem_raw[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
     double *rows_s = reinterpret_cast<double *>(smem_raw + 128);
     double *coef_s = rows_s + (size_t)SLOTS * K::SLOT_STRIDE;   // [k-1][c][cell]; later [F|D][c][cell]
     double *yt_s = coef_s + K::COEF_ELEMS;                      // [q][c][cell]
     double *carry_s = yt_s + K::YT_ELEMS;                       // [ncp|t1|gb|eb][c][cell]
-    __shared__ double red_s[STAGE_NT / 32];
 
     const int t = threadIdx.x;
     const int m = t >> 1;            // cell of this thread's pair
     const int h = t & 1;             // which half of the pair
     // strips split the columns evenly on even boundaries (TMA x origin alignment);
     // row runs split the rows evenly
-    const int x0 = 2 * (int)(((long long)blockIdx.x * p.nx) / (2LL * gridDim.x));
-    const int x1 = (blockIdx.x + 1 == gridDim.x) ? p.nx : 2 * (int)(((long long)(blockIdx.x + 1) * p.nx) / (2LL * gridDim.x));
+    const int x0 = 2 * (int)(((long long)strip * p.nx) / (2LL * p.strips));
+    const int x1 = (strip + 1 == p.strips) ? p.nx : 2 * (int)(((long long)(strip + 1) * p.nx) / (2LL * p.strips));
     const int owc = x1 - x0;
-    const int y0 = (int)(((long long)blockIdx.y * p.ny) / gridDim.y);
-    const int H = (int)(((long long)(blockIdx.y + 1) * p.ny) / gridDim.y) - y0;
+    const int y0 = (int)(((long long)run * p.ny) / p.runs);
+    const int H = (int)(((long long)(run + 1) * p.ny) / p.runs) - y0;
     if (owc > CELLS - 2 || owc < 1 || H < 1) {   // launch geometry outside what the tiling covers
         if (threadIdx.x == 0) raise_error(p.sc, ERR_BAD_LAUNCH, 0u);
         return;
@@ -204,6 +208,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
     const Eos eos = p.eos;
     const double r1_h = p.r1_h;
 
+    __syncthreads();   // the previous tile of this block is done with every buffer
     if (t == 0) {
         for (int s = 0; s < SLOTS; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
@@ -230,7 +235,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::ROW_BYTES);
-                tma_load_3d(row_ptr(row), &tmap, xs, src, 0, bar);
+                tma_load_3d(row_ptr(row), tmap, xs, src, 0, bar);
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {
@@ -242,7 +247,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
             }
             if (__syncthreads_or(!ok)) {
                 if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
-                return;   // block-uniform exit
+                return;   // block-uniform exit; the caller's next barrier is block-uniform too
             }
             double *rp = row_ptr(row);
             const int src = map_axis(row, p.ny, bcB, bcT);
@@ -594,6 +599,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 
     // ---------------- CFL maximum: warp shuffle, block, one atomic ------------
     if (bad) raise_error(p.sc, ERR_INADMISSIBLE_FACE, bad_cell);
+    __syncthreads();   // red_s is reused tile after tile
     if (p.reduce_smax) {
         double mx = smax_loc;
 #pragma unroll
@@ -603,112 +609,117 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
         if (t == 0) {
             double b = red_s[0];
 #pragma unroll
-            for (int w = 1; w < STAGE_NT / 32; ++w) b = fmax(b, red_s[w]);
+            for (int w = 1; w < K::NT / 32; ++w) b = fmax(b, red_s[w]);
             if (b > 0.0) atomicMax(&p.sc->smax, (unsigned long long)__double_as_longlong(b));
         }
     }
+    for (int k = t; k < SLOTS; k += K::NT) mbar_inval(&bars[k]);
 }
 
-template <int SYS, int N>
-static cudaError_t configure_one()
+template <int SYS, int N, int CELLS>
+__global__ void __launch_bounds__(2 * CELLS, (StageKernel<SYS, N, CELLS>::MIN_BLOCKS))
+stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 {
-    return cudaFuncSetAttribute(stage_kernel<SYS, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)StageKernel<SYS, N>::smem_bytes());
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ double red_s[2 * CELLS / 32];
+    stage_tile<SYS, N, CELLS>(p, &tmap, blockIdx.x, blockIdx.y, smem_raw, red_s);
 }
 
-template <int SYS>
-static size_t smem_sys(int order)
+// Persistent form: the block walks a list of (grid, tile) work items; every grid
+// has its own parameters, tensor map and device scalars.
+template <int SYS, int N, int CELLS>
+__global__ void __launch_bounds__(2 * CELLS, (StageKernel<SYS, N, CELLS>::MIN_BLOCKS))
+stage_batch_kernel(const StageParams *__restrict__ inst, const CUtensorMap *__restrict__ tmaps,
+                   const int2 *__restrict__ work, int nwork)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ double red_s[2 * CELLS / 32];
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 it = work[w];
+        const StageParams &p = inst[it.x];
+        stage_tile<SYS, N, CELLS>(p, &tmaps[it.x], it.y % p.strips, it.y / p.strips, smem_raw, red_s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host dispatch over (system, order, tile width)
+// ---------------------------------------------------------------------------
+struct StageEntry {
+    const void *single;
+    const void *batch;
+    size_t smem;
+    int threads;
+};
+
+template <int SYS, int N, int CELLS>
+static StageEntry entry_of()
+{
+    return StageEntry{reinterpret_cast<const void *>(stage_kernel<SYS, N, CELLS>),
+                      reinterpret_cast<const void *>(stage_batch_kernel<SYS, N, CELLS>),
+                      StageKernel<SYS, N, CELLS>::smem_bytes(), 2 * CELLS};
+}
+
+template <int SYS, int CELLS>
+static StageEntry entry_sys(int order)
 {
     switch (order) {
-    case 0: return StageKernel<SYS, 0>::smem_bytes();
-    case 1: return StageKernel<SYS, 1>::smem_bytes();
-    case 2: return StageKernel<SYS, 2>::smem_bytes();
-    default: return StageKernel<SYS, 3>::smem_bytes();
+    case 0: return entry_of<SYS, 0, CELLS>();
+    case 1: return entry_of<SYS, 1, CELLS>();
+    case 2: return entry_of<SYS, 2, CELLS>();
+    default: return entry_of<SYS, 3, CELLS>();
     }
 }
 
-size_t stage_smem_bytes(int sys, int order)
+template <int CELLS>
+static StageEntry entry_cells(int sys, int order)
 {
     switch (sys) {
-    case SYS_EULER: return smem_sys<SYS_EULER>(order);
-    case SYS_KAPILA: return smem_sys<SYS_KAPILA>(order);
-    default: return smem_sys<SYS_BN>(order);
+    case SYS_EULER: return entry_sys<SYS_EULER, CELLS>(order);
+    case SYS_KAPILA: return entry_sys<SYS_KAPILA, CELLS>(order);
+    default: return entry_sys<SYS_BN, CELLS>(order);
     }
 }
 
-template <int SYS>
-static cudaError_t configure_sys(int order)
+static StageEntry stage_entry(int sys, int order, int cells)
 {
-    switch (order) {
-    case 0: return configure_one<SYS, 0>();
-    case 1: return configure_one<SYS, 1>();
-    case 2: return configure_one<SYS, 2>();
-    default: return configure_one<SYS, 3>();
-    }
+    return cells == 64 ? entry_cells<64>(sys, order) : entry_cells<128>(sys, order);
 }
 
-cudaError_t stage_configure(int sys, int order)
+size_t stage_smem_bytes(int sys, int order, int cells) { return stage_entry(sys, order, cells).smem; }
+int stage_threads(int cells) { return 2 * cells; }
+
+cudaError_t stage_configure(int sys, int order, int cells)
 {
-    switch (sys) {
-    case SYS_EULER: return configure_sys<SYS_EULER>(order);
-    case SYS_KAPILA: return configure_sys<SYS_KAPILA>(order);
-    default: return configure_sys<SYS_BN>(order);
-    }
+    const StageEntry e = stage_entry(sys, order, cells);
+    cudaError_t r = cudaFuncSetAttribute(e.single, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
+    if (r != cudaSuccess) return r;
+    return cudaFuncSetAttribute(e.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
 }
 
-template <int SYS, int N>
-static int bps_one()
+int stage_blocks_per_sm(int sys, int order, int cells)
 {
+    const StageEntry e = stage_entry(sys, order, cells);
     int nb = 0;
-    if (configure_one<SYS, N>() != cudaSuccess) return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, stage_kernel<SYS, N>, STAGE_NT, StageKernel<SYS, N>::smem_bytes()) != cudaSuccess)
-        return 0;
+    if (stage_configure(sys, order, cells) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, e.single, e.threads, e.smem) != cudaSuccess) return 0;
     return nb;
 }
-template <int SYS>
-static int bps_sys(int order)
+
+cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s)
 {
-    switch (order) {
-    case 0: return bps_one<SYS, 0>();
-    case 1: return bps_one<SYS, 1>();
-    case 2: return bps_one<SYS, 2>();
-    default: return bps_one<SYS, 3>();
-    }
-}
-int stage_blocks_per_sm(int sys, int order)
-{
-    switch (sys) {
-    case SYS_EULER: return bps_sys<SYS_EULER>(order);
-    case SYS_KAPILA: return bps_sys<SYS_KAPILA>(order);
-    default: return bps_sys<SYS_BN>(order);
-    }
+    const StageEntry e = stage_entry(sys, order, cells);
+    CUtensorMap tm = tmap;
+    StageParams pp = p;
+    void *args[] = {&tm, &pp};
+    return cudaLaunchKernel(e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
-template <int SYS, int N>
-static cudaError_t launch_one(const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s)
+cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
+                               const int2 *work, int nwork, int blocks, cudaStream_t s)
 {
-    stage_kernel<SYS, N><<<grid, STAGE_NT, StageKernel<SYS, N>::smem_bytes(), s>>>(tmap, p);
-    return cudaGetLastError();
-}
-
-template <int SYS>
-static cudaError_t launch_sys(int order, const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s)
-{
-    switch (order) {
-    case 0: return launch_one<SYS, 0>(tmap, p, grid, s);
-    case 1: return launch_one<SYS, 1>(tmap, p, grid, s);
-    case 2: return launch_one<SYS, 2>(tmap, p, grid, s);
-    default: return launch_one<SYS, 3>(tmap, p, grid, s);
-    }
-}
-
-cudaError_t launch_stage(int sys, int order, const CUtensorMap &tmap, const StageParams &p, dim3 grid, cudaStream_t s)
-{
-    switch (sys) {
-    case SYS_EULER: return launch_sys<SYS_EULER>(order, tmap, p, grid, s);
-    case SYS_KAPILA: return launch_sys<SYS_KAPILA>(order, tmap, p, grid, s);
-    default: return launch_sys<SYS_BN>(order, tmap, p, grid, s);
-    }
+    const StageEntry e = stage_entry(sys, order, cells);
+    void *args[] = {&inst, &tmaps, &work, &nwork};
+    return cudaLaunchKernel(e.batch, dim3((unsigned)blocks, 1, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
 }  // namespace hype

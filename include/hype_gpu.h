@@ -182,6 +182,13 @@ HYPE_API int hype_launch_info(const hype_solver *s, int *grid_x, int *grid_y, in
  * over `reps` launches timed with CUDA events on the solver's stream. */
 HYPE_API int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch);
 
+/* Autotuner: times the stage kernel (hype_time_stage, `reps` launches each) for
+ * every tile shape -- tile width 64 or 128 columns, 1, 2 or 4 waves of row runs
+ * -- on the solver's current state and keeps the fastest.  Results are
+ * unchanged by the choice (bit for bit).  Call before hype_begin or between
+ * steps; reports the chosen width and wave count. */
+HYPE_API int hype_autotune(hype_solver *s, int reps, int *cells, int *waves);
+
 /* Device time of the last hype_solve/hype_wait interval, in milliseconds
  * (CUDA events around the step replays). */
 HYPE_API int hype_last_elapsed_ms(const hype_solver *s, double *ms);

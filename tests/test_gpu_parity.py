@@ -185,3 +185,23 @@ def test_full_size_rhs_windows_and_shift_invariance(system, n, kind, hp, orc):
         R1, dt1, st1 = s.rhs_function_prim(0.0, Us)
     assert st0 == st1 == hp.OK and dt0 == dt1
     assert np.roll(R0.reshape(n, n, cfg.nvar), (37, 101), axis=(0, 1)).tobytes() == R1.reshape(n, n, cfg.nvar).tobytes()
+
+
+def test_autotuned_tiles_give_identical_bits(hp, orc):
+    """Every tile shape the autotuner may pick computes the same bits."""
+    _, cfg, kind, seed = cases.case_by_name("kapila_251x7_three_strips")
+    U = cases.state(cfg, kind, seed)
+    g = GOLDEN["rhs"]["kapila_251x7_three_strips"]
+    with hp.Solver(cases.to_pkg(cfg)) as s:
+        cells, waves = s.autotune(2)
+        assert cells in (64, 128) and waves in (1, 2, 4)
+        R, dt, st = s.rhs_function_prim(0.0, U)
+    assert st == hp.OK and sha(R) == g["sha_RHS"] and float(dt).hex() == g["dt"]
+    cfg2 = O.Config(system=O.KAPILA, order=2, nx=300, ny=40, bc_left=O.REFLECTIVE, **cases.KAPILA_EOS)
+    U2 = cases.state(cfg2, "rough", 3)
+    Ro, dto, _ = orc.rhs(cfg2, U2)
+    with hp.Solver(cases.to_pkg(cfg2)) as s:
+        for _ in range(2):
+            s.autotune(1)
+            R2, dt2, st2 = s.rhs_function_prim(0.0, U2)
+            assert st2 == hp.OK and dt2 == dto and R2.tobytes() == Ro.tobytes()
