@@ -219,6 +219,7 @@ def run_gpu(args, rank, world, local_rank):
         ms = float(tt.item())
     cells = NX * NY
     value = world * cells * args.steps / (ms * 1e-3)
+    U_fp64 = solver.get_state() if not args.no_mixed else None
 
     # dominant kernel: the stage kernel, timed alone (CUDA events, same stream)
     ms_stage = solver.time_stage(20)
@@ -253,6 +254,46 @@ def run_gpu(args, rank, world, local_rank):
     info = solver.launch_info()
     solver.close()
 
+    # mixed-precision form on the same workload and step count, and its error
+    # against the FP64 run (relative L1 / L-infinity per field)
+    mixed = None
+    if not args.no_mixed:
+        cm = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=NX, ny=NY, cfl=0.4, device=local_rank, precision=hp.PREC_MIXED)
+        sm = hp.Solver(cm)
+        sm.set_state(U0)
+        mtile = sm.autotune(3) if not args.no_autotune else None
+        sm.begin(0.0, 1e30, 1 << 30)
+        sm.advance(max(3, args.warmup))
+        sm.wait()
+        barrier()
+        sm.advance(args.steps)
+        _, tm, _, stm = sm.wait()
+        barrier()
+        ms_m = sm.last_elapsed_ms()
+        if world > 1:
+            tt = torch.tensor([ms_m], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms_m = float(tt.item())
+        M = sm.get_state().reshape(-1, 6)
+        F = U_fp64.reshape(-1, 6)
+        ms_stage_m = sm.time_stage(20)
+        sm.close()
+
+        def rel(a, b):
+            return [float(np.abs(a - b).sum() / np.abs(b).sum()), float(np.abs(a - b).max() / np.abs(b).max())]
+        errs = {"rho": rel(M[:, 0] + M[:, 1], F[:, 0] + F[:, 1]), "alpha1": rel(M[:, 5], F[:, 5])}
+        for c, nm in ((0, "a1rho1"), (1, "a2rho2"), (4, "E")):
+            errs[nm] = rel(M[:, c], F[:, c])
+        dm = np.hypot(M[:, 2] - F[:, 2], M[:, 3] - F[:, 3])
+        mag = np.hypot(F[:, 2], F[:, 3])
+        errs["momentum_vector"] = [float(dm.sum() / mag.sum()), float(dm.max() / mag.max())]
+        vm = world * cells * args.steps / (ms_m * 1e-3)
+        mixed = {"value": vm, "unit": UNIT, "ms_per_step": ms_m / args.steps, "speedup_vs_fp64": vm / value,
+                 "status": stm, "stage_ms_per_launch": ms_stage_m, "autotuned_tile": mtile,
+                 "bytes_per_cell_update": 9 * (4 * 4 + 2 * 8),
+                 "rel_error_vs_fp64_after_run": {"fields_L1_Linf": errs, "steps": args.steps + max(3, args.warmup)},
+                 "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt"}
+
     if rank != 0:
         return 0
     cpu = None if args.no_cpu_baseline else cpu_baseline(1, 2)
@@ -271,7 +312,8 @@ def run_gpu(args, rank, world, local_rank):
             "e2e": e2e,
             "gpu_launches": args.steps * 6,
             "clocks": clk.summary(),
-            "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2}}
+            "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2},
+            "forms": {"mixed": mixed}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -285,6 +327,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default stage tile shape")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

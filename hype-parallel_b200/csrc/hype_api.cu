@@ -35,6 +35,11 @@ struct hype_solver {
     int sms = 0;
     int strips = 1, runs = 1;         // tile decomposition of the grid
     int bps = 0;                      // stage blocks per SM
+    // mixed precision (Kapila N=2): state k = 0 (U), 1 (S0), 2 (S1) as FP32 + FP64 planes
+    bool mixed = false;
+    float *mf[3] = {nullptr, nullptr, nullptr};
+    double *md[3] = {nullptr, nullptr, nullptr};
+    MixedMaps mm[3];
     bool began = false;
     double last_ms = 0.0;
     char err[512] = {0};
@@ -141,11 +146,47 @@ static StageParams base_params(const hype_solver *s)
 // resident blocks each), at least 8 rows per run.  Rebuilds the TMA
 // descriptors, whose box width follows the tile width, and drops the captured
 // step graph (recaptured on the next hype_begin / hype_advance).
+// FP32 (4 planes) and FP64 (2 planes) maps of a mixed state, box (cells + 8, 1, planes)
+static int make_mixed_maps(hype_solver *s, MixedMaps *mm, float *pf, double *pd)
+{
+    PFN_tmapEncodeTiled enc = get_encode();
+    if (!enc) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    const cuuint32_t bw = (cuuint32_t)mixed_box_width(s->cells);
+    cuuint64_t dimf[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, 4ull};
+    cuuint64_t strf[2] = {(cuuint64_t)s->pitch * 4ull, (cuuint64_t)s->plane * 4ull};
+    cuuint32_t boxf[3] = {bw, 1u, 4u};
+    cuuint64_t dimd[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, 2ull};
+    cuuint64_t strd[2] = {(cuuint64_t)s->pitch * 8ull, (cuuint64_t)s->plane * 8ull};
+    cuuint32_t boxd[3] = {bw, 1u, 2u};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    CUresult r = enc(&mm->f, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, pf, dimf, strf, boxf, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP32 planes) failed (%d)", (int)r);
+    r = enc(&mm->d, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, pd, dimd, strd, boxd, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP64 planes) failed (%d)", (int)r);
+    return HYPE_OK;
+}
+
 static int set_tiling(hype_solver *s, int cells, int waves = 1)
 {
     const hype_config *cfg = &s->cfg;
     int rc;
     s->cells = cells;
+    if (s->mixed) {
+        s->bps = mixed_blocks_per_sm(cells);
+        if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "mixed stage kernel does not fit on an SM");
+        s->strips = mixed_strips(cfg->nx, cells);
+        s->waves = waves > 0 ? waves : 1;
+        int runs = s->sms * s->bps * s->waves / s->strips;
+        if (runs < 1) runs = 1;
+        if (runs > cfg->ny / 8) runs = cfg->ny / 8 > 0 ? cfg->ny / 8 : 1;
+        s->runs = runs;
+        for (int k = 0; k < 3; ++k)
+            if ((rc = make_mixed_maps(s, &s->mm[k], s->mf[k], s->md[k]))) return rc;
+        if (s->step_exec) { cudaGraphExecDestroy(s->step_exec); s->step_exec = nullptr; }
+        return HYPE_OK;
+    }
     CUDA_TRY(s, stage_configure(cfg->system, cfg->order, cells));
     s->bps = stage_blocks_per_sm(cfg->system, cfg->order, cells);
     if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "stage kernel does not fit on an SM");
@@ -177,12 +218,41 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
     return launch_stage(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
 }
 
+// mixed-precision stage: input state k_in, output k_out (or the interleaved
+// FP64 RHS for OUT_RHS), second state k_x
+static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double ka, double kb, double kc, int k_x, int reduce,
+                           double *out_rhs = nullptr)
+{
+    MixedParams p;
+    std::memset(&p, 0, sizeof(p));
+    p.nx = s->cfg.nx; p.ny = s->cfg.ny; p.pitch = s->pitch; p.plane = s->plane;
+    p.bc[0] = s->cfg.bc_left; p.bc[1] = s->cfg.bc_right; p.bc[2] = s->cfg.bc_bottom; p.bc[3] = s->cfg.bc_top;
+    p.eos.g1 = s->cfg.gamma1; p.eos.g2 = s->cfg.gamma2; p.eos.pi1 = s->cfg.pi1; p.eos.pi2 = s->cfg.pi2;
+    p.r1_h = s->r1_h; p.cfl_h = s->cfl_h;
+    p.in_f = s->mf[k_in]; p.in_d = s->md[k_in];
+    if (k_x >= 0) { p.xn_f = s->mf[k_x]; p.xn_d = s->md[k_x]; }
+    if (k_out >= 0) { p.out_f = s->mf[k_out]; p.out_d = s->md[k_out]; }
+    p.out_rhs = out_rhs;
+    p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc;
+    p.sc = s->dSc; p.reduce_smax = reduce;
+    p.strips = s->strips; p.runs = s->runs;
+    return launch_mixed(s->cells, s->mm[k_in], p, s->stream);
+}
+
 // One SSP-RK step on the device state (hype.c:362-382 schemes, petsc TSSSP forms).
 static cudaError_t enqueue_step(hype_solver *s)
 {
     cudaError_t e;
     const double cfl_h = s->cfl_h;
     if ((e = launch_begin_step(s->dSc, s->stream)) != cudaSuccess) return e;
+    if (s->mixed) {   // SSPRKS3 with 4 stages, as below, on the mixed state
+        const int n = 2, ns = 4, r = ns - n;
+        if ((e = stage_m(s, 0, 1, OUT_AXPY, 0, (double)r, 0, -1, 0)) != cudaSuccess) return e;
+        if ((e = stage_m(s, 1, 2, OUT_AXPY, 0, (double)r, 0, -1, 0)) != cudaSuccess) return e;
+        if ((e = stage_m(s, 2, 1, OUT_ZXS, 1. * n / (2 * n - 1.), (double)(r * (2 * n - 1)), (n - 1.) / (2 * n - 1.), 0, 0)) != cudaSuccess) return e;
+        if ((e = stage_m(s, 1, 0, OUT_AXPY, 0, (double)r, 0, -1, 1)) != cudaSuccess) return e;
+        return launch_end_step(s->dSc, cfl_h, s->stream);
+    }
     switch (s->cfg.order) {
     case 0:   // TSEULER: u += dt F(u)
         if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, 1.0, 0, nullptr, nullptr, 1)) != cudaSuccess) return e;
@@ -251,6 +321,8 @@ static int check_config(const hype_config *c, hype_solver *s)
         return fail(s, HYPE_ERR_INVALID, "unknown precision %d", c->precision);
     if (c->precision == HYPE_PREC_MIXED && c->system != HYPE_KAPILA_5EQN)
         return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for the Kapila system");
+    if (c->precision == HYPE_PREC_MIXED && (c->order != 2 || c->bc_left == HYPE_BC_INLET))
+        return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for N = 2 without inlet boundaries");
     return HYPE_OK;
 }
 
@@ -313,6 +385,7 @@ int hype_destroy(hype_solver *s)
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
     double *bufs[] = {s->dU, s->dS0, s->dS1, s->dS2, s->dAosIn, s->dAosOut, s->dInlet, s->dRed};
     for (double *b : bufs) if (b) cudaFree(b);
+    for (int k = 0; k < 3; ++k) { if (s->mf[k]) cudaFree(s->mf[k]); if (s->md[k]) cudaFree(s->md[k]); }
     if (s->dSc) cudaFree(s->dSc);
     if (s->hSc) cudaFreeHost(s->hSc);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -339,10 +412,10 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     cudaDeviceProp prop;
     CUDA_TRY(s, cudaGetDeviceProperties(&prop, cfg->device));
     if (prop.major != 10) return fail(s, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", cfg->device, prop.major, prop.minor);
-    if (cfg->precision != HYPE_PREC_FP64) return fail(s, HYPE_ERR_INVALID, "mixed precision solver objects are created with hype_batch_*");
+    s->mixed = cfg->precision == HYPE_PREC_MIXED;
 
     s->nv = hype_nvar(cfg->system);
-    s->pitch = (cfg->nx + 15) & ~15;                 // 128-byte rows
+    s->pitch = s->mixed ? ((cfg->nx + 31) & ~31) : ((cfg->nx + 15) & ~15);   // 128-byte rows
     s->plane = (long long)s->pitch * cfg->ny;
     s->h = (cfg->x_max - cfg->x_min) / (double)cfg->nx;   // hype.c:57
     s->r1_h = 1. / s->h;                                  // rhs_function_prim.c:26
@@ -361,6 +434,15 @@ int hype_create(const hype_config *cfg, hype_solver **out)
         if (cudaMalloc(&s->dS2, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc failed");
         CUDA_TRY(s, cudaMemset(s->dS2, 0, state_bytes));
     }
+    if (s->mixed) {
+        for (int k = 0; k < 3; ++k) {
+            if (cudaMalloc(&s->mf[k], sizeof(float) * 4 * (size_t)s->plane) != cudaSuccess ||
+                cudaMalloc(&s->md[k], sizeof(double) * 2 * (size_t)s->plane) != cudaSuccess)
+                return fail(s, HYPE_ERR_NOMEM, "cudaMalloc of the mixed state failed");
+            CUDA_TRY(s, cudaMemset(s->mf[k], 0, sizeof(float) * 4 * (size_t)s->plane));
+            CUDA_TRY(s, cudaMemset(s->md[k], 0, sizeof(double) * 2 * (size_t)s->plane));
+        }
+    }
     if (cudaMalloc(&s->dAosIn, aos_bytes) != cudaSuccess || cudaMalloc(&s->dAosOut, aos_bytes) != cudaSuccess)
         return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", aos_bytes);
     CUDA_TRY(s, cudaMalloc(&s->dRed, sizeof(double) * TOTALS_SCRATCH));
@@ -375,7 +457,7 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     }
 
     s->sms = prop.multiProcessorCount;
-    return set_tiling(s, STAGE_CELLS);
+    return set_tiling(s, s->mixed ? MIXED_CELLS : STAGE_CELLS);
 }
 
 static int read_scalars(hype_solver *s)
@@ -400,11 +482,25 @@ static int reset_scalars(hype_solver *s)
     return HYPE_OK;
 }
 
+// interleaved FP64 state (device) -> state k (0 = U, 1 = S0) in the solver's layout
+static cudaError_t load_state(hype_solver *s, const double *aos, int k)
+{
+    if (s->mixed) return launch_aos_to_mixed(aos, s->mf[k], s->md[k], s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream);
+    return launch_aos_to_planes(aos, k == 0 ? s->dU : s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream);
+}
+static cudaError_t store_state(hype_solver *s, int k, double *aos)
+{
+    if (s->mixed) return launch_mixed_to_aos(s->mf[k], s->md[k], aos, s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream);
+    return launch_planes_to_aos(k == 0 ? s->dU : s->dS0, aos, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream);
+}
+
+// RHS of state S0 into an interleaved device array
 static int rhs_common(hype_solver *s, double *dRHS_aos, double *dt)
 {
     int rc;
     if ((rc = reset_scalars(s))) return rc;
-    CUDA_TRY(s, stage(s, s->dS0, dRHS_aos, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
+    if (s->mixed) CUDA_TRY(s, stage_m(s, 1, -1, OUT_RHS, 0, 1.0, 0, -1, 1, dRHS_aos));
+    else CUDA_TRY(s, stage(s, s->dS0, dRHS_aos, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
     if ((rc = read_scalars(s))) return rc;
     if (dt) {
         double smax;
@@ -419,11 +515,11 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
 {
     (void)t;
     if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
-    if (!s->dU) return fail(s, HYPE_ERR_INVALID, "solver not created");
+    if (!s->dSc) return fail(s, HYPE_ERR_INVALID, "solver not created");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
     CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(s, launch_aos_to_planes(s->dAosIn, s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, load_state(s, s->dAosIn, 1));
     int rc = rhs_common(s, s->dAosOut, dt);
     if (rc && rc != HYPE_ERR_INADMISSIBLE) return rc;
     CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
@@ -436,7 +532,7 @@ int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRH
     (void)t;
     if (!s || !dU || !dRHS) return fail(s, HYPE_ERR_INVALID, "null argument");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
-    CUDA_TRY(s, launch_aos_to_planes(dU, s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, load_state(s, dU, 1));
     return rhs_common(s, dRHS, dt);
 }
 
@@ -446,7 +542,7 @@ int hype_set_state(hype_solver *s, const double *U)
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
     CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(s, launch_aos_to_planes(s->dAosIn, s->dU, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, load_state(s, s->dAosIn, 0));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return HYPE_OK;
 }
@@ -456,7 +552,7 @@ int hype_get_state(hype_solver *s, double *U)
     if (!s || !U) return fail(s, HYPE_ERR_INVALID, "null argument");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
-    CUDA_TRY(s, launch_planes_to_aos(s->dU, s->dAosOut, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, store_state(s, 0, s->dAosOut));
     CUDA_TRY(s, cudaMemcpyAsync(U, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return HYPE_OK;
@@ -489,7 +585,8 @@ int hype_begin(hype_solver *s, double t0, double t_final, int max_steps)
     s->hSc->t = t0; s->hSc->t_final = t_final; s->hSc->max_steps = max_steps;
     CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
     // hype.c:343: one RHS evaluation of the initial state seeds Ctx.dt
-    CUDA_TRY(s, stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1));
+    if (s->mixed) CUDA_TRY(s, stage_m(s, 0, -1, OUT_RHS, 0, 1.0, 0, -1, 1, s->dAosOut));
+    else CUDA_TRY(s, stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1));
     CUDA_TRY(s, launch_seed_dt(s->dSc, s->cfl_h, s->stream));
     if ((rc = ensure_step_graph(s))) return rc;
     s->began = true;
@@ -545,7 +642,11 @@ int hype_totals(hype_solver *s, int scaled, double *totals, double *amin, double
     if (!s || !totals) return fail(s, HYPE_ERR_INVALID, "null argument");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     std::vector<double> h((size_t)s->nv + 2);
-    CUDA_TRY(s, launch_totals(s->dU, s->dRed, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane,
+    if (s->mixed) {   // the mixed state widened to FP64 planes in the S0 buffer first
+        CUDA_TRY(s, store_state(s, 0, s->dAosOut));
+        CUDA_TRY(s, launch_aos_to_planes(s->dAosOut, s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+    }
+    CUDA_TRY(s, launch_totals(s->mixed ? s->dS0 : s->dU, s->dRed, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane,
                               s->cfg.system == HYPE_EULER ? -1 : (s->cfg.system == HYPE_KAPILA_5EQN ? 5 : 8), s->stream));
     CUDA_TRY(s, cudaMemcpyAsync(h.data(), s->dRed, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
@@ -562,7 +663,7 @@ int hype_launch_info(const hype_solver *s, int *gx, int *gy, int *threads, size_
     if (gx) *gx = s->strips;
     if (gy) *gy = s->runs;
     if (threads) *threads = stage_threads(s->cells);
-    if (smem) *smem = stage_smem_bytes(s->cfg.system, s->cfg.order, s->cells);
+    if (smem) *smem = s->mixed ? mixed_smem_bytes(s->cells) : stage_smem_bytes(s->cfg.system, s->cfg.order, s->cells);
     if (bps) *bps = s->bps;
     return HYPE_OK;
 }
@@ -579,10 +680,19 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
     if ((rc = reset_scalars(s))) return rc;
     s->hSc->dt = 1e-30;   // a representative AXPY stage S0 -> S1 with a negligible step
     CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(s, cudaMemcpyAsync(s->dS0, s->dU, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream));
-    CUDA_TRY(s, stage(s, s->dS0, s->dS1, OUT_AXPY, 0, 2.0, 0, nullptr, nullptr, 1));   // warm
+    auto one = [&]() -> cudaError_t {
+        if (s->mixed) return stage_m(s, 1, 2, OUT_AXPY, 0, 2.0, 0, -1, 1);
+        return stage(s, s->dS0, s->dS1, OUT_AXPY, 0, 2.0, 0, nullptr, nullptr, 1);
+    };
+    if (s->mixed) {
+        CUDA_TRY(s, cudaMemcpyAsync(s->mf[1], s->mf[0], sizeof(float) * 4 * (size_t)s->plane, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(s->md[1], s->md[0], sizeof(double) * 2 * (size_t)s->plane, cudaMemcpyDeviceToDevice, s->stream));
+    } else {
+        CUDA_TRY(s, cudaMemcpyAsync(s->dS0, s->dU, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream));
+    }
+    CUDA_TRY(s, one());   // warm
     CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
-    for (int k = 0; k < reps; ++k) CUDA_TRY(s, stage(s, s->dS0, s->dS1, OUT_AXPY, 0, 2.0, 0, nullptr, nullptr, 1));
+    for (int k = 0; k < reps; ++k) CUDA_TRY(s, one());
     CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
     if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
     float ms = 0.f;
@@ -605,7 +715,7 @@ int hype_autotune(hype_solver *s, int reps, int *cells_out, int *waves_out)
     for (int c : cand_cells)
         for (int w : cand_waves) {
             if ((rc = set_tiling(s, c, w))) return rc;
-            if (stage_strips(s->cfg.nx, c) * s->runs < 1) continue;
+
             double ms = 0.0;
             if ((rc = hype_time_stage(s, reps, &ms))) return rc;
             if (ms < best) { best = ms; best_c = c; best_w = w; }

@@ -83,4 +83,45 @@ cudaError_t launch_totals(const double *planes, double *red, int nx, int ny, int
                           cudaStream_t s);
 constexpr size_t TOTALS_SCRATCH = 64 + 513 * 11;
 
+// ---------------------------------------------------------------------------
+// Mixed precision (Kapila five-equation model, N = 2).  State: four FP32
+// planes (a1 rho1, a2 rho2, rho u, rho v) and two FP64 planes (E, a1) with one
+// element pitch; the FP64 pair carries the quantities whose stiffened-gas
+// cancellation (p from E with P_inf ~ 6e8) FP32 cannot resolve.
+// ---------------------------------------------------------------------------
+struct MixedParams {
+    int nx, ny, pitch;          // element pitch of every plane (multiple of 32)
+    long long plane;            // elements per plane
+    int bc[4];
+    Eos eos;
+    double r1_h, cfl_h;
+    const float *in_f; const double *in_d;     // stage input S (behind the two tensor maps)
+    const float *xn_f; const double *xn_d;     // second state X (u^n)
+    float *out_f; double *out_d;               // output state
+    double *out_rhs;                           // OUT_RHS: interleaved FP64 RHS, 6 per cell
+    int mode;
+    double ka, kb, kc;
+    DevScalars *sc;
+    int reduce_smax;
+    int strips, runs;
+};
+struct MixedMaps {
+    CUtensorMap f;              // FP32 planes: (nx, ny, 4), box (cells + 8, 1, 4)
+    CUtensorMap d;              // FP64 planes: (nx, ny, 2), box (cells + 8, 1, 2)
+};
+constexpr int MIXED_CELLS = 128;
+inline int mixed_box_width(int cells) { return cells + 8; }
+// strips with origins 4*floor(s*nx/(4S)) (16-byte aligned FP32 TMA origin):
+// S = ceil(nx/(cells-6)) keeps every strip within cells-2 columns
+inline int mixed_strips(int nx, int cells) { return (nx + (cells - 6) - 1) / (cells - 6); }
+size_t mixed_smem_bytes(int cells);
+int mixed_threads(int cells);
+int mixed_blocks_per_sm(int cells);
+cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s);
+cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int nwork,
+                               int blocks, cudaStream_t s);
+// layout changes between the interleaved FP64 Vec and the mixed planes
+cudaError_t launch_aos_to_mixed(const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane, cudaStream_t s);
+cudaError_t launch_mixed_to_aos(const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane, cudaStream_t s);
+
 }  // namespace hype

@@ -1,0 +1,69 @@
+// hype_tma.cuh -- device helpers shared by the stage kernels: TMA tensor
+// loads and mbarriers (inline PTX), ghost-index mapping of the boundary
+// conditions, and the device error word.
+#pragma once
+#include <cuda.h>
+#include <cstdint>
+#include "hype_internal.h"
+
+namespace hype {
+
+// ---------------------------------------------------------------------------
+// TMA / mbarrier helpers (inline PTX, sm_90+ forms, valid on sm_100a)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                 ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Ghost source index along one axis (rhs_function_prim.c:75-315 and the DMDA
+// periodic wrap): transmissive copies the edge cell, reflective mirrors.
+__device__ __forceinline__ int map_axis(int g, int n, int bc_lo, int bc_hi)
+{
+    if (g < 0) {
+        if (bc_lo == BC_PERIODIC || bc_hi == BC_PERIODIC) return g + n;
+        if (bc_lo == BC_REFLECTIVE) return -1 - g;
+        return 0;   // transmissive (inlet columns are replaced after conversion)
+    }
+    if (g >= n) {
+        if (bc_lo == BC_PERIODIC || bc_hi == BC_PERIODIC) return g - n;
+        if (bc_hi == BC_REFLECTIVE) return 2 * (n - 1) - g + 1;
+        return n - 1;
+    }
+    return g;
+}
+
+__device__ __forceinline__ void raise_error(DevScalars *sc, unsigned bits, unsigned cell)
+{
+    atomicOr(&sc->err, bits);
+    atomicMin(&sc->err_cell, cell);
+}
+
+}  // namespace hype

@@ -65,6 +65,8 @@ def test_config_defaults_follow_reference_main(hp):
     (dict(cfl=0.0), "CFL"),
     (dict(x_max=0.0), "domain"),
     (dict(precision=7), "precision"),
+    (dict(precision=1, system=2), "Kapila"),
+    (dict(precision=1, order=1), "N = 2"),
 ])
 def test_invalid_configs_rejected_before_device(hp, change, needle):
     cfg = hp.Config(nx=16, ny=16)
