@@ -80,6 +80,16 @@ class Config:
         return _Cfg(**dataclasses.asdict(self))
 
 
+class _BatchCfg(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_instances", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
+                ("max_cells", ctypes.c_longlong)]
+
+
+class _InstStatus(ctypes.Structure):
+    _fields_ = [("active", ctypes.c_int), ("done", ctypes.c_int), ("steps", ctypes.c_int), ("status", ctypes.c_int),
+                ("t", ctypes.c_double), ("dt_next", ctypes.c_double)]
+
+
 _DP = ctypes.POINTER(ctypes.c_double)
 _lib = None
 
@@ -121,6 +131,25 @@ def lib() -> ctypes.CDLL:
         for name in ("hype_ic_bn_discs", "hype_ic_euler_quadrants"):
             getattr(L, name).argtypes = [ctypes.POINTER(_Cfg), ctypes.c_uint64, _DP]
         L.hype_ic_smooth_vortex.argtypes = [ctypes.POINTER(_Cfg), _DP]
+        # include/hype_batch.h
+        IP = ctypes.POINTER(ctypes.c_int)
+        L.hype_batch_config_default.argtypes = [ctypes.POINTER(_BatchCfg)]
+        L.hype_batch_create.argtypes = [ctypes.POINTER(_BatchCfg), ctypes.POINTER(vp)]
+        L.hype_batch_destroy.argtypes = [vp]
+        L.hype_batch_last_error.argtypes = [vp]
+        L.hype_batch_last_error.restype = ctypes.c_char_p
+        L.hype_batch_instance_bytes.argtypes = [ctypes.POINTER(_Cfg)]
+        L.hype_batch_instance_bytes.restype = ctypes.c_size_t
+        L.hype_batch_add.argtypes = [vp, ctypes.POINTER(_Cfg), _DP, ctypes.c_double, ctypes.c_double, ctypes.c_int, IP]
+        L.hype_batch_remove.argtypes = [vp, ctypes.c_int]
+        L.hype_batch_advance.argtypes = [vp, ctypes.c_int]
+        L.hype_batch_sync.argtypes = [vp]
+        L.hype_batch_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(_InstStatus)]
+        L.hype_batch_get_state.argtypes = [vp, ctypes.c_int, _DP]
+        L.hype_batch_set_tiling.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.hype_batch_autotune.argtypes = [vp, ctypes.c_int, IP, IP]
+        L.hype_batch_info.argtypes = [vp, IP, IP, ctypes.POINTER(ctypes.c_size_t)]
+        L.hype_batch_last_elapsed_ms.argtypes = [vp, _DP]
         _lib = L
     return _lib
 
@@ -278,4 +307,107 @@ class Solver:
     def last_elapsed_ms(self) -> float:
         ms = ctypes.c_double(0.0)
         self._check(lib().hype_last_elapsed_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+
+class Batch:
+    """Many independent instances stepped together (include/hype_batch.h).
+
+    ``add(cfg, U0, t0, t_final, max_steps)`` admits an instance (its own time
+    loop, as ``Solver.solve``) and returns its id; ``advance(n)`` enqueues n
+    steps of every instance; ``sync()`` waits and refreshes ``status(id)``.
+    """
+
+    def __init__(self, max_instances: int = 256, hbm_budget: int = 0, max_cells: int = 2048 * 2048, device: int = 0):
+        c = _BatchCfg()
+        lib().hype_batch_config_default(ctypes.byref(c))
+        c.device, c.max_instances, c.hbm_budget, c.max_cells = device, max_instances, hbm_budget, max_cells
+        self._h = ctypes.c_void_p()
+        self.cfgs = {}
+        st = lib().hype_batch_create(ctypes.byref(c), ctypes.byref(self._h))
+        if st != OK:
+            msg = lib().hype_batch_last_error(self._h).decode() if self._h else lib().hype_status_string(st).decode()
+            lib().hype_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            raise HypeError(st, msg)
+
+    def close(self):
+        if self._h:
+            lib().hype_batch_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int) -> None:
+        if st != OK:
+            raise HypeError(st, lib().hype_batch_last_error(self._h).decode())
+
+    @staticmethod
+    def instance_bytes(cfg: Config) -> int:
+        return lib().hype_batch_instance_bytes(ctypes.byref(cfg.c_struct()))
+
+    def try_add(self, cfg: Config, U0: np.ndarray, t0: float, t_final: float, max_steps: int):
+        """Returns (status, id); status ERR_NOMEM / ERR_BUSY when admission refuses."""
+        U0 = np.ascontiguousarray(U0, dtype=np.float64)
+        if U0.size != cfg.nx * cfg.ny * cfg.nvar:
+            raise ValueError("U0 has the wrong size")
+        i = ctypes.c_int(-1)
+        st = lib().hype_batch_add(self._h, ctypes.byref(cfg.c_struct()), _ptr(U0), t0, t_final, max_steps, ctypes.byref(i))
+        if st == OK:
+            self.cfgs[i.value] = cfg
+        return st, i.value
+
+    def add(self, cfg: Config, U0: np.ndarray, t0: float, t_final: float, max_steps: int) -> int:
+        st, i = self.try_add(cfg, U0, t0, t_final, max_steps)
+        self._check(st)
+        return i
+
+    def remove(self, i: int) -> None:
+        self._check(lib().hype_batch_remove(self._h, i))
+        self.cfgs.pop(i, None)
+
+    def advance(self, nsteps: int) -> None:
+        self._check(lib().hype_batch_advance(self._h, nsteps))
+
+    def sync(self) -> None:
+        self._check(lib().hype_batch_sync(self._h))
+
+    def status(self, i: int) -> dict:
+        s = _InstStatus()
+        self._check(lib().hype_batch_status(self._h, i, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in _InstStatus._fields_}
+
+    def get_state(self, i: int) -> np.ndarray:
+        c = self.cfgs[i]
+        U = np.empty(c.nx * c.ny * c.nvar, dtype=np.float64)
+        self._check(lib().hype_batch_get_state(self._h, i, _ptr(U)))
+        return U
+
+    def set_tiling(self, cells: int, rows: int) -> None:
+        self._check(lib().hype_batch_set_tiling(self._h, cells, rows))
+
+    def autotune(self, reps: int = 3):
+        c, r = ctypes.c_int(0), ctypes.c_int(0)
+        self._check(lib().hype_batch_autotune(self._h, reps, ctypes.byref(c), ctypes.byref(r)))
+        return c.value, r.value
+
+    def info(self) -> dict:
+        n, w = ctypes.c_int(0), ctypes.c_int(0)
+        b = ctypes.c_size_t(0)
+        self._check(lib().hype_batch_info(self._h, ctypes.byref(n), ctypes.byref(w), ctypes.byref(b)))
+        return {"instances": n.value, "work_items": w.value, "bytes_in_use": b.value}
+
+    def last_elapsed_ms(self) -> float:
+        ms = ctypes.c_double(0.0)
+        self._check(lib().hype_batch_last_elapsed_ms(self._h, ctypes.byref(ms)))
         return ms.value

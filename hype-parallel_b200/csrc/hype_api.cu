@@ -81,31 +81,40 @@ static PFN_tmapEncodeTiled get_encode()
     return fn;
 }
 
+namespace hype {
+CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, int ny, int nplanes, int pitch, long long plane,
+                           int box_w)
+{
+    PFN_tmapEncodeTiled enc = get_encode();
+    if (!enc) return CUDA_ERROR_NOT_SUPPORTED;
+    const cuuint64_t es = fp32 ? 4ull : 8ull;
+    cuuint64_t dims[3] = {(cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nplanes};
+    cuuint64_t strides[2] = {(cuuint64_t)pitch * es, (cuuint64_t)plane * es};
+    cuuint32_t box[3] = {(cuuint32_t)box_w, 1u, (cuuint32_t)nplanes};
+    cuuint32_t estr[3] = {1u, 1u, 1u};
+    return enc(m, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<void *>(base), dims,
+               strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+}
+}  // namespace hype
+
 // 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (cells + 6, 1, nvar).
 static int make_tmap(hype_solver *s, CUtensorMap *m, double *base)
 {
-    PFN_tmapEncodeTiled enc = get_encode();
-    if (!enc) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    cuuint64_t dims[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, (cuuint64_t)s->nv};
-    cuuint64_t strides[2] = {(cuuint64_t)s->pitch * 8ull, (cuuint64_t)s->plane * 8ull};
-    cuuint32_t box[3] = {(cuuint32_t)stage_box_width(s->cells), 1u, (cuuint32_t)s->nv};
-    cuuint32_t estr[3] = {1u, 1u, 1u};
-    CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = encode_planes_map(m, base, false, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, stage_box_width(s->cells));
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return HYPE_OK;
 }
 
 // kapila_5eqn.c:485-513 evaluated once on the host (the profile does not depend
 // on t) for the three left ghost columns of every ghost-extended row.
-static void fill_inlet(const hype_solver *s, std::vector<double> &tab)
+void hype::inlet_table(const hype_config &c, double h, std::vector<double> &tab)
 {
-    const hype_config &c = s->cfg;
-    const int ny = c.ny, nv = s->nv;
+    const int ny = c.ny, nv = hype_nvar(c.system);
     tab.assign((size_t)3 * (ny + 6) * nv, 0.0);
     for (int g = -3; g < 0; ++g)
         for (int j = -3; j < ny + 3; ++j) {
-            const double y = c.y_min + ((double)j + 0.5) * s->h;
+            const double y = c.y_min + ((double)j + 0.5) * h;
             const double M = 2.0, rho_air = 1.0, rho_water = 1000.0, P = 1.013;
             const double U_avg = M * std::sqrt(c.gamma2 * P / rho_air);
             const double phi_R = 1.0 - 1.0e-6, phi_L = 1.0e-6;
@@ -149,21 +158,10 @@ static StageParams base_params(const hype_solver *s)
 // FP32 (4 planes) and FP64 (2 planes) maps of a mixed state, box (cells + 8, 1, planes)
 static int make_mixed_maps(hype_solver *s, MixedMaps *mm, float *pf, double *pd)
 {
-    PFN_tmapEncodeTiled enc = get_encode();
-    if (!enc) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    const cuuint32_t bw = (cuuint32_t)mixed_box_width(s->cells);
-    cuuint64_t dimf[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, 4ull};
-    cuuint64_t strf[2] = {(cuuint64_t)s->pitch * 4ull, (cuuint64_t)s->plane * 4ull};
-    cuuint32_t boxf[3] = {bw, 1u, 4u};
-    cuuint64_t dimd[3] = {(cuuint64_t)s->cfg.nx, (cuuint64_t)s->cfg.ny, 2ull};
-    cuuint64_t strd[2] = {(cuuint64_t)s->pitch * 8ull, (cuuint64_t)s->plane * 8ull};
-    cuuint32_t boxd[3] = {bw, 1u, 2u};
-    cuuint32_t estr[3] = {1u, 1u, 1u};
-    CUresult r = enc(&mm->f, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, pf, dimf, strf, boxf, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                     CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const int bw = mixed_box_width(s->cells);
+    CUresult r = encode_planes_map(&mm->f, pf, true, s->cfg.nx, s->cfg.ny, 4, s->pitch, s->plane, bw);
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP32 planes) failed (%d)", (int)r);
-    r = enc(&mm->d, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, pd, dimd, strd, boxd, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    r = encode_planes_map(&mm->d, pd, false, s->cfg.nx, s->cfg.ny, 2, s->pitch, s->plane, bw);
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP64 planes) failed (%d)", (int)r);
     return HYPE_OK;
 }
@@ -239,62 +237,45 @@ static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double
     return launch_mixed(s->cells, s->mm[k_in], p, s->stream);
 }
 
-// One SSP-RK step on the device state (hype.c:362-382 schemes, petsc TSSSP forms).
+static double *buf_of(hype_solver *s, int b)
+{
+    switch (b) {
+    case B_U: return s->dU;
+    case B_S0: return s->dS0;
+    case B_S1: return s->dS1;
+    case B_S2: return s->dS2;
+    default: return nullptr;
+    }
+}
+
+// One SSP-RK step on the device state: the stage list of ssp_plan between the
+// step-control kernels.  The mixed state has the same buffer roles (U, S0, S1).
 static cudaError_t enqueue_step(hype_solver *s)
 {
     cudaError_t e;
-    const double cfl_h = s->cfl_h;
+    PlanStage plan[MAX_PLAN];
+    int copy_back = 0;
+    const int ns = ssp_plan(s->cfg.order, plan, &copy_back);
     if ((e = launch_begin_step(s->dSc, s->stream)) != cudaSuccess) return e;
-    if (s->mixed) {   // SSPRKS3 with 4 stages, as below, on the mixed state
-        const int n = 2, ns = 4, r = ns - n;
-        if ((e = stage_m(s, 0, 1, OUT_AXPY, 0, (double)r, 0, -1, 0)) != cudaSuccess) return e;
-        if ((e = stage_m(s, 1, 2, OUT_AXPY, 0, (double)r, 0, -1, 0)) != cudaSuccess) return e;
-        if ((e = stage_m(s, 2, 1, OUT_ZXS, 1. * n / (2 * n - 1.), (double)(r * (2 * n - 1)), (n - 1.) / (2 * n - 1.), 0, 0)) != cudaSuccess) return e;
-        if ((e = stage_m(s, 1, 0, OUT_AXPY, 0, (double)r, 0, -1, 1)) != cudaSuccess) return e;
-        return launch_end_step(s->dSc, cfl_h, s->stream);
+    for (int k = 0; k < ns; ++k) {
+        const PlanStage &q = plan[k];
+        if (s->mixed) e = stage_m(s, q.in, q.out, q.mode, q.ka, q.kb, q.kc, q.x, q.reduce);
+        else e = stage(s, buf_of(s, q.in), buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x), buf_of(s, q.out2), q.reduce);
+        if (e != cudaSuccess) return e;
     }
-    switch (s->cfg.order) {
-    case 0:   // TSEULER: u += dt F(u)
-        if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, 1.0, 0, nullptr, nullptr, 1)) != cudaSuccess) return e;
-        if ((e = cudaMemcpyAsync(s->dU, s->dS0, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream)) != cudaSuccess) return e;
-        break;
-    case 1: { // SSPRKS2, s = 2: w = u + (dt/1) F(u); u = ((1/2) w + (dt/2) F(w)) + (1/2) u
-        const int ns = 2;
-        if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, (ns - 1.), 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
-        if ((e = stage(s, s->dS0, s->dU, OUT_ZSX, (ns - 1.) / ns, (double)ns, 1. / ns, s->dU, nullptr, 1)) != cudaSuccess) return e;
-        break;
-    }
-    case 2: { // SSPRKS3, s = 4, n = 2, r = 2
-        const int n = 2, ns = 4, r = ns - n;
-        if ((e = stage(s, s->dU, s->dS0, OUT_AXPY, 0, (double)r, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
-        if ((e = stage(s, s->dS0, s->dS1, OUT_AXPY, 0, (double)r, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
-        // VecAXPBYPCZ(w0, n/(2n-1), (n-1) dt/(r(2n-1)), (n-1)/(2n-1), w1 = u^n, F)
-        if ((e = stage(s, s->dS1, s->dS0, OUT_ZXS, 1. * n / (2 * n - 1.), (double)(r * (2 * n - 1)), (n - 1.) / (2 * n - 1.),
-                       s->dU, nullptr, 0)) != cudaSuccess) return e;
-        if ((e = stage(s, s->dS0, s->dU, OUT_AXPY, 0, (double)r, 0, nullptr, nullptr, 1)) != cudaSuccess) return e;
-        break;
-    }
-    default: { // SSPRK(10,4)
-        const double *in = s->dU;
-        double *bufs[2] = {s->dS0, s->dS1};
-        int k = 0;
-        for (int i = 0; i < 4; ++i) {
-            if ((e = stage(s, in, bufs[k], OUT_AXPY, 0, 6.0, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
-            in = bufs[k]; k ^= 1;
-        }
-        // fifth stage + w1 = u/25 + 9 w/25 (into S2) + w = 15 w1 - 5 w
-        if ((e = stage(s, in, bufs[k], OUT_RK104_5, 0, 6.0, 0, s->dU, s->dS2, 0)) != cudaSuccess) return e;
-        in = bufs[k]; k ^= 1;
-        for (int i = 5; i < 9; ++i) {
-            if ((e = stage(s, in, bufs[k], OUT_AXPY, 0, 6.0, 0, nullptr, nullptr, 0)) != cudaSuccess) return e;
-            in = bufs[k]; k ^= 1;
-        }
-        // VecAXPBYPCZ(w1, 3/5, dt/10, 1, w0, F); sol = w1
-        if ((e = stage(s, in, s->dU, OUT_ZSX, 3. / 5, 10.0, 1.0, s->dS2, nullptr, 1)) != cudaSuccess) return e;
-        break;
-    }
-    }
-    return launch_end_step(s->dSc, cfl_h, s->stream);
+    if (copy_back &&
+        (e = cudaMemcpyAsync(s->dU, s->dS0, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream)) != cudaSuccess)
+        return e;
+    return launch_end_step(s->dSc, s->cfl_h, s->stream);
+}
+
+static int check_config(const hype_config *c, hype_solver *s);
+int hype::validate_config(const hype_config *c, char *err, size_t errlen)
+{
+    hype_solver tmp;
+    const int rc = check_config(c, &tmp);
+    if (rc && err && errlen) snprintf(err, errlen, "%s", tmp.err);
+    return rc;
 }
 
 static int check_config(const hype_config *c, hype_solver *s)
@@ -451,7 +432,7 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     CUDA_TRY(s, cudaMallocHost(&s->hSc, sizeof(DevScalars)));
     if (cfg->bc_left == HYPE_BC_INLET) {
         std::vector<double> tab;
-        fill_inlet(s, tab);
+        inlet_table(*cfg, s->h, tab);
         CUDA_TRY(s, cudaMalloc(&s->dInlet, sizeof(double) * tab.size()));
         CUDA_TRY(s, cudaMemcpy(s->dInlet, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
     }

@@ -75,10 +75,11 @@ __global__ void seed_dt_kernel(DevScalars *sc, double cfl_h)
 
 // Start of a step: the monitor hands TS the last RHS's dt; TS stops at
 // max_steps or t_final and clips the last step to land on t_final (MATCHSTEP).
-__global__ void begin_step_kernel(DevScalars *sc)
+// A run whose RHS raised an error stops there (the reference aborts the job).
+__device__ __forceinline__ void begin_step(DevScalars *sc)
 {
     if (sc->done) return;
-    if (sc->steps >= sc->max_steps || sc->t >= sc->t_final) { sc->done = 1; return; }
+    if (sc->err || sc->steps >= sc->max_steps || sc->t >= sc->t_final) { sc->done = 1; return; }
     double dt = sc->time_step;
     if (sc->t + dt > sc->t_final) dt = sc->t_final - sc->t;
     sc->dt = dt;
@@ -86,13 +87,42 @@ __global__ void begin_step_kernel(DevScalars *sc)
 }
 
 // End of a step: the last stage's RHS set Ctx->dt for the next step.
-__global__ void end_step_kernel(DevScalars *sc, double cfl_h)
+__device__ __forceinline__ void end_step(DevScalars *sc, double cfl_h)
 {
     if (sc->done) return;
     const double smax = __longlong_as_double((long long)sc->smax);
     sc->time_step = cfl_h / (2.0 * smax);
     sc->t = sc->t + sc->dt;
     sc->steps = sc->steps + 1;
+}
+
+__global__ void begin_step_kernel(DevScalars *sc) { begin_step(sc); }
+__global__ void end_step_kernel(DevScalars *sc, double cfl_h) { end_step(sc, cfl_h); }
+
+__global__ void begin_step_batch_kernel(DevScalars *sc, const int *members)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < members[0]; k += gridDim.x * blockDim.x)
+        begin_step(&sc[members[1 + k]]);
+}
+__global__ void end_step_batch_kernel(DevScalars *sc, const int *members)
+{
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < members[0]; k += gridDim.x * blockDim.x) {
+        DevScalars *p = &sc[members[1 + k]];
+        end_step(p, p->cfl_h);
+    }
+}
+// one block per member; skipped for finished instances like the stages
+__global__ void copy_batch_kernel(double *const *dst, const double *const *src, const long long *n, const int *members,
+                                  const DevScalars *sc)
+{
+    for (int k = blockIdx.x; k < members[0]; k += gridDim.x) {
+        const int m = members[1 + k];
+        if (sc[m].done) continue;
+        const double2 *a = reinterpret_cast<const double2 *>(src[m]);
+        double2 *b = reinterpret_cast<double2 *>(dst[m]);
+        for (long long i = threadIdx.x; i < n[m] / 2; i += blockDim.x) b[i] = a[i];
+        if ((n[m] & 1) && threadIdx.x == 0) dst[m][n[m] - 1] = src[m][n[m] - 1];
+    }
 }
 
 cudaError_t launch_seed_dt(DevScalars *sc, double cfl_h, cudaStream_t s)
@@ -109,6 +139,69 @@ cudaError_t launch_end_step(DevScalars *sc, double cfl_h, cudaStream_t s)
 {
     end_step_kernel<<<1, 1, 0, s>>>(sc, cfl_h);
     return cudaGetLastError();
+}
+static unsigned member_blocks(int max_members, int per_block) { return (unsigned)((max_members + per_block - 1) / per_block > 0 ? (max_members + per_block - 1) / per_block : 1); }
+cudaError_t launch_begin_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s)
+{
+    begin_step_batch_kernel<<<member_blocks(max_members, 128), 128, 0, s>>>(sc, members);
+    return cudaGetLastError();
+}
+cudaError_t launch_end_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s)
+{
+    end_step_batch_kernel<<<member_blocks(max_members, 128), 128, 0, s>>>(sc, members);
+    return cudaGetLastError();
+}
+cudaError_t launch_copy_batch(double *const *dst, const double *const *src, const long long *n, const int *members,
+                              int max_members, const DevScalars *sc, cudaStream_t s)
+{
+    copy_batch_kernel<<<member_blocks(max_members, 1), 512, 0, s>>>(dst, src, n, members, sc);
+    return cudaGetLastError();
+}
+
+// The SSP schemes of hype.c:362-382 as stage lists.  PETSc's TSSSP writes
+// each stage as VecAXPY(w, dt/kb, F) or VecAXPBYPCZ; the coefficients below
+// are computed with the expressions of its step functions so that they round
+// identically.
+int ssp_plan(int order, PlanStage *st, int *copy_back)
+{
+    auto S = [&](int k, int in, int out, int mode, double ka, double kb, double kc, int x, int out2, int reduce) {
+        st[k] = PlanStage{in, out, mode, ka, kb, kc, x, out2, reduce};
+    };
+    *copy_back = 0;
+    switch (order) {
+    case 0:   // TSEULER: S0 = u + dt F(u); u = S0
+        S(0, B_U, B_S0, OUT_AXPY, 0, 1.0, 0, B_NONE, B_NONE, 1);
+        *copy_back = 1;
+        return 1;
+    case 1: { // SSPRKS2, s = 2: w = u + (dt/(s-1)) F(u); u = ((s-1)/s) w + (dt/s) F(w) + (1/s) u
+        const int ns = 2;
+        S(0, B_U, B_S0, OUT_AXPY, 0, (ns - 1.), 0, B_NONE, B_NONE, 0);
+        S(1, B_S0, B_U, OUT_ZSX, (ns - 1.) / ns, (double)ns, 1. / ns, B_U, B_NONE, 1);
+        return 2;
+    }
+    case 2: { // SSPRKS3, s = 4, n = 2, r = 2
+        const int n = 2, ns = 4, r = ns - n;
+        S(0, B_U, B_S0, OUT_AXPY, 0, (double)r, 0, B_NONE, B_NONE, 0);
+        S(1, B_S0, B_S1, OUT_AXPY, 0, (double)r, 0, B_NONE, B_NONE, 0);
+        // VecAXPBYPCZ(w0, n/(2n-1), (n-1) dt/(r(2n-1)), (n-1)/(2n-1), w1 = u^n, F)
+        S(2, B_S1, B_S0, OUT_ZXS, 1. * n / (2 * n - 1.), (double)(r * (2 * n - 1)), (n - 1.) / (2 * n - 1.), B_U, B_NONE, 0);
+        S(3, B_S0, B_U, OUT_AXPY, 0, (double)r, 0, B_NONE, B_NONE, 1);
+        return 4;
+    }
+    case 3: { // SSPRK(10,4)
+        int in = B_U, k = 0, ns = 0;
+        const int bufs[2] = {B_S0, B_S1};
+        for (int i = 0; i < 4; ++i) { S(ns++, in, bufs[k], OUT_AXPY, 0, 6.0, 0, B_NONE, B_NONE, 0); in = bufs[k]; k ^= 1; }
+        // fifth stage + w1 = u/25 + 9 w/25 (into S2) + w = 15 w1 - 5 w
+        S(ns++, in, bufs[k], OUT_RK104_5, 0, 6.0, 0, B_U, B_S2, 0); in = bufs[k]; k ^= 1;
+        for (int i = 5; i < 9; ++i) { S(ns++, in, bufs[k], OUT_AXPY, 0, 6.0, 0, B_NONE, B_NONE, 0); in = bufs[k]; k ^= 1; }
+        // VecAXPBYPCZ(w1, 3/5, dt/10, 1, w0, F); sol = w1
+        S(ns++, in, B_U, OUT_ZSX, 3. / 5, 10.0, 1.0, B_S2, B_NONE, 1);
+        return ns;
+    }
+    default:
+        return 0;
+    }
 }
 
 // Conservation totals: per-block partial sums over whole rows (FP64, fixed

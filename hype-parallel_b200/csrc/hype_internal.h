@@ -1,10 +1,13 @@
 // hype_internal.h -- host/device interface between the C ABI (hype_api.cu) and
 // the kernels (hype_stage.cu, hype_aux.cu).  Not installed; not part of the ABI.
 #pragma once
+#include <cstddef>
 #include <cstdint>
+#include <vector>
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include "hype_physics.cuh"
+#include "../../include/hype_gpu.h"
 
 namespace hype {
 
@@ -30,6 +33,7 @@ struct DevScalars {
     int steps, max_steps;
     int done;                  // set when the run reached t_final or max_steps
     int pad_;
+    double cfl_h;              // CFL*h of the instance (read by the batched step control)
 };
 
 struct StageParams {
@@ -63,13 +67,29 @@ size_t stage_smem_bytes(int sys, int order, int cells);
 int stage_threads(int cells);
 cudaError_t stage_configure(int sys, int order, int cells);   // raises the dynamic smem limit
 int stage_blocks_per_sm(int sys, int order, int cells);
+int stage_batch_blocks_per_sm(int sys, int order, int cells);   // resident blocks of the persistent form
 cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
-                               const int2 *work, int nwork, int blocks, cudaStream_t s);
+                               const int2 *work, int *sched, int blocks, cudaStream_t s);
 // Strips of a grid: with S = ceil(nx/(cells-4)) strips and even origins
 // 2*floor(s*nx/(2S)), every strip has at most 2*ceil(nx/(2S)) <= cells-4
 // columns and the last one at most nx/S + 2 <= cells-2.
 inline int stage_strips(int nx, int cells) { return (nx + (cells - 4) - 1) / (cells - 4); }
+
+// One stage of an SSP-RK step over a solver's state buffers (B_U = u^n, B_S0..B_S2
+// work vectors; B_NONE = unused): in -> out with OUT_* `mode` and coefficients
+// ka, kb, kc; x = second state, out2 = second output; reduce = fold the max
+// wave speed into DevScalars.smax (the stage whose RHS sets the next dt).
+enum : int { B_NONE = -1, B_U = 0, B_S0 = 1, B_S1 = 2, B_S2 = 3 };
+struct PlanStage {
+    int in, out, mode;
+    double ka, kb, kc;
+    int x, out2, reduce;
+};
+constexpr int MAX_PLAN = 10;
+// Stages of one step of the SSP scheme of `order` (hype.c:362-382; PETSc TSSSP
+// forms); *copy_back is set when the step ends with u^n = S0 (forward Euler).
+int ssp_plan(int order, PlanStage *plan, int *copy_back);
 
 // hype_aux.cu
 cudaError_t launch_aos_to_planes(const double *aos, double *planes, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s);
@@ -77,6 +97,13 @@ cudaError_t launch_planes_to_aos(const double *planes, double *aos, int nx, int 
 cudaError_t launch_begin_step(DevScalars *sc, cudaStream_t s);
 cudaError_t launch_end_step(DevScalars *sc, double cfl_h, cudaStream_t s);
 cudaError_t launch_seed_dt(DevScalars *sc, double cfl_h, cudaStream_t s);
+// Batched step control over a member list: members[0] = count, members[1..] =
+// instance indices into sc[]; each instance uses its own sc[k].cfl_h.
+cudaError_t launch_begin_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s);
+cudaError_t launch_end_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s);
+// u^n = S0 for every member (forward Euler), one pointer pair per instance
+cudaError_t launch_copy_batch(double *const *dst, const double *const *src, const long long *n, const int *members,
+                              int max_members, const DevScalars *sc, cudaStream_t s);
 // writes nv sums then min/max of field acomp (acomp < 0: zeros) to red[0..nv+1];
 // red must hold 64 + (512 + 1) * (nv + 2) doubles
 cudaError_t launch_totals(const double *planes, double *red, int nx, int ny, int nv, int pitch, long long plane, int acomp,
@@ -117,11 +144,18 @@ inline int mixed_strips(int nx, int cells) { return (nx + (cells - 6) - 1) / (ce
 size_t mixed_smem_bytes(int cells);
 int mixed_threads(int cells);
 int mixed_blocks_per_sm(int cells);
+int mixed_batch_blocks_per_sm(int cells);
 cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s);
-cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int nwork,
+cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
                                int blocks, cudaStream_t s);
 // layout changes between the interleaved FP64 Vec and the mixed planes
 cudaError_t launch_aos_to_mixed(const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane, cudaStream_t s);
 cudaError_t launch_mixed_to_aos(const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane, cudaStream_t s);
+
+// hype_api.cu, shared with the batch (hype_batch.cu)
+CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, int ny, int nplanes, int pitch, long long plane,
+                           int box_w);
+int validate_config(const hype_config *c, char *err, size_t errlen);
+void inlet_table(const hype_config &c, double h, std::vector<double> &tab);
 
 }  // namespace hype

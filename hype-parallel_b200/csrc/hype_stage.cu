@@ -573,15 +573,23 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 template <int SYS, int N, int CELLS>
 __global__ void __launch_bounds__(2 * CELLS, (StageKernel<SYS, N, CELLS>::MIN_BLOCKS))
 stage_batch_kernel(const StageParams *__restrict__ inst, const CUtensorMap *__restrict__ tmaps,
-                   const int2 *__restrict__ work, int nwork)
+                   const int2 *__restrict__ work, int *__restrict__ sched)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    __shared__ int item_s;
+    const int nwork = sched[0];
+    const DevScalars *last = nullptr;
+    for (;;) {
+        const int w = work_take(sched, nwork, last, &item_s);
+        if (w >= nwork) break;
         const int2 it = work[w];
         const StageParams &p = inst[it.x];
+        if (threadIdx.x == 0) fence_tensormap_acquire(&tmaps[it.x]);
         stage_tile<SYS, N, CELLS>(p, &tmaps[it.x], it.y % p.strips, it.y / p.strips, smem_raw, red_s);
+        last = p.sc;
     }
+    work_finish(sched);
 }
 
 // ---------------------------------------------------------------------------
@@ -648,6 +656,15 @@ int stage_blocks_per_sm(int sys, int order, int cells)
     return nb;
 }
 
+int stage_batch_blocks_per_sm(int sys, int order, int cells)
+{
+    const StageEntry e = stage_entry(sys, order, cells);
+    int nb = 0;
+    if (stage_configure(sys, order, cells) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, e.batch, e.threads, e.smem) != cudaSuccess) return 0;
+    return nb;
+}
+
 cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s)
 {
     const StageEntry e = stage_entry(sys, order, cells);
@@ -658,10 +675,10 @@ cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap,
 }
 
 cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
-                               const int2 *work, int nwork, int blocks, cudaStream_t s)
+                               const int2 *work, int *sched, int blocks, cudaStream_t s)
 {
     const StageEntry e = stage_entry(sys, order, cells);
-    void *args[] = {&inst, &tmaps, &work, &nwork};
+    void *args[] = {&inst, &tmaps, &work, &sched};
     return cudaLaunchKernel(e.batch, dim3((unsigned)blocks, 1, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 

@@ -592,15 +592,26 @@ mixed_kernel(const __grid_constant__ MixedMaps maps, const MixedParams p)
 template <int CELLS>
 __global__ void __launch_bounds__(2 * CELLS, (MixedKernel<CELLS>::MIN_BLOCKS))
 mixed_batch_kernel(const MixedParams *__restrict__ inst, const MixedMaps *__restrict__ maps, const int2 *__restrict__ work,
-                   int nwork)
+                   int *__restrict__ sched)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    __shared__ int item_s;
+    const int nwork = sched[0];
+    const DevScalars *last = nullptr;
+    for (;;) {
+        const int w = work_take(sched, nwork, last, &item_s);
+        if (w >= nwork) break;
         const int2 it = work[w];
         const MixedParams &p = inst[it.x];
+        if (threadIdx.x == 0) {
+            fence_tensormap_acquire(&maps[it.x].f);
+            fence_tensormap_acquire(&maps[it.x].d);
+        }
         mixed_tile<CELLS>(p, &maps[it.x], it.y % p.strips, it.y / p.strips, smem_raw, red_s);
+        last = p.sc;
     }
+    work_finish(sched);
 }
 
 struct MixedEntry {
@@ -636,6 +647,15 @@ int mixed_blocks_per_sm(int cells)
     return nb;
 }
 
+int mixed_batch_blocks_per_sm(int cells)
+{
+    const MixedEntry e = mixed_entry(cells);
+    int nb = 0;
+    if (mixed_configure(cells) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, e.batch, e.threads, e.smem) != cudaSuccess) return 0;
+    return nb;
+}
+
 cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s)
 {
     const MixedEntry e = mixed_entry(cells);
@@ -645,11 +665,11 @@ cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p,
     return cudaLaunchKernel(e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
-cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int nwork,
+cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
                                int blocks, cudaStream_t s)
 {
     const MixedEntry e = mixed_entry(cells);
-    void *args[] = {&inst, &maps, &work, &nwork};
+    void *args[] = {&inst, &maps, &work, &sched};
     return cudaLaunchKernel(e.batch, dim3((unsigned)blocks, 1, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 

@@ -66,4 +66,39 @@ __device__ __forceinline__ void raise_error(DevScalars *sc, unsigned bits, unsig
     atomicMin(&sc->err_cell, cell);
 }
 
+// A tensor map in global memory written by the host (or an earlier kernel)
+// between launches: order those writes before the TMA unit reads it.
+__device__ __forceinline__ void fence_tensormap_acquire(const void *map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+// Work distribution of the persistent (batched) kernels over a list of
+// (instance, tile) items: sched[0] = item count, sched[1] = next item,
+// sched[2] = blocks finished.  Blocks take items in list order (the host sorts
+// it longest first); the last block to finish zeroes sched[1] and sched[2], so
+// back-to-back launches (graph replays) need no reset in between.  A block
+// stops taking items once the instance of its last tile saw a TMA timeout.
+__device__ __forceinline__ int work_take(int *sched, int nwork, const DevScalars *last_sc, int *item_s)
+{
+    if (threadIdx.x == 0) {
+        const bool stop = last_sc && (*(volatile const unsigned *)&last_sc->err & ERR_TMA_TIMEOUT);
+        *item_s = stop ? nwork : atomicAdd(&sched[1], 1);
+    }
+    __syncthreads();
+    const int w = *item_s;
+    __syncthreads();
+    return w;
+}
+__device__ __forceinline__ void work_finish(int *sched)
+{
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&sched[2], 1) == (int)gridDim.x - 1) {
+            atomicExch(&sched[1], 0);
+            atomicExch(&sched[2], 0);
+        }
+    }
+}
+
 }  // namespace hype
