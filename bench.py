@@ -184,12 +184,12 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 def batch_leg(hp, args, local_rank):
     """Batched form: 64 independent Kapila shock-bubble grids of seeded uneven
-    sizes (nx, ny in 128..1024) stepped together -- one persistent launch per RK
+    sizes (nx, ny drawn from {128, 192, ..., 1024}) stepped together -- one persistent launch per RK
     stage over a (grid, tile) work-list, each step one CUDA graph, tile shape
     from the batch autotuner -- in FP64 and in mixed precision, against the
     plain FP64 path (one solver per grid, run one after another)."""
     rng = np.random.default_rng(2024)
-    sizes = [(int(a), int(b)) for a, b in rng.integers(128, 1025, size=(64, 2))]
+    sizes = [(64 * int(a), 64 * int(b)) for a, b in rng.integers(2, 17, size=(64, 2))]   # sides in {128, 192, ..., 1024}
     nb = [int(k) for k in rng.integers(1, 5, size=64)]
     cells = sum(a * b for a, b in sizes)
     steps = args.batch_steps
@@ -233,12 +233,68 @@ def batch_leg(hp, args, local_rank):
         return float(np.abs(a - b).sum() / np.abs(b).sum())
     err_rho = max(rel_l1(M[:, 0] + M[:, 1], F[:, 0] + F[:, 1]) for M, F in zip(finals["mixed"], finals["fp64"]))
     err_a = max(rel_l1(M[:, 5], F[:, 5]) for M, F in zip(finals["mixed"], finals["fp64"]))
-    return {"workload": "64 kapila5 shock-bubble grids, nx,ny seeded uniform in 128..1024, N=2 SSPRK(4,3)",
+    return {"workload": "64 kapila5 shock-bubble grids, nx,ny seeded uniform in {128,192,...,1024}, N=2 SSPRK(4,3)",
             "cells_total": cells, "plain_fp64": {"value": plain, "unit": UNIT, "steps_each": plain_steps},
             "batched_fp64": out["fp64"], "batched_mixed": out["mixed"],
             "speedup_batched_mixed_vs_plain": out["mixed"]["value"] / plain,
             "speedup_batched_fp64_vs_plain": out["fp64"]["value"] / plain,
             "mixed_vs_fp64_max_rel_L1": {"rho": err_rho, "alpha1": err_a}}
+
+
+def serve_leg(hp, args, local_rank, capacity):
+    """Serving: a Poisson stream of solve requests through the C request loop
+    (hype_serve_run) -- 70/20/10 Kapila / Baer-Nunziato / Euler, square grids
+    with side log-uniform in 64..2048, runs of 50..2000 steps (log-uniform),
+    150 GB HBM budget, continuous batching.  The arrival rate is seed-drawn as
+    a load factor rho ~ U[0.5, 0.8] of the batched throughput measured above."""
+    rng = np.random.default_rng(7)
+    n = args.serve_requests
+    T = hp.BC_TRANSMISSIVE
+    kap_prec = hp.PREC_MIXED if args.serve_kapila == "mixed" else hp.PREC_FP64
+    reqs, work = [], []
+    for i in range(n):
+        u = rng.uniform()
+        side = int(round(64 * 32 ** rng.uniform()))
+        steps = int(round(50 * 40 ** rng.uniform()))
+        if u < 0.7:
+            cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=side, ny=side, cfl=0.4, device=local_rank, precision=kap_prec)
+            ic, par = hp.IC_SHOCK_BUBBLE, int(rng.integers(1, 5))
+        elif u < 0.9:
+            # phase-2 flux pressure from V[7]; the reference's V[8] (baer_nunziato.c:271) aborts these runs early
+            cfg = hp.Config(system=hp.BAER_NUNZIATO, order=2, nx=side, ny=side, cfl=0.4, device=local_rank,
+                            flags=hp.FLAG_BN_FIX_P2)
+            ic, par = hp.IC_BN_DISCS, 0
+        else:
+            cfg = hp.Config(system=hp.EULER, order=2, nx=side, ny=side, cfl=0.4, device=local_rank, gamma1=1.4, gamma2=1.4,
+                            pi1=0.0, pi2=0.0)
+            ic, par = hp.IC_EULER_QUADRANTS, 0
+        reqs.append(hp.Request(0.0, cfg, 0.0, 1e30, steps, ic, 5000 + i, par))
+        work.append(side * side * steps)
+    rho = float(rng.uniform(0.5, 0.8))
+    rate = rho * capacity / float(np.mean(work))
+    t = 0.0
+    for r in reqs:
+        r.arrival_s = t
+        t += float(rng.exponential(1.0 / rate))
+    res, st = hp.serve(reqs, device=local_rank, hbm_budget=150 * 10 ** 9, max_instances=1024, max_cells=2048 * 2048,
+                       poll_ms=args.serve_poll_ms, realtime=True)
+    lat = np.array([r["latency_s"] for r in res])
+    by_sys = {}
+    for nm, sysid in (("kapila", hp.KAPILA_5EQN), ("bn", hp.BAER_NUNZIATO), ("euler", hp.EULER)):
+        sel = np.array([r.cfg.system == sysid for r in reqs])
+        if sel.any():
+            by_sys[nm] = {"n": int(sel.sum()), "p50_s": float(np.percentile(lat[sel], 50)),
+                          "p99_s": float(np.percentile(lat[sel], 99))}
+    return {"workload": f"Poisson stream of {n} solves: 70/20/10 kapila5/bn/euler, square grids 64..2048 log-uniform, "
+                        "50..2000 steps log-uniform, N=2 SSPRK(4,3), 150 GB HBM budget",
+            "requests": n, "kapila_precision": args.serve_kapila, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
+            "offered_cell_updates": float(np.sum(work)),
+            "p50_s": st["p50_s"], "p90_s": st["p90_s"], "p99_s": st["p99_s"], "max_s": st["max_s"], "mean_s": st["mean_s"],
+            "queue_p50_s": st["queue_p50_s"], "queue_p99_s": st["queue_p99_s"],
+            "value": st["cell_updates_per_s"], "unit": UNIT, "wall_s": st["wall_s"],
+            "completed": st["completed"], "failed": st["failed"], "peak_instances": st["peak_instances"],
+            "peak_bytes": st["peak_bytes"], "polls": st["polls"], "batch_steps": st["steps_replayed"],
+            "by_system": by_sys}
 
 
 def run_gpu(args, rank, world, local_rank):
@@ -354,6 +410,8 @@ def run_gpu(args, rank, world, local_rank):
                  "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt"}
 
     batched = None if args.no_batch else batch_leg(hp, args, local_rank)
+    capacity = batched["batched_mixed"]["value"] if batched else 5e8
+    serving = None if args.serve_requests <= 0 else serve_leg(hp, args, local_rank, capacity)
 
     if rank != 0:
         return 0
@@ -374,7 +432,7 @@ def run_gpu(args, rank, world, local_rank):
             "gpu_launches": args.steps * 6,
             "clocks": clk.summary(),
             "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2},
-            "forms": {"mixed": mixed, "batched": batched}}
+            "forms": {"mixed": mixed, "batched": batched, "serving": serving}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -391,6 +449,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-grids leg")
     ap.add_argument("--batch-steps", type=int, default=300, help="steps of the batched-grids leg")
+    ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip)")
+    ap.add_argument("--serve-kapila", default="mixed", choices=["mixed", "fp64"], help="precision of Kapila requests")
+    ap.add_argument("--serve-poll-ms", type=float, default=10.0)
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -90,6 +90,36 @@ class _InstStatus(ctypes.Structure):
                 ("t", ctypes.c_double), ("dt_next", ctypes.c_double)]
 
 
+class _Request(ctypes.Structure):
+    _fields_ = [("arrival_s", ctypes.c_double), ("cfg", _Cfg), ("t0", ctypes.c_double), ("t_final", ctypes.c_double),
+                ("max_steps", ctypes.c_int), ("ic", ctypes.c_int), ("ic_seed", ctypes.c_uint64), ("ic_param", ctypes.c_int)]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("steps", ctypes.c_int), ("t_end", ctypes.c_double), ("admit_s", ctypes.c_double),
+                ("done_s", ctypes.c_double), ("latency_s", ctypes.c_double)]
+
+
+class _ServeCfg(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("max_instances", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
+                ("max_cells", ctypes.c_longlong), ("poll_ms", ctypes.c_double), ("realtime", ctypes.c_int),
+                ("autotune", ctypes.c_int), ("fetch_results", ctypes.c_int)]
+
+
+class _ServeStats(ctypes.Structure):
+    _fields_ = [("completed", ctypes.c_int), ("failed", ctypes.c_int), ("wall_s", ctypes.c_double),
+                ("p50_s", ctypes.c_double), ("p90_s", ctypes.c_double), ("p99_s", ctypes.c_double),
+                ("max_s", ctypes.c_double), ("mean_s", ctypes.c_double), ("queue_p50_s", ctypes.c_double),
+                ("queue_p99_s", ctypes.c_double), ("cell_updates", ctypes.c_double),
+                ("cell_updates_per_s", ctypes.c_double), ("peak_instances", ctypes.c_int),
+                ("peak_bytes", ctypes.c_size_t), ("polls", ctypes.c_longlong), ("steps_replayed", ctypes.c_longlong)]
+
+
+_FILL_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_Request),
+                            ctypes.POINTER(ctypes.c_double))
+_SINK_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_double),
+                            ctypes.POINTER(_Result))
+
 _DP = ctypes.POINTER(ctypes.c_double)
 _lib = None
 
@@ -148,8 +178,12 @@ def lib() -> ctypes.CDLL:
         L.hype_batch_get_state.argtypes = [vp, ctypes.c_int, _DP]
         L.hype_batch_set_tiling.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.hype_batch_autotune.argtypes = [vp, ctypes.c_int, IP, IP]
-        L.hype_batch_info.argtypes = [vp, IP, IP, ctypes.POINTER(ctypes.c_size_t)]
+        L.hype_batch_info.argtypes = [vp, IP, IP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
         L.hype_batch_last_elapsed_ms.argtypes = [vp, _DP]
+        # include/hype_serve.h
+        L.hype_serve_config_default.argtypes = [ctypes.POINTER(_ServeCfg)]
+        L.hype_serve_run.argtypes = [ctypes.POINTER(_ServeCfg), ctypes.POINTER(_Request), ctypes.c_int, _FILL_FN, _SINK_FN,
+                                     vp, ctypes.POINTER(_Result), ctypes.POINTER(_ServeStats)]
         _lib = L
     return _lib
 
@@ -403,11 +437,72 @@ class Batch:
 
     def info(self) -> dict:
         n, w = ctypes.c_int(0), ctypes.c_int(0)
-        b = ctypes.c_size_t(0)
-        self._check(lib().hype_batch_info(self._h, ctypes.byref(n), ctypes.byref(w), ctypes.byref(b)))
-        return {"instances": n.value, "work_items": w.value, "bytes_in_use": b.value}
+        b, g = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        self._check(lib().hype_batch_info(self._h, ctypes.byref(n), ctypes.byref(w), ctypes.byref(b), ctypes.byref(g)))
+        return {"instances": n.value, "work_items": w.value, "bytes_in_use": b.value, "budget": g.value}
 
     def last_elapsed_ms(self) -> float:
         ms = ctypes.c_double(0.0)
         self._check(lib().hype_batch_last_elapsed_ms(self._h, ctypes.byref(ms)))
         return ms.value
+
+
+# include/hype_serve.h
+IC_CALLBACK, IC_SHOCK_BUBBLE, IC_BN_DISCS, IC_EULER_QUADRANTS, IC_SMOOTH_VORTEX = range(5)
+
+
+@dataclasses.dataclass
+class Request:
+    """One solve: configuration, time interval and step limit, initial state
+    (a built-in seeded generator, or IC_CALLBACK with ``fill``)."""
+    arrival_s: float
+    cfg: Config
+    t0: float = 0.0
+    t_final: float = 1e30
+    max_steps: int = 100
+    ic: int = IC_SHOCK_BUBBLE
+    ic_seed: int = 0
+    ic_param: int = 1
+
+
+def serve(requests, *, device: int = 0, max_instances: int = 256, hbm_budget: int = 0, max_cells: int = 2048 * 2048,
+          poll_ms: float = 10.0, realtime: bool = True, autotune: bool = True, fetch_results: bool = True,
+          fill=None, sink=None):
+    """Runs hype_serve_run over ``requests`` (sorted by arrival).
+
+    fill(index, U0) fills the initial state of IC_CALLBACK requests in place;
+    sink(index, U, result) receives each final state (a copy).  Returns
+    (results, stats) as lists/dicts of the C structures' fields.
+    """
+    L = lib()
+    n = len(requests)
+    arr = (_Request * max(n, 1))()
+    for i, r in enumerate(requests):
+        arr[i] = _Request(r.arrival_s, r.cfg.c_struct(), r.t0, r.t_final, r.max_steps, r.ic, r.ic_seed, r.ic_param)
+    res = (_Result * max(n, 1))()
+    st = _ServeStats()
+    c = _ServeCfg()
+    L.hype_serve_config_default(ctypes.byref(c))
+    c.device, c.max_instances, c.hbm_budget, c.max_cells = device, max_instances, hbm_budget, max_cells
+    c.poll_ms, c.realtime, c.autotune, c.fetch_results = poll_ms, int(realtime), int(autotune), int(fetch_results)
+
+    def _fill(_ctx, i, _req, U):
+        try:
+            cfg = requests[i].cfg
+            fill(i, np.ctypeslib.as_array(U, shape=(cfg.nx * cfg.ny * cfg.nvar,)))
+            return 0
+        except Exception:
+            return 1
+
+    def _sink(_ctx, i, _req, U, rp):
+        cfg = requests[i].cfg
+        out = np.ctypeslib.as_array(U, shape=(cfg.nx * cfg.ny * cfg.nvar,)).copy()
+        sink(i, out, {f: getattr(rp.contents, f) for f, _ in _Result._fields_})
+
+    fcb = _FILL_FN(_fill) if fill is not None else _FILL_FN()
+    scb = _SINK_FN(_sink) if sink is not None else _SINK_FN()
+    rc = L.hype_serve_run(ctypes.byref(c), arr, n, fcb, scb, None, res, ctypes.byref(st))
+    if rc != OK:
+        raise HypeError(rc, f"hype_serve_run: {L.hype_status_string(rc).decode()}")
+    results = [{f: getattr(res[i], f) for f, _ in _Result._fields_} for i in range(n)]
+    return results, {f: getattr(st, f) for f, _ in _ServeStats._fields_}

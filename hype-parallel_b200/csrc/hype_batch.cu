@@ -758,7 +758,7 @@ int hype_batch_autotune(hype_batch *b, int reps, int *cells_out, int *rows_out)
     return HYPE_OK;
 }
 
-int hype_batch_info(const hype_batch *b, int *instances, int *work_items, size_t *bytes_in_use)
+int hype_batch_info(const hype_batch *b, int *instances, int *work_items, size_t *bytes_in_use, size_t *budget)
 {
     if (!b) return HYPE_ERR_INVALID;
     int n = 0, w = 0;
@@ -767,6 +767,7 @@ int hype_batch_info(const hype_batch *b, int *instances, int *work_items, size_t
     if (instances) *instances = n;
     if (work_items) *work_items = w;
     if (bytes_in_use) *bytes_in_use = b->in_use;
+    if (budget) *budget = b->budget;
     return HYPE_OK;
 }
 

@@ -1,0 +1,267 @@
+/*
+ * hype_serve.c -- the request loop of include/hype_serve.h, in C over the
+ * batch ABI (include/hype_batch.h).
+ *
+ * One iteration of the loop:
+ *   1. admit, in arrival order, every request that has arrived while the
+ *      batch has a free slot and HBM budget for it (its initial state is
+ *      built on the host, uploaded, and its dt seeded by one RHS evaluation);
+ *      a request that does not fit waits at the head of the queue until
+ *      finished instances free their memory;
+ *   2. enqueue k steps of the whole batch (k graph replays, k sized so that
+ *      they take about poll_ms of GPU time); while they run, build the
+ *      initial state of the next waiting request on the host; then wait;
+ *   3. retire every instance whose time loop ended: copy its state out, hand
+ *      it to the sink, free its slot and memory.
+ * Instances stop on the device at their own t_final / max_steps, so the k
+ * steps of step 2 never overrun a request.
+ */
+#define _POSIX_C_SOURCE 200809L
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <cuda_runtime_api.h>
+#include "../../include/hype_batch.h"
+#include "../../include/hype_ic.h"
+#include "../../include/hype_serve.h"
+
+static double now_s(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+static void sleep_s(double s)
+{
+    if (s <= 0.0) return;
+    struct timespec ts;
+    ts.tv_sec = (time_t)s;
+    ts.tv_nsec = (long)((s - (double)ts.tv_sec) * 1e9);
+    nanosleep(&ts, NULL);
+}
+
+static int cmp_double(const void *a, const void *b)
+{
+    const double x = *(const double *)a, y = *(const double *)b;
+    return (x > y) - (x < y);
+}
+
+/* nearest-rank percentile of sorted v[0..n-1] */
+static double pct(const double *v, int n, double p)
+{
+    if (n <= 0) return 0.0;
+    int k = (int)ceil(p / 100.0 * (double)n) - 1;
+    if (k < 0) k = 0;
+    if (k >= n) k = n - 1;
+    return v[k];
+}
+
+void hype_serve_config_default(hype_serve_config *c)
+{
+    if (!c) return;
+    memset(c, 0, sizeof(*c));
+    c->device = 0;
+    c->max_instances = 256;
+    c->hbm_budget = 0;
+    c->max_cells = 2048LL * 2048LL;
+    c->poll_ms = 10.0;
+    c->realtime = 1;
+    c->autotune = 1;
+    c->fetch_results = 1;
+}
+
+static int make_initial(const hype_request *r, int index, hype_fill_fn fill, void *ctx, double *U)
+{
+    switch (r->ic) {
+    case HYPE_IC_CALLBACK: return fill ? (fill(ctx, index, r, U) == 0 ? HYPE_OK : HYPE_ERR_INVALID) : HYPE_ERR_INVALID;
+    case HYPE_IC_SHOCK_BUBBLE: return hype_ic_shock_bubble(&r->cfg, r->ic_seed, r->ic_param, U);
+    case HYPE_IC_BN_DISCS: return hype_ic_bn_discs(&r->cfg, r->ic_seed, U);
+    case HYPE_IC_EULER_QUADRANTS: return hype_ic_euler_quadrants(&r->cfg, r->ic_seed, U);
+    case HYPE_IC_SMOOTH_VORTEX: return hype_ic_smooth_vortex(&r->cfg, U);
+    default: return HYPE_ERR_INVALID;
+    }
+}
+
+int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, hype_fill_fn fill, hype_sink_fn sink,
+                   void *ctx, hype_request_result *res, hype_serve_stats *stats)
+{
+    if (!c || (n > 0 && (!req || !res)) || n < 0 || !stats) return HYPE_ERR_INVALID;
+    if (c->max_instances < 1 || c->max_cells < 9 || !(c->poll_ms > 0.0)) return HYPE_ERR_INVALID;
+    for (int i = 1; i < n; ++i)
+        if (req[i].arrival_s < req[i - 1].arrival_s) return HYPE_ERR_INVALID;
+    memset(stats, 0, sizeof(*stats));
+    memset(res, 0, sizeof(*res) * (size_t)n);
+
+    hype_batch_config bc;
+    hype_batch_config_default(&bc);
+    bc.device = c->device;
+    bc.max_instances = c->max_instances;
+    bc.hbm_budget = c->hbm_budget;
+    bc.max_cells = c->max_cells;
+    hype_batch *b = NULL;
+    int rc = hype_batch_create(&bc, &b);
+    if (rc) { hype_batch_destroy(b); return rc; }
+
+    const int M = c->max_instances;
+    size_t budget = 0;
+    hype_batch_info(b, NULL, NULL, NULL, &budget);
+    int *req_of = (int *)malloc(sizeof(int) * (size_t)M);
+    /* pinned host staging: initial states in, final states out */
+    double *host = NULL, *host_out = NULL;
+    const size_t hbytes = sizeof(double) * 9 * (size_t)c->max_cells;
+    if (!req_of || cudaMallocHost((void **)&host, hbytes) != cudaSuccess || cudaMallocHost((void **)&host_out, hbytes) != cudaSuccess) {
+        free(req_of);
+        if (host) cudaFreeHost(host);
+        if (host_out) cudaFreeHost(host_out);
+        hype_batch_destroy(b);
+        return HYPE_ERR_NOMEM;
+    }
+    for (int s = 0; s < M; ++s) req_of[s] = -1;
+
+    int next = 0, finished = 0, running = 0, staged = -1;
+    int steps_per_poll = 1, tuned_at = 0;
+    double ms_per_step = -1.0;
+    const double t_start = now_s();
+    rc = HYPE_OK;
+
+    while (finished < n) {
+        double t = now_s() - t_start;
+        /* 1. admission, in arrival order */
+        int admitted = 0;
+        while (next < n && (!c->realtime || req[next].arrival_s <= t)) {
+            const hype_request *r = &req[next];
+            hype_request_result *o = &res[next];
+            const size_t need = hype_batch_instance_bytes(&r->cfg);
+            const long long cells = (long long)r->cfg.nx * r->cfg.ny;
+            if (need == 0 || cells > c->max_cells) {
+                o->status = HYPE_ERR_INVALID;
+            } else if (need > budget) {
+                o->status = HYPE_ERR_NOMEM;   /* can never be admitted */
+            } else {
+                int st = HYPE_OK;
+                if (staged != next) {   /* build the initial state once, even if admission waits */
+                    st = make_initial(r, next, fill, ctx, host);
+                    if (st == HYPE_OK) staged = next;
+                }
+                int id = -1;
+                if (st == HYPE_OK) st = hype_batch_add(b, &r->cfg, host, r->t0, r->t_final, r->max_steps, &id);
+                if (st == HYPE_ERR_NOMEM || st == HYPE_ERR_BUSY) {
+                    if (running > 0) break;   /* wait for retirements */
+                    st = HYPE_ERR_NOMEM;      /* nothing to wait for: it can never fit */
+                }
+                if (st == HYPE_OK) {
+                    req_of[id] = next;
+                    o->admit_s = now_s() - t_start;
+                    ++running;
+                    ++admitted;
+                    ++next;
+                    t = now_s() - t_start;
+                    continue;
+                }
+                o->status = st;
+            }
+            /* rejected request: finished with an error */
+            o->admit_s = o->done_s = now_s() - t_start;
+            o->latency_s = o->done_s - (c->realtime ? r->arrival_s : 0.0);
+            ++finished;
+            ++next;
+        }
+        if (running == 0) {
+            if (next < n && c->realtime) sleep_s(req[next].arrival_s - (now_s() - t_start));
+            continue;
+        }
+        if (admitted) {
+            int ninst = 0, nwork = 0;
+            size_t bytes = 0;
+            hype_batch_info(b, &ninst, &nwork, &bytes, NULL);
+            if (ninst > stats->peak_instances) stats->peak_instances = ninst;
+            if (bytes > stats->peak_bytes) stats->peak_bytes = bytes;
+            if (c->autotune && ninst >= 2 && 2 * ninst >= 3 * (tuned_at > 0 ? tuned_at : 1)) {
+                if ((rc = hype_batch_autotune(b, 2, NULL, NULL))) break;
+                tuned_at = ninst;
+                ms_per_step = -1.0;
+            }
+            if (ms_per_step < 0.0) steps_per_poll = 1;   /* re-measure the step time */
+        }
+        /* 2. k steps of every resident instance; the next waiting request's
+         *    initial state is built on the host meanwhile */
+        if ((rc = hype_batch_advance(b, steps_per_poll))) break;
+        if (next < n && staged != next && (!c->realtime || req[next].arrival_s <= now_s() - t_start) &&
+            hype_batch_instance_bytes(&req[next].cfg) != 0 && (long long)req[next].cfg.nx * req[next].cfg.ny <= c->max_cells &&
+            make_initial(&req[next], next, fill, ctx, host) == HYPE_OK)
+            staged = next;
+        if ((rc = hype_batch_sync(b))) break;
+        stats->polls++;
+        stats->steps_replayed += steps_per_poll;
+        double ms = 0.0;
+        hype_batch_last_elapsed_ms(b, &ms);
+        if (ms > 0.0) {
+            const double per = ms / steps_per_poll;
+            ms_per_step = ms_per_step < 0.0 ? per : 0.5 * (ms_per_step + per);
+            int k = (int)(c->poll_ms / ms_per_step + 0.5);
+            steps_per_poll = k < 1 ? 1 : (k > 64 ? 64 : k);
+        }
+        /* 3. retire finished instances */
+        for (int s = 0; s < M; ++s) {
+            if (req_of[s] < 0) continue;
+            hype_instance_status is;
+            hype_batch_status(b, s, &is);
+            if (!is.done && is.status == HYPE_OK) continue;
+            const int i = req_of[s];
+            hype_request_result *o = &res[i];
+            o->status = is.status;
+            o->steps = is.steps;
+            o->t_end = is.t;
+            if (c->fetch_results || sink) {
+                const int st = hype_batch_get_state(b, s, host_out);
+                if (st != HYPE_OK && o->status == HYPE_OK) o->status = st;
+            }
+            o->done_s = now_s() - t_start;
+            o->latency_s = o->done_s - (c->realtime ? req[i].arrival_s : 0.0);
+            if (sink) sink(ctx, i, &req[i], host_out, o);
+            if (o->status == HYPE_OK) stats->cell_updates += (double)req[i].cfg.nx * req[i].cfg.ny * is.steps;
+            hype_batch_remove(b, s);
+            req_of[s] = -1;
+            --running;
+            ++finished;
+        }
+    }
+    const double t_end = now_s() - t_start;
+
+    /* statistics over the finished requests */
+    double *lat = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    double *que = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    int m = 0;
+    double sum = 0.0, first = n > 0 && c->realtime ? req[0].arrival_s : 0.0;
+    for (int i = 0; i < n && lat && que; ++i) {
+        if (res[i].status == HYPE_OK) stats->completed++;
+        else stats->failed++;
+        if (res[i].done_s <= 0.0 && res[i].status == HYPE_OK) continue;   /* never ran (loop stopped) */
+        lat[m] = res[i].latency_s;
+        que[m] = res[i].admit_s - (c->realtime ? req[i].arrival_s : 0.0);
+        sum += lat[m];
+        ++m;
+    }
+    if (lat && que && m > 0) {
+        qsort(lat, (size_t)m, sizeof(double), cmp_double);
+        qsort(que, (size_t)m, sizeof(double), cmp_double);
+        stats->p50_s = pct(lat, m, 50);
+        stats->p90_s = pct(lat, m, 90);
+        stats->p99_s = pct(lat, m, 99);
+        stats->max_s = lat[m - 1];
+        stats->mean_s = sum / m;
+        stats->queue_p50_s = pct(que, m, 50);
+        stats->queue_p99_s = pct(que, m, 99);
+    }
+    stats->wall_s = t_end - first;
+    stats->cell_updates_per_s = stats->wall_s > 0.0 ? stats->cell_updates / stats->wall_s : 0.0;
+    free(lat);
+    free(que);
+    free(req_of);
+    cudaFreeHost(host);
+    cudaFreeHost(host_out);
+    hype_batch_destroy(b);
+    return rc;
+}

@@ -107,8 +107,9 @@ HYPE_API int hype_batch_set_tiling(hype_batch *b, int cells, int rows);
  */
 HYPE_API int hype_batch_autotune(hype_batch *b, int reps, int *cells, int *rows);
 
-/* Instances held, work items per stage launch (all kinds), device bytes held. */
-HYPE_API int hype_batch_info(const hype_batch *b, int *instances, int *work_items, size_t *bytes_in_use);
+/* Instances held, work items per stage launch (all kinds), device bytes held,
+ * the admission budget. */
+HYPE_API int hype_batch_info(const hype_batch *b, int *instances, int *work_items, size_t *bytes_in_use, size_t *budget);
 
 HYPE_API int hype_batch_last_elapsed_ms(const hype_batch *b, double *ms);
 

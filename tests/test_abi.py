@@ -133,3 +133,27 @@ def test_shock_bubble_rankine_hugoniot(hp):
     s = r1 * u1 / (r1 - r0)
     assert abs((p1 - p0) - r0 * s * u1) < 1e-6 * p1
     assert orc is not None
+
+
+def test_serve_validates_before_device(hp):
+    """The request loop rejects a trace whose arrivals go backwards before it
+    touches a device; without a GPU it reports that instead of running."""
+    import torch
+    c = hp.Config(nx=16, ny=16)
+    with pytest.raises(hp.HypeError) as ei:
+        hp.serve([hp.Request(1.0, c), hp.Request(0.5, c)])
+    assert ei.value.status == hp.ERR_INVALID
+    if not torch.cuda.is_available():
+        with pytest.raises(hp.HypeError) as ei:
+            hp.serve([hp.Request(0.0, c, max_steps=2)])
+        assert ei.value.status in (hp.ERR_NO_DEVICE, hp.ERR_CUDA)
+
+
+def test_batch_instance_bytes(hp):
+    k = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=100, ny=30)
+    assert hp.Batch.instance_bytes(k) == 3 * 112 * 30 * 6 * 8                # pitch 112, U/S0/S1
+    k3 = hp.Config(system=hp.KAPILA_5EQN, order=3, nx=100, ny=30)
+    assert hp.Batch.instance_bytes(k3) == 4 * 112 * 30 * 6 * 8               # + S2 for SSPRK(10,4)
+    km = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=100, ny=30, precision=hp.PREC_MIXED)
+    assert hp.Batch.instance_bytes(km) == 3 * 128 * 30 * (4 * 4 + 2 * 8)     # FP32 x4 + FP64 x2 planes
+    assert hp.Batch.instance_bytes(hp.Config(nx=2, ny=2)) == 0                # invalid
