@@ -153,30 +153,91 @@ def cpu_baseline(nproc: int, steps: int, nx: int = 256, ny: int = 256):
                       f"{'oracle/_ref: HyPE-2D sources on a one-rank PETSc stand-in' if use_ref else 'oracle port'}"}
 
 
+_REF = {}
+
+
+def _ref_init(nx, ny, use_ref):
+    """Pool worker set-up: one independent shock-bubble instance per process."""
+    sys.path.insert(0, ROOT)
+    hp = load_pkg()
+    import oracle as O
+    U = hp.initial_state(hp.Config(nx=nx, ny=ny), "shock_bubble", seed=SEED, nbubbles=NBUB)
+    cfg = O.Config(system=O.KAPILA, order=2, nx=nx, ny=ny, cfl=0.4)
+    _REF.update(cfg=cfg, U=U, t=0.0, cells=nx * ny)
+    if use_ref:
+        _REF["ref"] = O.Reference(O.KAPILA)
+        _REF["ref"].setup(cfg)
+    else:
+        _REF["orc"] = O.Oracle()
+
+
+def _ref_sample(steps):
+    """Advances this process's instance by `steps` SSPRK(4,3) steps (one TS solve, as hype.c runs it)."""
+    t0 = time.perf_counter()
+    if "ref" in _REF:
+        U, n, t, *_ = _REF["ref"].solve(_REF["U"], _REF["t"], 1e30, steps)
+    else:
+        U, n, t, *_ = _REF["orc"].solve(_REF["cfg"], _REF["U"], _REF["t"], 1e30, steps)
+    _REF["U"], _REF["t"] = U, t
+    return _REF["cells"] * n, time.perf_counter() - t0
+
+
 def run_reference(args, rank, world):
+    """The reference's own CPU implementation of the path (oracle/_ref: the
+    HyPE-2D sources on a one-rank PETSc stand-in, or the oracle port if it was
+    not built) on all host cores: one process per core, each stepping an
+    independent 128 x 128 instance of the workload, 4 steps per sample.  Under
+    torchrun only rank 0 runs."""
     if rank != 0:
         return 0
+    sys.path.insert(0, ROOT)
+    import oracle as O
+    use_ref = O.reference_available()
     nproc = os.cpu_count() or 1
-    sample_steps = 2
-    base = None
-    for _ in range(max(0, args.warmup)):
-        pass   # the reference has no warm-up state (first call already steady)
-    vals = []
-    for _ in range(args.steps):
-        b = cpu_baseline(nproc, sample_steps)
-        vals.append(b["value"])
-        base = b
+    nx = ny = 128
+    per = 4
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(nproc, initializer=_ref_init, initargs=(nx, ny, use_ref)) as pool:
+        for _ in range(max(0, args.warmup)):
+            pool.map(_ref_sample, [per] * nproc, chunksize=1)
+        vals = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_ref_sample, [per] * nproc, chunksize=1)
+            wall = time.perf_counter() - t0
+            vals.append(sum(r[0] for r in res) / wall)
     value = float(np.median(vals))
-    base["value"] = value
+    kind = "reference" if use_ref else "port"
+    base = {"value": value, "unit": UNIT, "cores": nproc, "kind": kind,
+            "sample": f"{nproc} processes x independent Kapila shock-bubble {nx}x{ny} (4 bubbles), {per} SSPRK(4,3) "
+                      f"steps per sample, median of {args.steps} samples; "
+                      f"{'oracle/_ref: HyPE-2D sources on a one-rank PETSc stand-in' if use_ref else 'oracle port'}"}
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded shock-bubble generator)",
-            "config": {"workload": "kapila5-shock-bubble-fp64-ssprk43", "grid": "256x256 per core (sample)",
-                       "cores": nproc},
+            "config": {"workload": "kapila5-shock-bubble-2048x2048-fp64-weno3-ssprk43", "grid": f"{nx}x{ny} per core (sample)",
+                       "system": "kapila5", "order": 2, "bubbles": NBUB, "cfl": 0.4, "cores": nproc},
             "cpu_baseline": base,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
+
+
+def max_over_ranks(x: float, world: int, device: str = "cuda") -> float:
+    """The job's time is its slowest rank's: MAX all-reduce of a per-rank time."""
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_throughput(world: int, cells: int, steps: int, ms: float) -> float:
+    """Whole-job cell-updates/s of `world` independent replicas that each ran
+    `steps` steps of `cells` cells, the slowest taking `ms` milliseconds."""
+    return world * cells * steps / (ms * 1e-3)
 
 
 # ---------------------------------------------------------------------------
@@ -327,13 +388,9 @@ def run_gpu(args, rank, world, local_rank):
     barrier()
     if st != hp.OK:
         raise RuntimeError(f"timed run failed: status {st}")
-    ms = solver.last_elapsed_ms()
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(solver.last_elapsed_ms(), world)
     cells = NX * NY
-    value = world * cells * args.steps / (ms * 1e-3)
+    value = replica_throughput(world, cells, args.steps, ms)
     U_fp64 = solver.get_state() if not args.no_mixed else None
 
     # dominant kernel: the stage kernel, timed alone (CUDA events, same stream)
@@ -356,11 +413,7 @@ def run_gpu(args, rank, world, local_rank):
         solver.wait()
         solver.get_state(out=pin_out.numpy())
     barrier()
-    e2e_s = max(time.perf_counter() - t0, 1e-9)
-    if world > 1:
-        tt = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(max(time.perf_counter() - t0, 1e-9), world)
     state_bytes = cells * 6 * 8
     e2e = {"value": (world * cells * e2e_steps / e2e_s) if e2e_steps else None, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
            "d2h_bytes_per_step": state_bytes,
@@ -384,11 +437,7 @@ def run_gpu(args, rank, world, local_rank):
         sm.advance(args.steps)
         _, tm, _, stm = sm.wait()
         barrier()
-        ms_m = sm.last_elapsed_ms()
-        if world > 1:
-            tt = torch.tensor([ms_m], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms_m = float(tt.item())
+        ms_m = max_over_ranks(sm.last_elapsed_ms(), world)
         M = sm.get_state().reshape(-1, 6)
         F = U_fp64.reshape(-1, 6)
         ms_stage_m = sm.time_stage(20)
@@ -402,7 +451,7 @@ def run_gpu(args, rank, world, local_rank):
         dm = np.hypot(M[:, 2] - F[:, 2], M[:, 3] - F[:, 3])
         mag = np.hypot(F[:, 2], F[:, 3])
         errs["momentum_vector"] = [float(dm.sum() / mag.sum()), float(dm.max() / mag.max())]
-        vm = world * cells * args.steps / (ms_m * 1e-3)
+        vm = replica_throughput(world, cells, args.steps, ms_m)
         mixed = {"value": vm, "unit": UNIT, "ms_per_step": ms_m / args.steps, "speedup_vs_fp64": vm / value,
                  "status": stm, "stage_ms_per_launch": ms_stage_m, "autotuned_tile": mtile,
                  "bytes_per_cell_update": 9 * (4 * 4 + 2 * 8),

@@ -578,16 +578,22 @@ stage_batch_kernel(const StageParams *__restrict__ inst, const CUtensorMap *__re
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
     __shared__ int item_s;
+    // the item's parameters live in shared memory: re-read after every barrier
+    // of the tile instead of pinning registers for the whole tile
+    __shared__ StageParams p_s;
     const int nwork = sched[0];
     const DevScalars *last = nullptr;
     for (;;) {
         const int w = work_take(sched, nwork, last, &item_s);
         if (w >= nwork) break;
         const int2 it = work[w];
-        const StageParams &p = inst[it.x];
-        if (threadIdx.x == 0) fence_tensormap_acquire(&tmaps[it.x]);
-        stage_tile<SYS, N, CELLS>(p, &tmaps[it.x], it.y % p.strips, it.y / p.strips, smem_raw, red_s);
-        last = p.sc;
+        if (threadIdx.x == 0) {
+            p_s = inst[it.x];
+            fence_tensormap_acquire(&tmaps[it.x]);
+        }
+        __syncthreads();
+        stage_tile<SYS, N, CELLS>(p_s, &tmaps[it.x], it.y % p_s.strips, it.y / p_s.strips, smem_raw, red_s);
+        last = p_s.sc;
     }
     work_finish(sched);
 }

@@ -597,19 +597,21 @@ mixed_batch_kernel(const MixedParams *__restrict__ inst, const MixedMaps *__rest
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
     __shared__ int item_s;
+    __shared__ MixedParams p_s;   // re-read after each barrier instead of held in registers
     const int nwork = sched[0];
     const DevScalars *last = nullptr;
     for (;;) {
         const int w = work_take(sched, nwork, last, &item_s);
         if (w >= nwork) break;
         const int2 it = work[w];
-        const MixedParams &p = inst[it.x];
         if (threadIdx.x == 0) {
+            p_s = inst[it.x];
             fence_tensormap_acquire(&maps[it.x].f);
             fence_tensormap_acquire(&maps[it.x].d);
         }
-        mixed_tile<CELLS>(p, &maps[it.x], it.y % p.strips, it.y / p.strips, smem_raw, red_s);
-        last = p.sc;
+        __syncthreads();
+        mixed_tile<CELLS>(p_s, &maps[it.x], it.y % p_s.strips, it.y / p_s.strips, smem_raw, red_s);
+        last = p_s.sc;
     }
     work_finish(sched);
 }

@@ -1,0 +1,118 @@
+/*
+ * petsc_glue.c -- RHSFunctionPrim with the reference's PETSc signature,
+ * forwarding to the C ABI of include/hype_gpu.h.
+ *
+ * It replaces HyPE-2D/rhs_function_prim.c in a HyPE-2D build: compile it in
+ * that tree (it includes the tree's hype.h for AppCtx, the PDE-system #define
+ * and the EOS constants GAMMA_1, GAMMA_2, PI_1, PI_2, and the tree's PETSc),
+ * link libhype_b200.so, and hype.c's
+ *     TSSetRHSFunction(ts, NULL, RHSFunctionPrim, &Ctx);       (hype.c:344)
+ * and its direct dt-seeding call (hype.c:343) reach the B200 kernels.
+ *
+ * Contract kept from rhs_function_prim.c:12-626 / hype.h:306:
+ *   - RHS is overwritten for every owned cell; U is not modified;
+ *   - Ctx->dt is set to CFL*h/(2*s_max) (rhs_function_prim.c:617-623);
+ *   - the scratch of AppCtx (W, localU, u_bnd, F, G, D, E) is not touched:
+ *     the kernels need none of it.
+ * Differences:
+ *   - an inadmissible face state (the reference prints and calls MPI_Abort,
+ *     e.g. kapila_5eqn.c:353-357) prints the same kind of message and returns
+ *     a non-zero PetscErrorCode, so TS stops through CHKERRQ instead of the
+ *     process ending;
+ *   - one MPI rank: the whole grid is on this rank's GPU (the DMDA must not
+ *     be split); with more ranks the call returns an error.
+ * The GPU solver is created on first use and re-created when the AppCtx
+ * parameters change (grid, order, CFL, boundaries).  The device is
+ * HYPE_DEVICE from the environment, else 0.
+ */
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include "hype.h"
+#include "hype_gpu.h"
+
+static hype_solver *glue_solver = NULL;
+static hype_config glue_cfg;
+
+static int glue_system(void)
+{
+#if defined(KAPILA_5EQN)
+    return HYPE_KAPILA_5EQN;
+#elif defined(BAER_NUNZIATO)
+    return HYPE_BAER_NUNZIATO;
+#else
+    return HYPE_EULER;
+#endif
+}
+
+/* AppCtx (hype.h:203-252) and the compile-time constants -> hype_config.
+ * enum bndry_type (hype.h:76) and HYPE_BC_* have the same values. */
+static void glue_config(const AppCtx *Ctx, hype_config *c)
+{
+    const char *dev = getenv("HYPE_DEVICE");
+    hype_config_default(c);
+    c->system = glue_system();
+    c->order = (int)Ctx->N;
+    c->nx = (int)Ctx->N_x;
+    c->ny = (int)Ctx->N_y;
+    c->x_min = Ctx->x_min; c->x_max = Ctx->x_max;
+    c->y_min = Ctx->y_min; c->y_max = Ctx->y_max;
+    c->cfl = Ctx->CFL;
+    c->bc_left = (int)Ctx->LeftBoundary;
+    c->bc_right = (int)Ctx->RightBoundary;
+    c->bc_bottom = (int)Ctx->BottomBoundary;
+    c->bc_top = (int)Ctx->TopBoundary;
+    c->gamma1 = GAMMA_1; c->gamma2 = GAMMA_2;
+    c->pi1 = PI_1; c->pi2 = PI_2;
+    c->precision = HYPE_PREC_FP64;
+    c->device = dev ? atoi(dev) : 0;
+}
+
+/* Frees the GPU solver (e.g. from the application's clean-up, hype.c:421-451). */
+void RHSFunctionPrimFinalize(void)
+{
+    hype_destroy(glue_solver);
+    glue_solver = NULL;
+}
+
+PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
+{
+    AppCtx *Ctx = (AppCtx *)ctx;
+    int size = 1;
+    (void)ts;
+    MPI_Comm_size(PETSC_COMM_WORLD, &size);
+    if (size != 1) {
+        fprintf(stderr, "RHSFunctionPrim (GPU): one MPI rank only, got %d\n", size);
+        return 1;
+    }
+    hype_config c;
+    glue_config(Ctx, &c);
+    if (!glue_solver || memcmp(&c, &glue_cfg, sizeof(c)) != 0) {
+        RHSFunctionPrimFinalize();
+        hype_solver *s = NULL;
+        const int st = hype_create(&c, &s);
+        if (st != HYPE_OK) {
+            fprintf(stderr, "RHSFunctionPrim (GPU): %s\n", s ? hype_last_error(s) : hype_status_string(st));
+            hype_destroy(s);
+            return (PetscErrorCode)st;
+        }
+        glue_solver = s;
+        glue_cfg = c;
+    }
+    const PetscScalar *u = NULL;
+    PetscScalar *r = NULL;
+    PetscErrorCode ierr = VecGetArrayRead(U, &u);
+    if (ierr) return ierr;
+    ierr = VecGetArray(RHS, &r);
+    if (ierr) { VecRestoreArrayRead(U, &u); return ierr; }
+    double dt = 0.0;
+    const int st = hype_rhs_prim(glue_solver, (double)t, (const double *)u, (double *)r, &dt);
+    VecRestoreArray(RHS, &r);
+    VecRestoreArrayRead(U, &u);
+    if (st != HYPE_OK) {
+        fprintf(stderr, "RHSFunctionPrim (GPU): %s\n", hype_last_error(glue_solver));
+        return (PetscErrorCode)st;
+    }
+    Ctx->dt = dt;   /* rhs_function_prim.c:623 */
+    return 0;
+}

@@ -1,0 +1,59 @@
+/*
+ * glue_driver.c -- TEST INFRASTRUCTURE.  Calls the product's PETSc-signature
+ * RHSFunctionPrim (hype-parallel_b200/csrc/petsc_glue.c) the way HyPE-2D's
+ * hype.c does (an AppCtx filled as hype.c:32-68 fills it, a DMDA global Vec,
+ * hype.c:343), on the one-rank PETSc stand-in of oracle/petsc_mini, and hands
+ * the RHS and Ctx.dt back to the Python test.  Built by tests/glue/Makefile
+ * with -include oracle/petsc_mini/hype_ref_cfg.h (AppCtx, bndry_type) and
+ * -D<SYSTEM> -DHYPE_REF_NVAR=<nVar>.
+ */
+#include <string.h>
+
+PetscReal GAMMA_1 = 1.4, GAMMA_2 = 1.4, PI_1 = 0.0, PI_2 = 0.0;
+
+PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx);
+void RHSFunctionPrimFinalize(void);
+
+int glue_nvar(void) { return nVar; }
+
+int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int bc[4], const double eos[4],
+             const double *Uin, double *Rout, double *dt)
+{
+    GAMMA_1 = eos[0]; GAMMA_2 = eos[1]; PI_1 = eos[2]; PI_2 = eos[3];
+    AppCtx Ctx;
+    memset(&Ctx, 0, sizeof(Ctx));
+    Ctx.N = N; Ctx.N_x = nx; Ctx.N_y = ny;
+    Ctx.x_min = dom[0]; Ctx.x_max = dom[1]; Ctx.y_min = dom[2]; Ctx.y_max = dom[3];
+    Ctx.CFL = cfl;
+    Ctx.h = (Ctx.x_max - Ctx.x_min) / (PetscReal)Ctx.N_x;
+    Ctx.LeftBoundary = (enum bndry_type)bc[0]; Ctx.RightBoundary = (enum bndry_type)bc[1];
+    Ctx.BottomBoundary = (enum bndry_type)bc[2]; Ctx.TopBoundary = (enum bndry_type)bc[3];
+    Ctx.ReconsPrimitive = PETSC_TRUE;
+    const DMBoundaryType bx = (bc[0] == periodic || bc[1] == periodic) ? DM_BOUNDARY_PERIODIC : DM_BOUNDARY_GHOSTED;
+    const DMBoundaryType by = (bc[2] == periodic || bc[3] == periodic) ? DM_BOUNDARY_PERIODIC : DM_BOUNDARY_GHOSTED;
+    DM da;
+    Vec U, R;
+    DMDACreate2d(PETSC_COMM_WORLD, bx, by, DMDA_STENCIL_BOX, nx, ny, PETSC_DECIDE, PETSC_DECIDE, nVar, 3, NULL, NULL, &da);
+    DMSetUp(da);
+    DMCreateGlobalVector(da, &U);
+    VecDuplicate(U, &R);
+    PetscScalar *a;
+    VecGetArray(U, &a);
+    memcpy(a, Uin, sizeof(double) * (size_t)nx * ny * nVar);
+    VecRestoreArray(U, &a);
+    TS ts;
+    TSCreate(PETSC_COMM_WORLD, &ts);
+    TSSetDM(ts, da);
+    const PetscErrorCode ierr = RHSFunctionPrim(ts, 0.0, U, R, &Ctx);
+    VecGetArray(R, &a);
+    memcpy(Rout, a, sizeof(double) * (size_t)nx * ny * nVar);
+    VecRestoreArray(R, &a);
+    *dt = Ctx.dt;
+    TSDestroy(&ts);
+    VecDestroy(&U);
+    VecDestroy(&R);
+    DMDestroy(&da);
+    return (int)ierr;
+}
+
+void glue_finalize(void) { RHSFunctionPrimFinalize(); }

@@ -1,0 +1,78 @@
+"""The PETSc-signature drop-in (hype-parallel_b200/csrc/petsc_glue.c).
+
+The glue is compiled the way a HyPE-2D tree would compile it (hype.h's
+AppCtx and system #define, PETSc from the one-rank stand-in of
+oracle/petsc_mini) and called as hype.c calls RHSFunctionPrim.  On a GPU its
+RHS and Ctx->dt must equal the reference's bit for bit; without one it must
+return an error code instead of ending the process.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GLUE = os.path.join(ROOT, "tests", "glue")
+LIBNAME = {O.EULER: "euler", O.KAPILA: "kapila", O.BN: "bn"}
+
+
+@pytest.fixture(scope="module")
+def glue_libs(hp):
+    subprocess.run(["make", "-s", "-C", GLUE], check=True, capture_output=True)
+    libs = {}
+    for sysid, nm in LIBNAME.items():
+        L = ctypes.CDLL(os.path.join(GLUE, "_build", f"libglue_{nm}.so"))
+        DP = ctypes.POINTER(ctypes.c_double)
+        IP = ctypes.POINTER(ctypes.c_int)
+        L.glue_rhs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, ctypes.c_double, IP, DP, DP, DP, DP]
+        L.glue_rhs.restype = ctypes.c_int
+        libs[sysid] = L
+    return libs
+
+
+def glue_rhs(L, cfg, U):
+    dom = (ctypes.c_double * 4)(cfg.x_min, cfg.x_max, cfg.y_min, cfg.y_max)
+    bc = (ctypes.c_int * 4)(cfg.bc_left, cfg.bc_right, cfg.bc_bottom, cfg.bc_top)
+    eos = (ctypes.c_double * 4)(cfg.gamma1, cfg.gamma2, cfg.pi1, cfg.pi2)
+    R = np.empty_like(U)
+    dt = ctypes.c_double(0.0)
+    DP = ctypes.POINTER(ctypes.c_double)
+    st = L.glue_rhs(cfg.order, cfg.nx, cfg.ny, dom, cfg.cfl, bc, eos, U.ctypes.data_as(DP), R.ctypes.data_as(DP),
+                    ctypes.byref(dt))
+    return R, dt.value, st
+
+
+def test_glue_builds_and_exports_the_reference_signature(glue_libs):
+    for L in glue_libs.values():
+        assert L.RHSFunctionPrim is not None and L.RHSFunctionPrimFinalize is not None
+
+
+def test_glue_without_gpu_returns_an_error(hp, glue_libs):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    cfg = O.Config(system=O.KAPILA, order=2, nx=8, ny=8, **cases.KAPILA_EOS)
+    R, dt, st = glue_rhs(glue_libs[O.KAPILA], cfg, cases.state(cfg, "bubble", 1))
+    assert st == hp.ERR_NO_DEVICE
+
+
+GLUE_CASES = ["kapila_37x23_rough_mixed_bc", "kapila_18x14_inlet", "kapila_15x13_N3", "euler_21x19_reflective_N1",
+              "bn_16x16", "bn_13x21_periodic_N1"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", GLUE_CASES)
+def test_glue_rhs_bitwise_vs_oracle(name, hp, orc, glue_libs):
+    _, cfg, kind, seed = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    Ro, dto, sto = orc.rhs(cfg, U)
+    assert sto == O.OK
+    R, dt, st = glue_rhs(glue_libs[cfg.system], cfg, U)
+    assert st == 0
+    assert dt == dto
+    assert R.tobytes() == Ro.tobytes()
