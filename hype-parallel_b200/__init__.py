@@ -30,6 +30,7 @@ EULER, KAPILA_5EQN, BAER_NUNZIATO = 0, 1, 2
 BC_WALL, BC_INLET, BC_PERIODIC, BC_REFLECTIVE, BC_TRANSMISSIVE = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 FLAG_BN_FIX_P2 = 1
+FLAG_CONSERVATIVE = 2
 NVAR = {EULER: 4, KAPILA_5EQN: 6, BAER_NUNZIATO: 9}
 
 

@@ -134,6 +134,24 @@ void hype::inlet_table(const hype_config &c, double h, std::vector<double> &tab)
         }
 }
 
+// InletBC = PDEPrim2Cons(InletBCPrim(...)) (kapila_5eqn.c:289-320, 41-61),
+// evaluated on the host for the conservative path's ghost columns.
+void hype::inlet_to_conserved(const hype_config &c, std::vector<double> &tab)
+{
+    const double G1m1 = c.gamma1 - 1.0, G2m1 = c.gamma2 - 1.0;
+    for (size_t k = 0; k + 6 <= tab.size(); k += 6) {
+        double *V = &tab[k];
+        const double alpha_1 = V[5];
+        const double alpha_2 = 1.0 - alpha_1;
+        const double rho = alpha_1 * V[0] + alpha_2 * V[1];
+        const double u = V[2], v = V[3], p = V[4];
+        const double ei = (p * (alpha_1 * G2m1 + alpha_2 * G1m1) + alpha_1 * c.gamma1 * c.pi1 * G2m1 + alpha_2 * c.gamma2 * c.pi2 * G1m1) / (G1m1 * G2m1);
+        const double E = ei + 0.5 * rho * (u * u + v * v);
+        const double Q[6] = {alpha_1 * V[0], alpha_2 * V[1], rho * V[2], rho * V[3], E, alpha_1};
+        for (int q = 0; q < 6; ++q) V[q] = Q[q];
+    }
+}
+
 static StageParams base_params(const hype_solver *s)
 {
     StageParams p;
@@ -185,8 +203,15 @@ static int set_tiling(hype_solver *s, int cells, int waves = 1)
         if (s->step_exec) { cudaGraphExecDestroy(s->step_exec); s->step_exec = nullptr; }
         return HYPE_OK;
     }
-    CUDA_TRY(s, stage_configure(cfg->system, cfg->order, cells));
-    s->bps = stage_blocks_per_sm(cfg->system, cfg->order, cells);
+    if (cfg->flags & HYPE_FLAG_CONSERVATIVE) {   // the conservative kernels come in 128-column tiles only
+        cells = STAGE_CELLS;
+        s->cells = cells;
+        CUDA_TRY(s, stage_cons_configure(cfg->system, cfg->order));
+        s->bps = stage_cons_blocks_per_sm(cfg->system, cfg->order);
+    } else {
+        CUDA_TRY(s, stage_configure(cfg->system, cfg->order, cells));
+        s->bps = stage_blocks_per_sm(cfg->system, cfg->order, cells);
+    }
     if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "stage kernel does not fit on an SM");
     s->strips = stage_strips(cfg->nx, cells);
     const int slots = s->sms * s->bps * (waves > 0 ? waves : 1);
@@ -213,6 +238,7 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
     p.in = in; p.out = out; p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc; p.xn = xn; p.out2 = out2;
     p.reduce_smax = reduce;
     p.out_aos = out_aos;
+    if (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) return launch_stage_cons(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->stream);
     return launch_stage(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
 }
 
@@ -304,6 +330,10 @@ static int check_config(const hype_config *c, hype_solver *s)
         return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for the Kapila system");
     if (c->precision == HYPE_PREC_MIXED && (c->order != 2 || c->bc_left == HYPE_BC_INLET))
         return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for N = 2 without inlet boundaries");
+    if (c->precision == HYPE_PREC_MIXED && (c->flags & HYPE_FLAG_CONSERVATIVE))
+        return fail(s, HYPE_ERR_INVALID, "the conservative-variable path is FP64 only");
+    if (c->flags & ~(HYPE_FLAG_BN_FIX_P2 | HYPE_FLAG_CONSERVATIVE))
+        return fail(s, HYPE_ERR_INVALID, "unknown flags 0x%x", c->flags);
     return HYPE_OK;
 }
 
@@ -433,6 +463,7 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     if (cfg->bc_left == HYPE_BC_INLET) {
         std::vector<double> tab;
         inlet_table(*cfg, s->h, tab);
+        if (cfg->flags & HYPE_FLAG_CONSERVATIVE) inlet_to_conserved(*cfg, tab);
         CUDA_TRY(s, cudaMalloc(&s->dInlet, sizeof(double) * tab.size()));
         CUDA_TRY(s, cudaMemcpy(s->dInlet, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
     }

@@ -71,6 +71,10 @@ int stage_batch_blocks_per_sm(int sys, int order, int cells);   // resident bloc
 cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
                                const int2 *work, int *sched, int blocks, cudaStream_t s);
+// conservative-variable path (RHSFunction): 128-column tiles, grid form
+cudaError_t stage_cons_configure(int sys, int order);
+int stage_cons_blocks_per_sm(int sys, int order);
+cudaError_t launch_stage_cons(int sys, int order, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 // Strips of a grid: with S = ceil(nx/(cells-4)) strips and even origins
 // 2*floor(s*nx/(2S)), every strip has at most 2*ceil(nx/(2S)) <= cells-4
 // columns and the last one at most nx/S + 2 <= cells-2.
@@ -157,5 +161,6 @@ CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, 
                            int box_w);
 int validate_config(const hype_config *c, char *err, size_t errlen);
 void inlet_table(const hype_config &c, double h, std::vector<double> &tab);
+void inlet_to_conserved(const hype_config &c, std::vector<double> &tab);
 
 }  // namespace hype

@@ -224,6 +224,87 @@ template <> struct System<SYS_KAPILA> {
         if (alpha_1 < 0.0 || alpha_1 > 1.0) return false;
         return true;
     }
+
+    // ---- conservative-variable path (RHSFunction, rhs_function.c) ----
+    // kapila_5eqn.c:67-113
+    template <int DIR>
+    __device__ __forceinline__ static double flux_cons(const Eos &e, const double *Q, double *F, bool &bad)
+    {
+        constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
+        double alpha_1 = Q[5];
+        double alpha_2 = 1.0 - alpha_1;
+        double rho_1 = Q[0] / alpha_1;
+        double rho_2 = Q[1] / alpha_2;
+        double rho = Q[0] + Q[1];
+        double u = Q[2] / rho;
+        double v = Q[3] / rho;
+        double E = Q[4];
+        double ei = E - 0.5 * rho * (u * u + v * v);
+        double G1m1 = e.g1 - 1.0;
+        double G2m1 = e.g2 - 1.0;
+        double p = (ei * G1m1 * G2m1 - alpha_1 * e.g1 * e.pi1 * G2m1 - alpha_2 * e.g2 * e.pi2 * G1m1) / (alpha_1 * G2m1 + alpha_2 * G1m1);
+        double un = u * nx + v * ny;
+        double a1_sq = e.g1 * (p + e.pi1) / rho_1;
+        double a2_sq = e.g2 * (p + e.pi2) / rho_2;
+        double a_sq = (rho_1 * a1_sq * rho_2 * a2_sq) / (rho * (alpha_2 * rho_1 * a1_sq + alpha_1 * rho_2 * a2_sq));
+        bad |= (a_sq < PRS_FLOOR);
+        F[0] = alpha_1 * rho_1 * un;
+        F[1] = alpha_2 * rho_2 * un;
+        F[2] = rho * u * un + p * nx;
+        F[3] = rho * v * un + p * ny;
+        F[4] = (E + p) * un;
+        F[5] = 0.0;
+        return fabs(un) + sqrt(a_sq);
+    }
+    // kapila_5eqn.c:164-198
+    __device__ __forceinline__ static void ncp_cons(const Eos &e, const double *Q, const double *gx, const double *gy, double *B)
+    {
+        double alpha_1 = Q[5];
+        double alpha_2 = 1.0 - alpha_1;
+        double rho_1 = Q[0] / alpha_1;
+        double rho_2 = Q[1] / alpha_2;
+        double rho = Q[0] + Q[1];
+        double irho = 1.0 / rho;
+        double u = Q[2] / rho;
+        double v = Q[3] / rho;
+        double E = Q[4];
+        double ei = E - 0.5 * rho * (u * u + v * v);
+        double G1m1 = e.g1 - 1.0;
+        double G2m1 = e.g2 - 1.0;
+        double p = (ei * G1m1 * G2m1 - alpha_1 * e.g1 * e.pi1 * G2m1 - alpha_2 * e.g2 * e.pi2 * G1m1) / (alpha_1 * G2m1 + alpha_2 * G1m1);
+        double a1_sq = e.g1 * (p + e.pi1) / rho_1;
+        double a2_sq = e.g2 * (p + e.pi2) / rho_2;
+        double K = alpha_1 * alpha_2 * (rho_2 * a2_sq - rho_1 * a1_sq) / (alpha_1 * rho_2 * a2_sq + alpha_2 * rho_1 * a1_sq);
+        double alpha1_x = gx[5], alpha1_y = gy[5];
+        double u_x = irho * irho * (gx[2] * rho - Q[2] * (gx[0] + gx[1]));
+        double v_y = irho * irho * (gy[3] * rho - Q[3] * (gy[0] + gy[1]));
+        B[0] = 0.0; B[1] = 0.0; B[2] = 0.0; B[3] = 0.0; B[4] = 0.0;
+        B[5] = u * alpha1_x + v * alpha1_y - K * (u_x + v_y);
+    }
+    static constexpr bool ncp_cons_nonzero(int c) { return c == 5; }
+    // kapila_5eqn.c:247-283; its alpha test (line 278) rejects every alpha_1 != 1
+    __device__ __forceinline__ static bool pad_cons(const Eos &e, const double *Q)
+    {
+        double alpha_1 = Q[5];
+        double alpha_2 = 1.0 - alpha_1;
+        double rho_1 = Q[0] / alpha_1;
+        double rho_2 = Q[1] / alpha_2;
+        double rho = Q[0] + Q[1];
+        double u = Q[2] / rho;
+        double v = Q[3] / rho;
+        double E = Q[4];
+        double ei = E - 0.5 * rho * (u * u + v * v);
+        double G1m1 = e.g1 - 1.0;
+        double G2m1 = e.g2 - 1.0;
+        double p = (ei * G1m1 * G2m1 - alpha_1 * e.g1 * e.pi1 * G2m1 - alpha_2 * e.g2 * e.pi2 * G1m1) / (alpha_1 * G2m1 + alpha_2 * G1m1);
+        double a1_sq = e.g1 * (p + e.pi1) / rho_1;
+        double a2_sq = e.g2 * (p + e.pi2) / rho_2;
+        double a_sq = (rho_1 * a1_sq * rho_2 * a2_sq) / (rho * (alpha_2 * rho_1 * a1_sq + alpha_1 * rho_2 * a2_sq));
+        if (rho < RHO_FLOOR) return false;
+        if (a_sq < PRS_FLOOR) return false;
+        if (alpha_1 < 1.0 || alpha_1 > 1.0) return false;
+        return true;
+    }
 };
 
 // baer_nunziato.c: cons [a1 r1, a1 r1 u1, a1 r1 v1, a1 E1, a2 r2, a2 r2 u2, a2 r2 v2, a2 E2, a1]
@@ -319,6 +400,81 @@ template <> struct System<SYS_BN> {
         if (V[8] < 0.0 || V[8] > 1.0) ok = false;
         return ok;
     }
+
+    // ---- conservative-variable path (RHSFunction, rhs_function.c) ----
+    // baer_nunziato.c:66-131
+    template <int DIR>
+    __device__ __forceinline__ static double flux_cons(const Eos &e, const double *Q, double *F, bool &bad)
+    {
+        constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
+        double phi_1 = Q[8];
+        double phi_2 = 1.0 - Q[8];
+        double rho_1 = Q[0] / phi_1;
+        double rho_2 = Q[4] / phi_2;
+        double u_1 = Q[1] / Q[0], v_1 = Q[2] / Q[0];
+        double u_2 = Q[5] / Q[4], v_2 = Q[6] / Q[4];
+        double E_1 = Q[3] / phi_1;
+        double E_2 = Q[7] / phi_2;
+        double p_1 = (e.g1 - 1.0) * (E_1 - 0.5 * rho_1 * (u_1 * u_1 + v_1 * v_1)) - e.g1 * e.pi1;
+        double p_2 = (e.g2 - 1.0) * (E_2 - 0.5 * rho_2 * (u_2 * u_2 + v_2 * v_2)) - e.g2 * e.pi2;
+        double un_1 = nx * u_1 + ny * v_1;
+        double un_2 = nx * u_2 + ny * v_2;
+        bad |= (rho_1 < RHO_FLOOR) | (rho_2 < RHO_FLOOR) | ((p_1 + e.pi1) < PRS_FLOOR) | ((p_2 + e.pi2) < PRS_FLOOR);
+        F[0] = phi_1 * rho_1 * un_1;
+        F[1] = phi_1 * (rho_1 * u_1 * un_1 + nx * p_1);
+        F[2] = phi_1 * (rho_1 * v_1 * un_1 + ny * p_1);
+        F[3] = phi_1 * un_1 * (E_1 + p_1);
+        F[4] = phi_2 * rho_2 * un_2;
+        F[5] = phi_2 * (rho_2 * u_2 * un_2 + nx * p_2);
+        F[6] = phi_2 * (rho_2 * v_2 * un_2 + ny * p_2);
+        F[7] = phi_2 * un_2 * (E_2 + p_2);
+        F[8] = 0.0;
+        double s_1 = fabs(un_1) + sqrt(e.g1 * (p_1 + e.pi1) / rho_1);
+        double s_2 = fabs(un_2) + sqrt(e.g2 * (p_2 + e.pi2) / rho_2);
+        return (s_1 < s_2) ? s_2 : s_1;
+    }
+    // baer_nunziato.c:137-165: u_I = u_1, p_I = p_2 from the phase-2 state
+    __device__ __forceinline__ static void ncp_cons(const Eos &e, const double *Q, const double *gx, const double *gy, double *B)
+    {
+        double phi_2 = 1.0 - Q[8];
+        double rho_2 = Q[4] / phi_2;
+        double u_1 = Q[1] / Q[0], v_1 = Q[2] / Q[0];
+        double u_2 = Q[5] / Q[4], v_2 = Q[6] / Q[4];
+        double E_2 = Q[7] / phi_2;
+        double p_I = (e.g2 - 1.0) * (E_2 - 0.5 * rho_2 * (u_2 * u_2 + v_2 * v_2)) - e.g2 * e.pi2;
+        double phi_x = gx[8], phi_y = gy[8];
+        B[0] = 0.0;
+        B[1] = -p_I * phi_x;
+        B[2] = -p_I * phi_y;
+        B[3] = -p_I * (u_1 * phi_x + v_1 * phi_y);
+        B[4] = 0.0;
+        B[5] = p_I * phi_x;
+        B[6] = p_I * phi_y;
+        B[7] = p_I * (u_1 * phi_x + v_1 * phi_y);
+        B[8] = u_1 * phi_x + v_1 * phi_y;
+    }
+    static constexpr bool ncp_cons_nonzero(int c) { return c != 0 && c != 4; }
+    // baer_nunziato.c:207-250
+    __device__ __forceinline__ static bool pad_cons(const Eos &e, const double *Q)
+    {
+        bool ok = true;
+        double phi_1 = Q[8];
+        double phi_2 = 1.0 - Q[8];
+        double rho_1 = Q[0] / phi_1;
+        double rho_2 = Q[4] / phi_2;
+        double u_1 = Q[1] / Q[0], v_1 = Q[2] / Q[0];
+        double u_2 = Q[5] / Q[4], v_2 = Q[6] / Q[4];
+        double E_1 = Q[3] / phi_1;
+        double E_2 = Q[7] / phi_2;
+        double p_1 = (e.g1 - 1.0) * (E_1 - 0.5 * rho_1 * (u_1 * u_1 + v_1 * v_1)) - e.g1 * e.pi1;
+        double p_2 = (e.g2 - 1.0) * (E_2 - 0.5 * rho_2 * (u_2 * u_2 + v_2 * v_2)) - e.g2 * e.pi2;
+        if (rho_1 < RHO_FLOOR) ok = false;
+        if (rho_2 < RHO_FLOOR) ok = false;
+        if ((p_1 + e.pi1) < PRS_FLOOR) ok = false;
+        if ((p_2 + e.pi2) < PRS_FLOOR) ok = false;
+        if (phi_1 < 0.0 || phi_1 > 1.0) ok = false;
+        return ok;
+    }
 };
 
 // euler.c: cons [rho, rho u, rho v, E], prim [rho, u, v, p], ideal gas GAMMA_1
@@ -373,6 +529,47 @@ template <> struct System<SYS_EULER> {
         bool ok = true;
         if (V[0] < RHO_FLOOR) ok = false;
         if (V[3] < PRS_FLOOR) ok = false;
+        return ok;
+    }
+
+    // ---- conservative-variable path (RHSFunction, rhs_function.c) ----
+    // euler.c:44-84
+    template <int DIR>
+    __device__ __forceinline__ static double flux_cons(const Eos &e, const double *Q, double *F, bool &bad)
+    {
+        constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
+        double rho = Q[0];
+        double irho = 1.0 / rho;
+        double u = irho * Q[1];
+        double v = irho * Q[2];
+        double un = nx * u + ny * v;
+        double rhoun = rho * un;
+        double E = Q[3];
+        double p = (e.g1 - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+        bad |= (rho < RHO_FLOOR) | (p < PRS_FLOOR);
+        F[0] = rhoun;
+        F[1] = rhoun * u + nx * p;
+        F[2] = rhoun * v + ny * p;
+        F[3] = un * (E + p);
+        return fabs(un) + sqrt(e.g1 * p * irho);
+    }
+    __device__ __forceinline__ static void ncp_cons(const Eos &, const double *, const double *, const double *, double *B)
+    {
+        B[0] = 0.0; B[1] = 0.0; B[2] = 0.0; B[3] = 0.0;
+    }
+    static constexpr bool ncp_cons_nonzero(int) { return false; }
+    // euler.c:169-191
+    __device__ __forceinline__ static bool pad_cons(const Eos &e, const double *Q)
+    {
+        bool ok = true;
+        double rho = Q[0];
+        double irho = 1.0 / rho;
+        double u = irho * Q[1];
+        double v = irho * Q[2];
+        double E = Q[3];
+        double p = (e.g1 - 1.0) * (E - 0.5 * rho * (u * u + v * v));
+        if (rho < RHO_FLOOR) ok = false;
+        if (p < PRS_FLOOR) ok = false;
         return ok;
     }
 };

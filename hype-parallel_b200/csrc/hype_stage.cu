@@ -1,563 +1,16 @@
-// hype_stage.cu -- the fused FP64 stage kernel: one launch evaluates HyPE-2D's
-// primitive-variable right-hand side L(S) (RHSFunctionPrim, rhs_function_prim.c:12-626)
-// on the stage input S and writes one SSP-RK stage combination of it, folding
-// the CFL wave-speed maximum (rhs_function_prim.c:617-623) into a device scalar.
-//
-// Tiling.  A tile is a strip of up to CELLS-2 columns and a run of rows of one
-// grid, processed by a block of 2*CELLS threads, two per column.  The block
-// marches up its rows; at row r the thread pair m reconstructs the cell in
-// column x0-1+m (the strip plus one ring column each side), so only two of
-// CELLS reconstructions per row are repeated by the neighbouring strip.  Rows of the conserved state arrive by one TMA 3-D box
-// load per row (all fields, columns x0-4 .. x0+NT+1) into a ring of
-// STAGE_SLOTS shared-memory rows, are patched at domain edges with the
-// boundary-condition copies, and are converted to primitive variables in place.
-// Reconstruction coefficients go to shared memory, the x-face Riemann problem
-// at the left of each column is solved by that column's thread from its own
-// and its left neighbour's coefficients, the y-face problem below each cell by
-// the cell's thread from its coefficients and the top-face values it kept
-// from the row below.  Row r-1 is completed (y-flux difference, volume
-// non-conservative term, RK combination) while row r is processed.
+// hype_stage.cu -- the primitive-variable stage kernels (RHSFunctionPrim,
+// rhs_function_prim.c:12-626) in their grid form (one block per tile) and
+// persistent form (blocks walk a work-list of tiles of many grids), and the
+// host dispatch over (system, order, tile width).  The tile itself is
+// stage_tile in hype_stage_tile.cuh.
 //
 // Built with --fmad=false: arithmetic rounds exactly as the reference's C does.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdio>
-#include "hype_internal.h"
-#include "hype_tma.cuh"
+#include "hype_stage_tile.cuh"
 
 namespace hype {
-
-template <int SYS, int N, int CELLS_>
-struct StageKernel {
-    using S = System<SYS>;
-    using QD = Quad<N>;
-    static constexpr int NV = S::NV;
-    static constexpr int CELLS = CELLS_;         // reconstruction columns per tile
-    static constexpr int NT = 2 * CELLS;         // two threads per cell
-    static constexpr int BW = CELLS + 6;         // TMA box width
-    static constexpr int SLOTS = STAGE_SLOTS;
-    static constexpr int NDOF = QD::NDOF;
-    static constexpr int NC = NDOF - 1;                    // stored coefficients (k >= 1)
-    static constexpr int ROW_ELEMS = BW * NV;
-    static constexpr int ROW_BYTES = ROW_ELEMS * 8;
-    static constexpr int SLOT_STRIDE = ((ROW_BYTES + 127) / 128) * 128 / 8;   // doubles
-    // per-cell arrays, [k][c][cell] so consecutive cells hit consecutive banks
-    static constexpr int COEF_ELEMS = (NC > 2 ? NC : 2) * NV * CELLS;         // also the x-flux exchange (2 NV)
-    static constexpr int YT_ELEMS = 2 * NV * CELLS;                            // top-face values, by Gauss point
-    static constexpr int CARRY_ELEMS = 4 * NV * CELLS;                         // ncp, t1, G below, E below
-    static constexpr int MIN_BLOCKS = (NV <= 6 ? 2 : 1) * (128 / CELLS);
-    static constexpr size_t smem_bytes()
-    {
-        return 128 /* barriers */ + (size_t)SLOTS * SLOT_STRIDE * 8 + (size_t)(COEF_ELEMS + YT_ELEMS + CARRY_ELEMS) * 8 + 64;
-    }
-};
-
-// Value of one variable's polynomial cf[0..NDOF) at Gauss point q (0/1, run
-// time) of face F.  Where both Gauss points share a basis value it is folded
-// at compile time (zero terms dropped, exact as in poly_eval); otherwise the
-// product with the selected value is formed exactly as the reference does.
-template <int N, int F>
-__device__ __forceinline__ double face_val(const double *cf, int q)
-{
-    using QD = Quad<N>;
-    double v = 0.0;
-    static_for<QD::NDOF>([&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        constexpr double p0 = QD::phi_face(F, 0, k);
-        constexpr double p1 = QD::phi_face(F, QD::NFGP > 1 ? 1 : 0, k);
-        if constexpr (p0 == p1) {
-            if constexpr (p0 != 0.0) {
-                if constexpr (p0 == 1.0) v = v + cf[k];
-                else v = v + cf[k] * p0;
-            }
-        } else {
-            const double p = q ? p1 : p0;
-            v = v + cf[k] * p;
-        }
-    });
-    return v;
-}
-
-// one face Gauss point: riemann.c:112-140 (RiemannSolverPrim) with n = e_x (DIR 0) or e_y (DIR 1)
-template <int SYS, int DIR>
-__device__ __forceinline__ double riemann_gp(const Eos &eos, const double *VL, const double *VR, double *F, double *D, bool &bad)
-{
-    using S = System<SYS>;
-    constexpr int NV = S::NV;
-    constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
-    double QL[NV], QR[NV], FL[NV], FR[NV];
-    S::prim2cons(eos, VL, QL);
-    S::prim2cons(eos, VR, QR);
-    const double sl = S::template flux<DIR>(eos, VL, FL, bad);
-    const double sr = S::template flux<DIR>(eos, VR, FR, bad);
-    const double s = (sl < sr) ? sr : sl;
-    double Vav[NV], gx[NV], gy[NV];
-#pragma unroll
-    for (int c = 0; c < NV; ++c) {
-        Vav[c] = 0.5 * (VR[c] + VL[c]);
-        gx[c] = nx * (VR[c] - VL[c]);
-        gy[c] = ny * (VR[c] - VL[c]);
-        F[c] = 0.5 * (FR[c] + FL[c] - s * (QR[c] - QL[c]));
-    }
-    S::ncp(eos, Vav, gx, gy, D);
-    return s;
-}
-
-// One tile of one grid: columns of strip `strip` (of p.strips) and rows of run
-// `run` (of p.runs).  Called by every thread of a block of K::NT threads.
-template <int SYS, int N, int CELLS_>
-__device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorMap *tmap, int strip, int run,
-                                           unsigned char *smem_raw, double *red_s)
-{
-    using K = StageKernel<SYS, N, CELLS_>;
-    using S = typename K::S;
-    using QD = typename K::QD;
-    constexpr int NV = K::NV, CELLS = K::CELLS, BW = K::BW, SLOTS = K::SLOTS, NDOF = K::NDOF;
-    constexpr int NFGP = QD::NFGP, NVGP = QD::NVGP, NNODE = QD::NNODE;
-    constexpr int NVH = (NV + 1) / 2;          // variables per half in the reconstruction
-    constexpr unsigned FULL = 0xffffffffu;
-
-    if (p.sc->done) return;
-
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
-    double *rows_s = reinterpret_cast<double *>(smem_raw + 128);
-    double *coef_s = rows_s + (size_t)SLOTS * K::SLOT_STRIDE;   // [k-1][c][cell]; later [F|D][c][cell]
-    double *yt_s = coef_s + K::COEF_ELEMS;                      // [q][c][cell]
-    double *carry_s = yt_s + K::YT_ELEMS;                       // [ncp|t1|gb|eb][c][cell]
-
-    const int t = threadIdx.x;
-    const int m = t >> 1;            // cell of this thread's pair
-    const int h = t & 1;             // which half of the pair
-    // strips split the columns evenly on even boundaries (TMA x origin alignment);
-    // row runs split the rows evenly
-    const int x0 = 2 * (int)(((long long)strip * p.nx) / (2LL * p.strips));
-    const int x1 = (strip + 1 == p.strips) ? p.nx : 2 * (int)(((long long)(strip + 1) * p.nx) / (2LL * p.strips));
-    const int owc = x1 - x0;
-    const int y0 = (int)(((long long)run * p.ny) / p.runs);
-    const int H = (int)(((long long)(run + 1) * p.ny) / p.runs) - y0;
-    if (owc > CELLS - 2 || owc < 1 || H < 1) {   // launch geometry outside what the tiling covers
-        if (threadIdx.x == 0) raise_error(p.sc, ERR_BAD_LAUNCH, 0u);
-        return;
-    }
-    const int xs = x0 - 4;                    // TMA box origin (even: x0 is even)
-    const int i = x0 - 1 + m;                 // this pair's reconstruction column
-    const bool active = m <= owc + 1;
-    const bool owned = m >= 1 && m <= owc;
-    const bool xface = m >= 1 && m <= owc + 1;
-    const bool touches_x = (x0 == 0) || (x0 + owc >= p.nx);
-    const int bcL = p.bc[0], bcR = p.bc[1], bcB = p.bc[2], bcT = p.bc[3];
-    const bool py = (bcB == BC_PERIODIC || bcT == BC_PERIODIC);
-    const double dt = (p.mode == OUT_RHS) ? 0.0 : p.sc->dt;
-    const Eos eos = p.eos;
-    const double r1_h = p.r1_h;
-
-    __syncthreads();   // the previous tile of this block is done with every buffer
-    if (t == 0) {
-        for (int s = 0; s < SLOTS; ++s) mbar_init(&bars[s], 1);
-        fence_mbar_init();
-    }
-    __syncthreads();
-
-    const int row_lo = y0 - 3, row_hi = y0 + H + 2;   // rows of state this block reads
-    int next_issue = row_lo, next_conv = row_lo;
-    auto slot_of = [&](int row) { return (row - row_lo) % SLOTS; };
-    auto row_ptr = [&](int row) { return rows_s + (size_t)slot_of(row) * K::SLOT_STRIDE; };   // [c][BW]
-    auto cidx = [&](int k1, int c, int cell) { return (k1 * NV + c) * CELLS + cell; };         // coef_s index, k1 = k-1
-    auto carry = [&](int which, int c) -> double & { return carry_s[(which * NV + c) * CELLS + m]; };
-
-    double smax_loc = 0.0;
-    bool bad = false;
-    unsigned bad_cell = 0xffffffffu;
-
-    for (int r = y0 - 1; r <= y0 + H; ++r) {
-        // ---------------- A. bring rows up to r+2 into the ring --------------
-        if (t == 0) {
-            fence_proxy_async();   // earlier generic accesses to the slots precede the TMA writes
-            for (; next_issue <= min(r + 3, row_hi); ++next_issue) {
-                const int row = next_issue;
-                const int src = map_axis(row, p.ny, bcB, bcT);
-                uint64_t *bar = &bars[slot_of(row)];
-                mbar_expect_tx(bar, K::ROW_BYTES);
-                tma_load_3d(row_ptr(row), tmap, xs, src, 0, bar);
-            }
-        }
-        for (; next_conv <= r + 2; ++next_conv) {
-            const int row = next_conv;
-            const unsigned parity = (unsigned)(((row - row_lo) / SLOTS) & 1);
-            bool ok = false;
-            for (long it = 0; it < (1L << 24); ++it) {
-                if (mbar_try_wait(&bars[slot_of(row)], parity)) { ok = true; break; }
-            }
-            if (__syncthreads_or(!ok)) {
-                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
-                return;   // block-uniform exit; the caller's next barrier is block-uniform too
-            }
-            double *rp = row_ptr(row);
-            const int src = map_axis(row, p.ny, bcB, bcT);
-            const bool yg = row < 0 || row >= p.ny;
-            const bool yrefl = yg && ((row < 0 ? bcB : bcT) == BC_REFLECTIVE);
-            // column cc = 1 + t; columns 1 .. owc+6 are the ones the stencils read
-            const int cc = 1 + t;
-            const bool conv = cc <= owc + 6;
-            const int g = xs + cc;
-            const bool isg = conv && (g < 0 || g >= p.nx);
-            double Q[NV];
-            if (touches_x) {
-                // Phase 1: ghost columns fetch their conserved source values before anyone converts
-                if (isg) {
-                    const int gm = map_axis(g, p.nx, bcL, bcR);
-                    if (gm - xs >= 0 && gm - xs < BW) {
-#pragma unroll
-                        for (int c = 0; c < NV; ++c) Q[c] = rp[c * BW + (gm - xs)];
-                    } else {
-#pragma unroll
-                        for (int c = 0; c < NV; ++c) Q[c] = p.in[(size_t)c * p.plane + (size_t)src * p.pitch + gm];
-                    }
-                }
-                __syncthreads();
-            }
-            // Phase 2: convert in place, apply reflections / inlet values
-            if (conv) {
-                if (!isg) {
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) Q[c] = rp[c * BW + cc];
-                }
-                double V[NV];
-                S::cons2prim(eos, Q, V);
-                if (isg) {
-                    const int side_bc = g < 0 ? bcL : bcR;
-                    if (side_bc == BC_INLET && p.inlet) {
-                        const int jr = py ? row : map_axis(row, p.ny, bcB, bcT);
-#pragma unroll
-                        for (int c = 0; c < NV; ++c) V[c] = p.inlet[((size_t)(g + 3) * (p.ny + 6) + (jr + 3)) * NV + c];
-                    } else if (side_bc == BC_REFLECTIVE) {
-                        if (S::RX0 >= 0) V[S::RX0] = -V[S::RX0];
-                        if (S::RX1 >= 0) V[S::RX1] = -V[S::RX1];
-                    }
-                }
-                if (yrefl) {
-                    if (S::RY0 >= 0) V[S::RY0] = -V[S::RY0];
-                    if (S::RY1 >= 0) V[S::RY1] = -V[S::RY1];
-                }
-#pragma unroll
-                for (int c = 0; c < NV; ++c) rp[c * BW + cc] = V[c];
-            }
-        }
-        __syncthreads();   // S1: prim rows r-2 .. r+2 ready
-
-        // ---------------- B. reconstruction of cell (r, i), split by variable ---
-        const int ccm = m + 3;                                    // column of i in the ring rows
-        const double *w_m2 = row_ptr(r - 2), *w_m1 = row_ptr(r - 1), *w_0 = row_ptr(r), *w_p1 = row_ptr(r + 1), *w_p2 = row_ptr(r + 2);
-        if (active) {
-#pragma unroll 1
-            for (int kv = 0; kv < NVH; ++kv) {
-                const int c = h * NVH + kv;
-                if (c >= NV) break;
-                Stencil st;
-                const double *a0 = w_0 + c * BW + ccm;
-                st.c = a0[0];
-                st.xm2 = a0[-2]; st.xm1 = a0[-1]; st.xp1 = a0[1]; st.xp2 = a0[2];
-                st.ym2 = w_m2[c * BW + ccm]; st.ym1 = w_m1[c * BW + ccm]; st.yp1 = w_p1[c * BW + ccm]; st.yp2 = w_p2[c * BW + ccm];
-                st.pp = w_p1[c * BW + ccm + 1]; st.pm = w_m1[c * BW + ccm + 1]; st.mp = w_p1[c * BW + ccm - 1]; st.mm = w_m1[c * BW + ccm - 1];
-                double cf[NDOF];
-                Recon<N>::run(st, cf);
-#pragma unroll
-                for (int k = 1; k < NDOF; ++k) coef_s[cidx(k - 1, c, m)] = cf[k];
-            }
-        }
-        __syncwarp();
-        // own coefficients of one variable of cell `cell`, k = 0 from the ring row
-        auto load_cf = [&](int c, int cell, double *cf) {
-            cf[0] = w_0[c * BW + cell + 3];
-#pragma unroll
-            for (int k = 1; k < NDOF; ++k) cf[k] = coef_s[cidx(k - 1, c, cell)];
-        };
-        // admissibility at the nodes (rhs_function_prim.c:382-404), nodes split between the pair
-        bool ok = true;
-        if (active) {
-            static_for<NNODE / 2>([&](auto sq) {
-                constexpr int s0 = decltype(sq)::value, s1 = NNODE / 2 + s0;
-                if (!ok) return;
-                double V[NV];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) {
-                    double cf[NDOF];
-                    load_cf(c, m, cf);
-                    double v = 0.0;
-                    static_for<NDOF>([&](auto kk) {
-                        constexpr int k = decltype(kk)::value;
-                        constexpr double p0 = QD::phi_node(s0, k), p1 = QD::phi_node(s1, k);
-                        if constexpr (p0 == p1) {
-                            if constexpr (p0 != 0.0) { if constexpr (p0 == 1.0) v = v + cf[k]; else v = v + cf[k] * p0; }
-                        } else {
-                            v = v + cf[k] * (h ? p1 : p0);
-                        }
-                    });
-                    V[c] = v;
-                }
-                ok = S::pad(eos, V);
-            });
-        }
-        {
-            // every lane takes part in the shuffle (no short-circuit around it)
-            const int ok_pair = __shfl_xor_sync(FULL, (int)ok, 1);
-            ok = ok && (ok_pair != 0);
-        }
-        if (!ok && N >= 2 && active) {   // rhs_function_prim.c:407-421: [w, minmod_x, minmod_y, 0 ...]
-#pragma unroll 1
-            for (int kv = 0; kv < NVH; ++kv) {
-                const int c = h * NVH + kv;
-                if (c >= NV) break;
-                const double w0 = w_0[c * BW + ccm];
-                coef_s[cidx(0, c, m)] = minmod(w_0[c * BW + ccm + 1] - w0, w0 - w_0[c * BW + ccm - 1]);
-                coef_s[cidx(1, c, m)] = minmod(w_p1[c * BW + ccm] - w0, w0 - w_m1[c * BW + ccm]);
-#pragma unroll
-                for (int k = 3; k < NDOF; ++k) coef_s[cidx(k - 1, c, m)] = 0.0;
-            }
-        }
-        __syncwarp();
-
-        // ---------------- C. y-face below (r, i): Gauss point q = h ----------------
-        const bool in_rows = r >= y0 && r <= y0 + H;
-        const int q = NFGP > 1 ? h : 0;
-        {
-            double G[NV], E[NV];
-            const bool doit = owned && in_rows;
-            double Fq[NV], Dq[NV];
-            if (doit) {
-                double VL[NV], VR[NV];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) {
-                    double cf[NDOF];
-                    load_cf(c, m, cf);
-                    VR[c] = face_val<N, 2>(cf, q);
-                    VL[c] = yt_s[(q * NV + c) * CELLS + m];
-                }
-                const double s = riemann_gp<SYS, 1>(eos, VL, VR, Fq, Dq, bad);
-                smax_loc = fmax(smax_loc, s);
-#pragma unroll
-                for (int c = 0; c < NV; ++c) { Fq[c] = QD::wf(0) * Fq[c]; Dq[c] = QD::wf(0) * Dq[c]; }
-            } else {
-#pragma unroll
-                for (int c = 0; c < NV; ++c) { Fq[c] = 0.0; Dq[c] = 0.0; }
-            }
-            // Flux = 0.0; Flux += w F(q0); Flux += w F(q1)   (rhs_function_prim.c:548-577)
-#pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if constexpr (NFGP > 1) {
-                    const double fo = __shfl_xor_sync(FULL, Fq[c], 1), d_o = __shfl_xor_sync(FULL, Dq[c], 1);
-                    const double f0 = h ? fo : Fq[c], f1 = h ? Fq[c] : fo;
-                    const double d0 = h ? d_o : Dq[c], d1 = h ? Dq[c] : d_o;
-                    G[c] = (0.0 + f0) + f1;
-                    E[c] = (0.0 + d0) + d1;
-                } else {
-                    G[c] = 0.0 + Fq[c];
-                    E[c] = 0.0 + Dq[c];
-                }
-            }
-            if (doit && bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);
-            if (doit) {
-                if (r > y0) {
-                    // row r-1: rhs = ncp + ((-1/h) X - (1/h) Y)  (rhs_function_prim.c:589-602), then the RK combination
-                    const int jo = r - 1;
-                    const size_t gidx = (size_t)jo * p.pitch + i;
-                    const double b = dt / p.kb;
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) {
-                        if ((c & 1) != h) continue;
-                        const double Y = G[c] - carry(2, c) + 0.5 * (E[c] + carry(3, c));
-                        const double ty = r1_h * Y;
-                        const double rhs = carry(0, c) + (carry(1, c) - ty);
-                        if (p.mode == OUT_RHS) {
-                            if (p.out_aos) p.out[((size_t)jo * p.nx + i) * NV + c] = rhs;
-                            else p.out[(size_t)c * p.plane + gidx] = rhs;
-                            continue;
-                        }
-                        const double Sv = p.in[(size_t)c * p.plane + gidx];
-                        const double bF = b * rhs;
-                        double o;
-                        if (p.mode == OUT_AXPY) {
-                            o = Sv + bF;
-                        } else if (p.mode == OUT_ZXS) {
-                            const double Xv = p.xn[(size_t)c * p.plane + gidx];
-                            const double s0 = p.ka * Xv + bF;
-                            o = s0 + p.kc * Sv;
-                        } else if (p.mode == OUT_ZSX) {
-                            const double Xv = p.xn[(size_t)c * p.plane + gidx];
-                            const double s0 = p.ka * Sv + bF;
-                            o = s0 + p.kc * Xv;
-                        } else {   // OUT_RK104_5
-                            const double Xv = p.xn[(size_t)c * p.plane + gidx];
-                            const double w = Sv + bF;
-                            const double w1 = (1. / 25) * Xv + (9. / 25) * w;
-                            p.out2[(size_t)c * p.plane + gidx] = w1;
-                            o = 15.0 * w1 + (-5.0) * w;
-                        }
-                        p.out[(size_t)c * p.plane + gidx] = o;
-                    }
-                }
-#pragma unroll
-                for (int c = 0; c < NV; ++c) {
-                    if ((c & 1) != h) continue;
-                    carry(2, c) = G[c];
-                    carry(3, c) = E[c];
-                }
-            }
-        }
-
-        // ---------------- D. keep the top-face values (Gauss point q) for row r+1 --
-        if (owned && r >= y0 - 1 && r < y0 + H && (NFGP > 1 || h == 0)) {
-#pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                double cf[NDOF];
-                load_cf(c, m, cf);
-                yt_s[(q * NV + c) * CELLS + m] = face_val<N, 3>(cf, q);
-            }
-        }
-
-        // ---------------- E. volume non-conservative term (rhs_function_prim.c:459-479)
-        const bool full_row = r >= y0 && r < y0 + H;
-        {
-            // rhs = 0.0; rhs += -w_q B_q for q = 0..NVGP-1; the pair holds q = 2h, 2h+1
-            constexpr int QH = NVGP > 1 ? NVGP / 2 : 1;
-            double tq[QH][NV];
-#pragma unroll
-            for (int a = 0; a < QH; ++a)
-#pragma unroll
-                for (int c = 0; c < NV; ++c) tq[a][c] = 0.0;
-            const bool doit = owned && full_row && (NVGP > 1 || h == 0);
-            if (doit) {
-                static_for<QH>([&](auto sa) {
-                    constexpr int a = decltype(sa)::value;
-                    constexpr int q0 = a, q1 = (NVGP > 1 ? QH : 0) + a;   // half 0 -> q0, half 1 -> q1
-                    double V[NV], gx[NV], gy[NV], B[NV];
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) {
-                        double cf[NDOF];
-                        load_cf(c, m, cf);
-                        double v = 0.0, dx = 0.0, dy = 0.0;
-                        static_for<NDOF>([&](auto kk) {
-                            constexpr int k = decltype(kk)::value;
-                            constexpr double pv0 = QD::phi_vol(q0, k), pv1 = QD::phi_vol(q1, k);
-                            constexpr double px0 = QD::dphi_vol_x(q0, k), px1 = QD::dphi_vol_x(q1, k);
-                            constexpr double py0 = QD::dphi_vol_y(q0, k), py1 = QD::dphi_vol_y(q1, k);
-                            if constexpr (pv0 == pv1) { if constexpr (pv0 != 0.0) { if constexpr (pv0 == 1.0) v = v + cf[k]; else v = v + cf[k] * pv0; } }
-                            else v = v + cf[k] * (h ? pv1 : pv0);
-                            if constexpr (px0 == px1) { if constexpr (px0 != 0.0) { if constexpr (px0 == 1.0) dx = dx + cf[k]; else dx = dx + cf[k] * px0; } }
-                            else dx = dx + cf[k] * (h ? px1 : px0);
-                            if constexpr (py0 == py1) { if constexpr (py0 != 0.0) { if constexpr (py0 == 1.0) dy = dy + cf[k]; else dy = dy + cf[k] * py0; } }
-                            else dy = dy + cf[k] * (h ? py1 : py0);
-                        });
-                        V[c] = v; gx[c] = r1_h * dx; gy[c] = r1_h * dy;
-                    }
-                    S::ncp(eos, V, gx, gy, B);
-#pragma unroll
-                    for (int c = 0; c < NV; ++c) tq[a][c] = -QD::wv(0) * B[c];
-                });
-            }
-            static_for<NV>([&](auto cc_) {
-                constexpr int c = decltype(cc_)::value;
-                if constexpr (!S::ncp_nonzero(c)) {
-                    // B[c] is the constant 0.0 for every Gauss point: ((0 + -0) + -0) ... = +0
-                    if (owned && full_row && (c & 1) == h) carry(0, c) = 0.0;
-                } else if constexpr (NVGP > 1) {
-                    double parts[NVGP];
-#pragma unroll
-                    for (int a = 0; a < QH; ++a) {
-                        const double o = __shfl_xor_sync(FULL, tq[a][c], 1);
-                        parts[a] = h ? o : tq[a][c];
-                        parts[QH + a] = h ? tq[a][c] : o;
-                    }
-                    double acc = 0.0;
-#pragma unroll
-                    for (int a = 0; a < NVGP; ++a) acc += parts[a];
-                    if (owned && full_row && (c & 1) == h) carry(0, c) = acc;
-                } else {
-                    const double o = __shfl_xor_sync(FULL, tq[0][c], 1);
-                    const double acc = 0.0 + (h ? o : tq[0][c]);
-                    if (owned && full_row && (c & 1) == h) carry(0, c) = acc;
-                }
-            });
-        }
-        __syncthreads();   // S2: every column's coefficients of row r visible
-
-        // ---------------- F. x-face at the left of column i: Gauss point q ----------
-        double Fx[NV], Dx[NV];
-        {
-            const bool doit = xface && full_row;
-            double Fq[NV], Dq[NV];
-            if (doit) {
-                double VL[NV], VR[NV];
-#pragma unroll
-                for (int c = 0; c < NV; ++c) {
-                    double cl[NDOF], cr[NDOF];
-                    load_cf(c, m - 1, cl);
-                    load_cf(c, m, cr);
-                    VL[c] = face_val<N, 1>(cl, q);
-                    VR[c] = face_val<N, 0>(cr, q);
-                }
-                const double s = riemann_gp<SYS, 0>(eos, VL, VR, Fq, Dq, bad);
-                smax_loc = fmax(smax_loc, s);
-#pragma unroll
-                for (int c = 0; c < NV; ++c) { Fq[c] = QD::wf(0) * Fq[c]; Dq[c] = QD::wf(0) * Dq[c]; }
-                if (bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);
-            } else {
-#pragma unroll
-                for (int c = 0; c < NV; ++c) { Fq[c] = 0.0; Dq[c] = 0.0; }
-            }
-#pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if constexpr (NFGP > 1) {
-                    const double fo = __shfl_xor_sync(FULL, Fq[c], 1), d_o = __shfl_xor_sync(FULL, Dq[c], 1);
-                    const double f0 = h ? fo : Fq[c], f1 = h ? Fq[c] : fo;
-                    const double d0 = h ? d_o : Dq[c], d1 = h ? Dq[c] : d_o;
-                    Fx[c] = (0.0 + f0) + f1;
-                    Dx[c] = (0.0 + d0) + d1;
-                } else {
-                    Fx[c] = 0.0 + Fq[c];
-                    Dx[c] = 0.0 + Dq[c];
-                }
-            }
-        }
-        __syncthreads();   // S3: coefficient reads done; the buffer now carries face fluxes
-        if (xface && full_row) {
-#pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if ((c & 1) != h) continue;
-                coef_s[c * CELLS + m] = Fx[c];
-                coef_s[(NV + c) * CELLS + m] = Dx[c];
-            }
-        }
-        __syncthreads();   // S4
-        if (owned && full_row) {
-#pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if ((c & 1) != h) continue;
-                const double F1 = coef_s[c * CELLS + m + 1], D1 = coef_s[(NV + c) * CELLS + m + 1];
-                const double X = F1 - Fx[c] + 0.5 * (D1 + Dx[c]);
-                carry(1, c) = -r1_h * X;
-            }
-        }
-    }
-
-    // ---------------- CFL maximum: warp shuffle, block, one atomic ------------
-    if (bad) raise_error(p.sc, ERR_INADMISSIBLE_FACE, bad_cell);
-    __syncthreads();   // red_s is reused tile after tile
-    if (p.reduce_smax) {
-        double mx = smax_loc;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(FULL, mx, o));
-        if ((t & 31) == 0) red_s[t >> 5] = mx;
-        __syncthreads();
-        if (t == 0) {
-            double b = red_s[0];
-#pragma unroll
-            for (int w = 1; w < K::NT / 32; ++w) b = fmax(b, red_s[w]);
-            if (b > 0.0) atomicMax(&p.sc->smax, (unsigned long long)__double_as_longlong(b));
-        }
-    }
-    for (int k = t; k < SLOTS; k += K::NT) mbar_inval(&bars[k]);
-}
 
 template <int SYS, int N, int CELLS>
 __global__ void __launch_bounds__(2 * CELLS, (StageKernel<SYS, N, CELLS>::MIN_BLOCKS))
@@ -565,7 +18,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    stage_tile<SYS, N, CELLS>(p, &tmap, blockIdx.x, blockIdx.y, smem_raw, red_s);
+    stage_tile<SYS, N, CELLS, false>(p, &tmap, blockIdx.x, blockIdx.y, smem_raw, red_s);
 }
 
 // Persistent form: the block walks a list of (grid, tile) work items; every grid
@@ -592,7 +45,7 @@ stage_batch_kernel(const StageParams *__restrict__ inst, const CUtensorMap *__re
             fence_tensormap_acquire(&tmaps[it.x]);
         }
         __syncthreads();
-        stage_tile<SYS, N, CELLS>(p_s, &tmaps[it.x], it.y % p_s.strips, it.y / p_s.strips, smem_raw, red_s);
+        stage_tile<SYS, N, CELLS, false>(p_s, &tmaps[it.x], it.y % p_s.strips, it.y / p_s.strips, smem_raw, red_s);
         last = p_s.sc;
     }
     work_finish(sched);

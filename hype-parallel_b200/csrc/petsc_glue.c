@@ -1,15 +1,19 @@
 /*
- * petsc_glue.c -- RHSFunctionPrim with the reference's PETSc signature,
- * forwarding to the C ABI of include/hype_gpu.h.
+ * petsc_glue.c -- RHSFunctionPrim and RHSFunction with the reference's PETSc
+ * signatures, forwarding to the C ABI of include/hype_gpu.h.
  *
- * It replaces HyPE-2D/rhs_function_prim.c in a HyPE-2D build: compile it in
+ * It replaces HyPE-2D/rhs_function_prim.c and rhs_function.c in a HyPE-2D
+ * build (RHSFunction: the conservative-variable path that hype.c selects when
+ * Ctx.ReconsPrimitive is false, hype.c:341-352): compile it in
  * that tree (it includes the tree's hype.h for AppCtx, the PDE-system #define
  * and the EOS constants GAMMA_1, GAMMA_2, PI_1, PI_2, and the tree's PETSc),
  * link libhype_b200.so, and hype.c's
  *     TSSetRHSFunction(ts, NULL, RHSFunctionPrim, &Ctx);       (hype.c:344)
- * and its direct dt-seeding call (hype.c:343) reach the B200 kernels.
+ *     TSSetRHSFunction(ts, NULL, RHSFunction, &Ctx);           (hype.c:351)
+ * and its direct dt-seeding calls (hype.c:343, 350) reach the B200 kernels.
  *
- * Contract kept from rhs_function_prim.c:12-626 / hype.h:306:
+ * Contract kept from rhs_function_prim.c:12-626 / rhs_function.c:12-625 /
+ * hype.h:305-306:
  *   - RHS is overwritten for every owned cell; U is not modified;
  *   - Ctx->dt is set to CFL*h/(2*s_max) (rhs_function_prim.c:617-623);
  *   - the scratch of AppCtx (W, localU, u_bnd, F, G, D, E) is not touched:
@@ -31,8 +35,9 @@
 #include "hype.h"
 #include "hype_gpu.h"
 
-static hype_solver *glue_solver = NULL;
-static hype_config glue_cfg;
+/* one GPU solver per path: [0] primitive, [1] conservative reconstruction */
+static hype_solver *glue_solver[2] = {NULL, NULL};
+static hype_config glue_cfg[2];
 
 static int glue_system(void)
 {
@@ -47,7 +52,7 @@ static int glue_system(void)
 
 /* AppCtx (hype.h:203-252) and the compile-time constants -> hype_config.
  * enum bndry_type (hype.h:76) and HYPE_BC_* have the same values. */
-static void glue_config(const AppCtx *Ctx, hype_config *c)
+static void glue_config(const AppCtx *Ctx, int conservative, hype_config *c)
 {
     const char *dev = getenv("HYPE_DEVICE");
     hype_config_default(c);
@@ -65,39 +70,41 @@ static void glue_config(const AppCtx *Ctx, hype_config *c)
     c->gamma1 = GAMMA_1; c->gamma2 = GAMMA_2;
     c->pi1 = PI_1; c->pi2 = PI_2;
     c->precision = HYPE_PREC_FP64;
+    c->flags = conservative ? HYPE_FLAG_CONSERVATIVE : 0u;
     c->device = dev ? atoi(dev) : 0;
 }
 
-/* Frees the GPU solver (e.g. from the application's clean-up, hype.c:421-451). */
+/* Frees the GPU solvers (e.g. from the application's clean-up, hype.c:421-451). */
 void RHSFunctionPrimFinalize(void)
 {
-    hype_destroy(glue_solver);
-    glue_solver = NULL;
+    for (int k = 0; k < 2; ++k) {
+        hype_destroy(glue_solver[k]);
+        glue_solver[k] = NULL;
+    }
 }
 
-PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
+static PetscErrorCode glue_rhs(int conservative, PetscReal t, Vec U, Vec RHS, AppCtx *Ctx)
 {
-    AppCtx *Ctx = (AppCtx *)ctx;
     int size = 1;
-    (void)ts;
     MPI_Comm_size(PETSC_COMM_WORLD, &size);
     if (size != 1) {
-        fprintf(stderr, "RHSFunctionPrim (GPU): one MPI rank only, got %d\n", size);
+        fprintf(stderr, "RHSFunction (GPU): one MPI rank only, got %d\n", size);
         return 1;
     }
     hype_config c;
-    glue_config(Ctx, &c);
-    if (!glue_solver || memcmp(&c, &glue_cfg, sizeof(c)) != 0) {
-        RHSFunctionPrimFinalize();
+    glue_config(Ctx, conservative, &c);
+    if (!glue_solver[conservative] || memcmp(&c, &glue_cfg[conservative], sizeof(c)) != 0) {
+        hype_destroy(glue_solver[conservative]);
+        glue_solver[conservative] = NULL;
         hype_solver *s = NULL;
         const int st = hype_create(&c, &s);
         if (st != HYPE_OK) {
-            fprintf(stderr, "RHSFunctionPrim (GPU): %s\n", s ? hype_last_error(s) : hype_status_string(st));
+            fprintf(stderr, "RHSFunction (GPU): %s\n", s ? hype_last_error(s) : hype_status_string(st));
             hype_destroy(s);
             return (PetscErrorCode)st;
         }
-        glue_solver = s;
-        glue_cfg = c;
+        glue_solver[conservative] = s;
+        glue_cfg[conservative] = c;
     }
     const PetscScalar *u = NULL;
     PetscScalar *r = NULL;
@@ -106,13 +113,25 @@ PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
     ierr = VecGetArray(RHS, &r);
     if (ierr) { VecRestoreArrayRead(U, &u); return ierr; }
     double dt = 0.0;
-    const int st = hype_rhs_prim(glue_solver, (double)t, (const double *)u, (double *)r, &dt);
+    const int st = hype_rhs_prim(glue_solver[conservative], (double)t, (const double *)u, (double *)r, &dt);
     VecRestoreArray(RHS, &r);
     VecRestoreArrayRead(U, &u);
     if (st != HYPE_OK) {
-        fprintf(stderr, "RHSFunctionPrim (GPU): %s\n", hype_last_error(glue_solver));
+        fprintf(stderr, "RHSFunction (GPU): %s\n", hype_last_error(glue_solver[conservative]));
         return (PetscErrorCode)st;
     }
-    Ctx->dt = dt;   /* rhs_function_prim.c:623 */
+    Ctx->dt = dt;   /* rhs_function_prim.c:623, rhs_function.c:622 */
     return 0;
+}
+
+PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
+{
+    (void)ts;
+    return glue_rhs(0, t, U, RHS, (AppCtx *)ctx);
+}
+
+PetscErrorCode RHSFunction(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
+{
+    (void)ts;
+    return glue_rhs(1, t, U, RHS, (AppCtx *)ctx);
 }

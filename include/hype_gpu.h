@@ -62,6 +62,10 @@ extern "C" {
 /* ---- flags --------------------------------------------------------------- */
 #define HYPE_FLAG_BN_FIX_P2   1u  /* Baer-Nunziato: take the phase-2 flux pressure from V[7]
                                      instead of V[8] (baer_nunziato.c:271 reads alpha_1)   */
+#define HYPE_FLAG_CONSERVATIVE 2u /* reconstruct conserved variables: the RHS is HyPE-2D's
+                                     RHSFunction (rhs_function.c:12-625), which hype.c uses
+                                     when Ctx.ReconsPrimitive is false (hype.c:341-352).
+                                     FP64 solvers only (not mixed, batch or no-alloc).      */
 
 /*
  * Run-time form of the reference's compile-time and AppCtx parameters:

@@ -26,7 +26,8 @@ def to_pkg(cfg: O.Config) -> "hp.Config":
     return hp.Config(system=cfg.system, order=cfg.order, nx=cfg.nx, ny=cfg.ny, x_min=cfg.x_min, x_max=cfg.x_max,
                      y_min=cfg.y_min, y_max=cfg.y_max, cfl=cfg.cfl, bc_left=cfg.bc_left, bc_right=cfg.bc_right,
                      bc_bottom=cfg.bc_bottom, bc_top=cfg.bc_top, gamma1=cfg.gamma1, gamma2=cfg.gamma2, pi1=cfg.pi1,
-                     pi2=cfg.pi2, precision=hp.PREC_FP64, flags=hp.FLAG_BN_FIX_P2 if cfg.bn_fixed_p2 else 0)
+                     pi2=cfg.pi2, precision=hp.PREC_FP64,
+                     flags=(hp.FLAG_BN_FIX_P2 if cfg.bn_fixed_p2 else 0) | (hp.FLAG_CONSERVATIVE if cfg.conservative else 0))
 
 
 def kapila_rough(cfg: O.Config, seed: int) -> np.ndarray:
@@ -111,6 +112,21 @@ RHS_CASES = [
     _b("bn_23x19_fixed_p2", 23, 19, fixed=1, bcs=(R, T, R, T), seed=1),
     _b("bn_13x21_periodic_N1", 13, 21, order=1, bcs=(P, P, R, R), seed=2),
     _b("bn_12x10_N3", 12, 10, order=3, seed=3),
+    # conservative-variable path (RHSFunction, rhs_function.c)
+    _k("kapila_cons_24x20_bubble", 24, 20, bcs=(T, T, R, R), seed=20, conservative=1),
+    _k("kapila_cons_37x23_rough", 37, 23, bcs=(R, T, R, R), kind="rough", seed=21, conservative=1),
+    _k("kapila_cons_18x14_inlet", 18, 14, bcs=(I, T, R, R), kind="rough", seed=22, x_min=0.0, x_max=2.0, y_min=-1.0,
+       y_max=0.5556, conservative=1),
+    _k("kapila_cons_19x17_N1", 19, 17, order=1, kind="rough", seed=23, conservative=1),
+    _k("kapila_cons_15x13_N3", 15, 13, order=3, bcs=(R, T, P, P), seed=24, conservative=1),
+    _k("kapila_cons_11x10_N0", 11, 10, order=0, seed=25, conservative=1),
+    _k("kapila_cons_251x7_three_strips", 251, 7, bcs=(R, R, T, T), seed=26, conservative=1),
+    _e("euler_cons_21x19_reflective", 21, 19, bcs=(R, R, R, R), seed=27, conservative=1),
+    _e("euler_cons_17x12_periodic_N3", 17, 12, order=3, bcs=(P, P, P, P), seed=28, conservative=1),
+    _e("euler_cons_16x16_N1", 16, 16, order=1, seed=29, conservative=1),
+    _b("bn_cons_16x16", 16, 16, seed=30, conservative=1),
+    _b("bn_cons_13x21_periodic_N1", 13, 21, order=1, bcs=(P, P, R, R), seed=31, conservative=1),
+    _b("bn_cons_12x10_N3", 12, 10, order=3, bcs=(R, R, T, T), seed=32, conservative=1),
 ]
 
 # Multi-step solve cases (hype.c time loop)
@@ -121,6 +137,9 @@ SOLVE_CASES = [
     (_k("kapila_16x16_solve_N3", 16, 16, order=3, bcs=(P, P, P, P), seed=14), 0.0, 1.0, 3),
     (_e("euler_32x24_solve", 32, 24, bcs=(T, T, R, R), seed=15), 0.0, 0.05, 1000),
     (_b("bn_20x20_solve", 20, 20, seed=16), 0.0, 1.0, 4),
+    (_k("kapila_cons_32x32_solve", 32, 32, seed=33, conservative=1), 0.0, 1.0, 8),
+    (_e("euler_cons_32x24_solve", 32, 24, bcs=(T, T, R, R), seed=34, conservative=1), 0.0, 0.05, 1000),
+    (_b("bn_cons_20x20_solve", 20, 20, bcs=(R, R, R, R), seed=35, conservative=1), 0.0, 1.0, 4),
 ]
 
 

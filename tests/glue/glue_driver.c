@@ -12,11 +12,12 @@
 PetscReal GAMMA_1 = 1.4, GAMMA_2 = 1.4, PI_1 = 0.0, PI_2 = 0.0;
 
 PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx);
+PetscErrorCode RHSFunction(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx);
 void RHSFunctionPrimFinalize(void);
 
 int glue_nvar(void) { return nVar; }
 
-int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int bc[4], const double eos[4],
+int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int bc[4], const double eos[4], int conservative,
              const double *Uin, double *Rout, double *dt)
 {
     GAMMA_1 = eos[0]; GAMMA_2 = eos[1]; PI_1 = eos[2]; PI_2 = eos[3];
@@ -28,7 +29,7 @@ int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int b
     Ctx.h = (Ctx.x_max - Ctx.x_min) / (PetscReal)Ctx.N_x;
     Ctx.LeftBoundary = (enum bndry_type)bc[0]; Ctx.RightBoundary = (enum bndry_type)bc[1];
     Ctx.BottomBoundary = (enum bndry_type)bc[2]; Ctx.TopBoundary = (enum bndry_type)bc[3];
-    Ctx.ReconsPrimitive = PETSC_TRUE;
+    Ctx.ReconsPrimitive = conservative ? PETSC_FALSE : PETSC_TRUE;
     const DMBoundaryType bx = (bc[0] == periodic || bc[1] == periodic) ? DM_BOUNDARY_PERIODIC : DM_BOUNDARY_GHOSTED;
     const DMBoundaryType by = (bc[2] == periodic || bc[3] == periodic) ? DM_BOUNDARY_PERIODIC : DM_BOUNDARY_GHOSTED;
     DM da;
@@ -44,7 +45,8 @@ int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int b
     TS ts;
     TSCreate(PETSC_COMM_WORLD, &ts);
     TSSetDM(ts, da);
-    const PetscErrorCode ierr = RHSFunctionPrim(ts, 0.0, U, R, &Ctx);
+    /* hype.c:341-352: ReconsPrimitive picks the RHS function */
+    const PetscErrorCode ierr = Ctx.ReconsPrimitive ? RHSFunctionPrim(ts, 0.0, U, R, &Ctx) : RHSFunction(ts, 0.0, U, R, &Ctx);
     VecGetArray(R, &a);
     memcpy(Rout, a, sizeof(double) * (size_t)nx * ny * nVar);
     VecRestoreArray(R, &a);

@@ -43,6 +43,12 @@ def main():
             # the reference has only the shipped flux; the fixed variant is pinned to the oracle with one line changed
             R, dt, st = O.Oracle().rhs(cfg, U)
             src = "oracle(bn_fixed_p2)"
+        elif cfg.conservative and cfg.order == 0:
+            # rhs_function.c:412-414 writes sol[1], sol[2] of a 1-row array (nDOF = 1) whenever PDECheckPAD
+            # fails -- for Kapila at every cell (kapila_5eqn.c:278) -- and the reference crashes; the
+            # oracle's reading (the fallback leaves the cell mean) is the defined behaviour kept here
+            R, dt, st = O.Oracle().rhs(cfg, U)
+            src = "oracle(conservative N=0: reference writes past nDOF)"
         else:
             ref = refs[cfg.system]
             ref.setup(cfg)

@@ -67,6 +67,29 @@ def test_solve_bitwise(name, hp, orc):
         pytest.fail(f"final state differs: {describe_diff(Ue, Uo, cfg.nvar)}")
 
 
+@pytest.mark.parametrize("seed", range(3))
+def test_rhs_fresh_seeds_conservative_vs_oracle(seed, hp, orc):
+    """RHSFunction (conservative reconstruction) on random sizes, orders and boundaries."""
+    rng = np.random.default_rng(2000 + seed)
+    for system, kind in ((O.KAPILA, "rough"), (O.KAPILA, "bubble"), (O.BN, "discs"), (O.EULER, "quadrants")):
+        nx, ny = int(rng.integers(3, 300)), int(rng.integers(3, 40))
+        order = int(rng.integers(0, 4))
+        bcs = [int(b) for b in rng.choice([O.TRANSMISSIVE, O.REFLECTIVE], 4)]
+        if rng.uniform() < 0.3:
+            bcs[0] = bcs[1] = O.PERIODIC
+        eos = cases.EULER_EOS if system == O.EULER else cases.KAPILA_EOS
+        cfg = O.Config(system=system, order=order, nx=nx, ny=ny, bc_left=bcs[0], bc_right=bcs[1], bc_bottom=bcs[2],
+                       bc_top=bcs[3], conservative=1, **eos)
+        U = cases.state(cfg, kind, seed)
+        Ro, dto, sto = orc.rhs(cfg, U)
+        with hp.Solver(cases.to_pkg(cfg)) as s:
+            R, dt, st = s.rhs_function_prim(0.0, U)
+        assert (st == hp.OK) == (sto == O.OK), (system, nx, ny, order, bcs)
+        if sto == O.OK:
+            assert dt == dto
+            assert R.tobytes() == Ro.tobytes(), describe_diff(R, Ro, cfg.nvar)
+
+
 @pytest.mark.parametrize("seed", range(4))
 def test_rhs_fresh_seeds_vs_oracle(seed, hp, orc):
     rng = np.random.default_rng(1000 + seed)

@@ -29,7 +29,7 @@ def glue_libs(hp):
         L = ctypes.CDLL(os.path.join(GLUE, "_build", f"libglue_{nm}.so"))
         DP = ctypes.POINTER(ctypes.c_double)
         IP = ctypes.POINTER(ctypes.c_int)
-        L.glue_rhs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, ctypes.c_double, IP, DP, DP, DP, DP]
+        L.glue_rhs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, ctypes.c_double, IP, DP, ctypes.c_int, DP, DP, DP]
         L.glue_rhs.restype = ctypes.c_int
         libs[sysid] = L
     return libs
@@ -42,14 +42,14 @@ def glue_rhs(L, cfg, U):
     R = np.empty_like(U)
     dt = ctypes.c_double(0.0)
     DP = ctypes.POINTER(ctypes.c_double)
-    st = L.glue_rhs(cfg.order, cfg.nx, cfg.ny, dom, cfg.cfl, bc, eos, U.ctypes.data_as(DP), R.ctypes.data_as(DP),
-                    ctypes.byref(dt))
+    st = L.glue_rhs(cfg.order, cfg.nx, cfg.ny, dom, cfg.cfl, bc, eos, cfg.conservative, U.ctypes.data_as(DP),
+                    R.ctypes.data_as(DP), ctypes.byref(dt))
     return R, dt.value, st
 
 
 def test_glue_builds_and_exports_the_reference_signature(glue_libs):
     for L in glue_libs.values():
-        assert L.RHSFunctionPrim is not None and L.RHSFunctionPrimFinalize is not None
+        assert L.RHSFunctionPrim is not None and L.RHSFunction is not None and L.RHSFunctionPrimFinalize is not None
 
 
 def test_glue_without_gpu_returns_an_error(hp, glue_libs):
@@ -62,7 +62,9 @@ def test_glue_without_gpu_returns_an_error(hp, glue_libs):
 
 
 GLUE_CASES = ["kapila_37x23_rough_mixed_bc", "kapila_18x14_inlet", "kapila_15x13_N3", "euler_21x19_reflective_N1",
-              "bn_16x16", "bn_13x21_periodic_N1"]
+              "bn_16x16", "bn_13x21_periodic_N1",
+              # RHSFunction (Ctx.ReconsPrimitive false)
+              "kapila_cons_37x23_rough", "kapila_cons_18x14_inlet", "euler_cons_17x12_periodic_N3", "bn_cons_12x10_N3"]
 
 
 @pytest.mark.gpu
