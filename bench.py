@@ -302,6 +302,36 @@ def batch_leg(hp, args, local_rank):
             "mixed_vs_fp64_max_rel_L1": {"rho": err_rho, "alpha1": err_a}}
 
 
+def bn_leg(hp, args, local_rank):
+    """Baer-Nunziato 1024 x 1024, FP64, N = 2, 200 SSPRK(4,3) steps on the seeded
+    disc state (alpha_1 from 8 tanh discs, Fourier velocities |u| <= 50,
+    p in [1e5, 1e7]; stiffened gases 4.4/6e8 and 1.4/0), in both flux forms:
+    as the reference writes it (phase-2 flux pressure V[8]) and fixed (V[7])."""
+    out = {}
+    n = 1024
+    for name, flags in (("reference_form", 0), ("fixed_p2", hp.FLAG_BN_FIX_P2)):
+        cfg = hp.Config(system=hp.BAER_NUNZIATO, order=2, nx=n, ny=n, cfl=0.4, device=local_rank, flags=flags)
+        U0 = hp.initial_state(cfg, "bn_discs", seed=SEED)
+        with hp.Solver(cfg) as s:
+            s.set_state(U0)
+            tile = s.autotune(3) if not args.no_autotune else None
+            s.begin(0.0, 1e30, 200)
+            s.advance(200)
+            steps, t, dtn, st = s.wait()
+            ms = s.last_elapsed_ms()
+            ms_stage = s.time_stage(10)
+            tot, amin, amax = s.totals()
+        out[name] = {"steps_done": steps, "status": st, "t_end": t,
+                     "value": n * n * steps / (ms * 1e-3) if steps else None, "unit": UNIT,
+                     "ms_per_step": ms / steps if steps else None, "stage_ms_per_launch": ms_stage,
+                     "stage_roofline_GBs": (2 * 9 * 8) * n * n / (ms_stage * 1e-3) / 1e9, "autotuned_tile": tile,
+                     "alpha_min": amin, "alpha_max": amax}
+    out["workload"] = "bn9 discs 1024x1024 fp64, N=2 SSPRK(4,3), 200 steps"
+    out["note"] = ("the reference's flux form stops where the reference would MPI_Abort (inadmissible face state); "
+                   "steps after the stop are skipped on the device, so its value counts the steps taken")
+    return out
+
+
 def serve_leg(hp, args, local_rank, capacity):
     """Serving: a Poisson stream of solve requests through the C request loop
     (hype_serve_run) -- 70/20/10 Kapila / Baer-Nunziato / Euler, square grids
@@ -332,13 +362,15 @@ def serve_leg(hp, args, local_rank, capacity):
         reqs.append(hp.Request(0.0, cfg, 0.0, 1e30, steps, ic, 5000 + i, par))
         work.append(side * side * steps)
     rho = float(rng.uniform(0.5, 0.8))
+    if args.serve_load is not None:
+        rho = args.serve_load
     rate = rho * capacity / float(np.mean(work))
     t = 0.0
     for r in reqs:
         r.arrival_s = t
         t += float(rng.exponential(1.0 / rate))
     res, st = hp.serve(reqs, device=local_rank, hbm_budget=150 * 10 ** 9, max_instances=1024, max_cells=2048 * 2048,
-                       poll_ms=args.serve_poll_ms, realtime=True)
+                       poll_ms=args.serve_poll_ms, realtime=True, active_cells=args.serve_active_cells)
     lat = np.array([r["latency_s"] for r in res])
     by_sys = {}
     for nm, sysid in (("kapila", hp.KAPILA_5EQN), ("bn", hp.BAER_NUNZIATO), ("euler", hp.EULER)):
@@ -348,7 +380,7 @@ def serve_leg(hp, args, local_rank, capacity):
                           "p99_s": float(np.percentile(lat[sel], 99))}
     return {"workload": f"Poisson stream of {n} solves: 70/20/10 kapila5/bn/euler, square grids 64..2048 log-uniform, "
                         "50..2000 steps log-uniform, N=2 SSPRK(4,3), 150 GB HBM budget",
-            "requests": n, "kapila_precision": args.serve_kapila, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
+            "requests": n, "kapila_precision": args.serve_kapila, "active_cells": args.serve_active_cells, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
             "offered_cell_updates": float(np.sum(work)),
             "p50_s": st["p50_s"], "p90_s": st["p90_s"], "p99_s": st["p99_s"], "max_s": st["max_s"], "mean_s": st["mean_s"],
             "queue_p50_s": st["queue_p50_s"], "queue_p99_s": st["queue_p99_s"],
@@ -458,6 +490,7 @@ def run_gpu(args, rank, world, local_rank):
                  "rel_error_vs_fp64_after_run": {"fields_L1_Linf": errs, "steps": args.steps + max(3, args.warmup)},
                  "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt"}
 
+    bn = None if args.no_bn else bn_leg(hp, args, local_rank)
     batched = None if args.no_batch else batch_leg(hp, args, local_rank)
     capacity = batched["batched_mixed"]["value"] if batched else 5e8
     serving = None if args.serve_requests <= 0 else serve_leg(hp, args, local_rank, capacity)
@@ -481,7 +514,7 @@ def run_gpu(args, rank, world, local_rank):
             "gpu_launches": args.steps * 6,
             "clocks": clk.summary(),
             "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2},
-            "forms": {"mixed": mixed, "batched": batched, "serving": serving}}
+            "forms": {"mixed": mixed, "bn1024": bn, "batched": batched, "serving": serving}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -497,10 +530,14 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default stage tile shape")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-grids leg")
+    ap.add_argument("--no-bn", action="store_true", help="skip the Baer-Nunziato 1024^2 leg")
     ap.add_argument("--batch-steps", type=int, default=300, help="steps of the batched-grids leg")
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serve-kapila", default="mixed", choices=["mixed", "fp64"], help="precision of Kapila requests")
     ap.add_argument("--serve-poll-ms", type=float, default=10.0)
+    ap.add_argument("--serve-active-cells", type=int, default=8 << 20,
+                    help="scheduler: cells stepped at once, least remaining work first (0: all resident requests)")
+    ap.add_argument("--serve-load", type=float, default=None, help="load factor of the arrival rate (default: seed-drawn)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -88,7 +88,7 @@ class _BatchCfg(ctypes.Structure):
 
 class _InstStatus(ctypes.Structure):
     _fields_ = [("active", ctypes.c_int), ("done", ctypes.c_int), ("steps", ctypes.c_int), ("status", ctypes.c_int),
-                ("t", ctypes.c_double), ("dt_next", ctypes.c_double)]
+                ("t", ctypes.c_double), ("dt_next", ctypes.c_double), ("held", ctypes.c_int)]
 
 
 class _Request(ctypes.Structure):
@@ -104,7 +104,7 @@ class _Result(ctypes.Structure):
 class _ServeCfg(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_instances", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
                 ("max_cells", ctypes.c_longlong), ("poll_ms", ctypes.c_double), ("realtime", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("fetch_results", ctypes.c_int)]
+                ("autotune", ctypes.c_int), ("fetch_results", ctypes.c_int), ("active_cells", ctypes.c_longlong)]
 
 
 class _ServeStats(ctypes.Structure):
@@ -177,6 +177,7 @@ def lib() -> ctypes.CDLL:
         L.hype_batch_sync.argtypes = [vp]
         L.hype_batch_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(_InstStatus)]
         L.hype_batch_get_state.argtypes = [vp, ctypes.c_int, _DP]
+        L.hype_batch_hold.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.hype_batch_set_tiling.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.hype_batch_autotune.argtypes = [vp, ctypes.c_int, IP, IP]
         L.hype_batch_info.argtypes = [vp, IP, IP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
@@ -422,6 +423,9 @@ class Batch:
         self._check(lib().hype_batch_status(self._h, i, ctypes.byref(s)))
         return {f: getattr(s, f) for f, _ in _InstStatus._fields_}
 
+    def hold(self, i: int, hold: bool = True) -> None:
+        self._check(lib().hype_batch_hold(self._h, i, int(hold)))
+
     def get_state(self, i: int) -> np.ndarray:
         c = self.cfgs[i]
         U = np.empty(c.nx * c.ny * c.nvar, dtype=np.float64)
@@ -468,7 +472,7 @@ class Request:
 
 def serve(requests, *, device: int = 0, max_instances: int = 256, hbm_budget: int = 0, max_cells: int = 2048 * 2048,
           poll_ms: float = 10.0, realtime: bool = True, autotune: bool = True, fetch_results: bool = True,
-          fill=None, sink=None):
+          active_cells: int | None = None, fill=None, sink=None):
     """Runs hype_serve_run over ``requests`` (sorted by arrival).
 
     fill(index, U0) fills the initial state of IC_CALLBACK requests in place;
@@ -486,6 +490,8 @@ def serve(requests, *, device: int = 0, max_instances: int = 256, hbm_budget: in
     L.hype_serve_config_default(ctypes.byref(c))
     c.device, c.max_instances, c.hbm_budget, c.max_cells = device, max_instances, hbm_budget, max_cells
     c.poll_ms, c.realtime, c.autotune, c.fetch_results = poll_ms, int(realtime), int(autotune), int(fetch_results)
+    if active_cells is not None:
+        c.active_cells = active_cells
 
     def _fill(_ctx, i, _req, U):
         try:

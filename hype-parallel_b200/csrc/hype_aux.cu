@@ -76,10 +76,15 @@ __global__ void seed_dt_kernel(DevScalars *sc, double cfl_h)
 // Start of a step: the monitor hands TS the last RHS's dt; TS stops at
 // max_steps or t_final and clips the last step to land on t_final (MATCHSTEP).
 // A run whose RHS raised an error stops there (the reference aborts the job).
+// A finished or held run sits this step out: `idle` tells the stages and
+// end_step to leave it untouched.
 __device__ __forceinline__ void begin_step(DevScalars *sc)
 {
+    sc->idle = 1;
     if (sc->done) return;
     if (sc->err || sc->steps >= sc->max_steps || sc->t >= sc->t_final) { sc->done = 1; return; }
+    if (sc->hold) return;
+    sc->idle = 0;
     double dt = sc->time_step;
     if (sc->t + dt > sc->t_final) dt = sc->t_final - sc->t;
     sc->dt = dt;
@@ -89,7 +94,7 @@ __device__ __forceinline__ void begin_step(DevScalars *sc)
 // End of a step: the last stage's RHS set Ctx->dt for the next step.
 __device__ __forceinline__ void end_step(DevScalars *sc, double cfl_h)
 {
-    if (sc->done) return;
+    if (sc->idle) return;
     const double smax = __longlong_as_double((long long)sc->smax);
     sc->time_step = cfl_h / (2.0 * smax);
     sc->t = sc->t + sc->dt;
@@ -99,10 +104,13 @@ __device__ __forceinline__ void end_step(DevScalars *sc, double cfl_h)
 __global__ void begin_step_kernel(DevScalars *sc) { begin_step(sc); }
 __global__ void end_step_kernel(DevScalars *sc, double cfl_h) { end_step(sc, cfl_h); }
 
-__global__ void begin_step_batch_kernel(DevScalars *sc, const int *members)
+__global__ void begin_step_batch_kernel(DevScalars *sc, const int *members, const int *hold)
 {
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < members[0]; k += gridDim.x * blockDim.x)
-        begin_step(&sc[members[1 + k]]);
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < members[0]; k += gridDim.x * blockDim.x) {
+        const int m = members[1 + k];
+        sc[m].hold = hold[m];
+        begin_step(&sc[m]);
+    }
 }
 __global__ void end_step_batch_kernel(DevScalars *sc, const int *members)
 {
@@ -111,13 +119,13 @@ __global__ void end_step_batch_kernel(DevScalars *sc, const int *members)
         end_step(p, p->cfl_h);
     }
 }
-// one block per member; skipped for finished instances like the stages
+// one block per member; skipped for idle instances like the stages
 __global__ void copy_batch_kernel(double *const *dst, const double *const *src, const long long *n, const int *members,
                                   const DevScalars *sc)
 {
     for (int k = blockIdx.x; k < members[0]; k += gridDim.x) {
         const int m = members[1 + k];
-        if (sc[m].done) continue;
+        if (sc[m].idle) continue;
         const double2 *a = reinterpret_cast<const double2 *>(src[m]);
         double2 *b = reinterpret_cast<double2 *>(dst[m]);
         for (long long i = threadIdx.x; i < n[m] / 2; i += blockDim.x) b[i] = a[i];
@@ -141,9 +149,9 @@ cudaError_t launch_end_step(DevScalars *sc, double cfl_h, cudaStream_t s)
     return cudaGetLastError();
 }
 static unsigned member_blocks(int max_members, int per_block) { return (unsigned)((max_members + per_block - 1) / per_block > 0 ? (max_members + per_block - 1) / per_block : 1); }
-cudaError_t launch_begin_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s)
+cudaError_t launch_begin_step_batch(DevScalars *sc, const int *members, const int *hold, int max_members, cudaStream_t s)
 {
-    begin_step_batch_kernel<<<member_blocks(max_members, 128), 128, 0, s>>>(sc, members);
+    begin_step_batch_kernel<<<member_blocks(max_members, 128), 128, 0, s>>>(sc, members, hold);
     return cudaGetLastError();
 }
 cudaError_t launch_end_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s)

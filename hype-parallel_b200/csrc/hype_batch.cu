@@ -85,6 +85,10 @@ struct hype_batch {
     std::vector<Inst> inst;
     DevScalars *dSc = nullptr;
     DevScalars *hSc = nullptr;        // pinned mirror, [M]
+    int *dHold = nullptr;             // per-slot hold flags read by begin-step, [M]
+    int *hHold = nullptr;             // pinned host copy
+    bool hold_dirty = false;
+    cudaEvent_t hold_ev = nullptr;    // completion of the last hold upload
     double *dStage = nullptr;         // Vec-layout staging, max_cells * 9 doubles
     Kind kinds[NKIND];
     cudaGraphExec_t exec = nullptr;
@@ -379,7 +383,7 @@ static cudaError_t enqueue_kind_step(hype_batch *b, int id, cudaStream_t s)
     Kind &k = b->kinds[id];
     const int M = b->cfg.max_instances;
     cudaError_t e;
-    if ((e = launch_begin_step_batch(b->dSc, k.dMembers, M, s)) != cudaSuccess) return e;
+    if ((e = launch_begin_step_batch(b->dSc, k.dMembers, b->dHold, M, s)) != cudaSuccess) return e;
     for (int st = 0; st < k.nstage; ++st)
         if ((e = enqueue_kind_stage(b, id, st, s)) != cudaSuccess) return e;
     if (k.copy_back && (e = launch_copy_batch(k.dCopyDst, k.dCopySrc, k.dCopyN, k.dMembers, M, b->dSc, s)) != cudaSuccess) return e;
@@ -483,6 +487,9 @@ int hype_batch_destroy(hype_batch *b)
     if (b->pool) cudaMemPoolDestroy(b->pool);
     if (b->dSc) cudaFree(b->dSc);
     if (b->hSc) cudaFreeHost(b->hSc);
+    if (b->dHold) cudaFree(b->dHold);
+    if (b->hHold) cudaFreeHost(b->hHold);
+    if (b->hold_ev) cudaEventDestroy(b->hold_ev);
     if (b->dStage) cudaFree(b->dStage);
     for (int k = 0; k < NKIND; ++k) {
         if (b->side[k]) cudaStreamDestroy(b->side[k]);
@@ -536,6 +543,11 @@ int hype_batch_create(const hype_batch_config *c, hype_batch **out)
     BCUDA(b, cudaMemset(b->dSc, 0, sizeof(DevScalars) * M));
     BCUDA(b, cudaMallocHost(&b->hSc, sizeof(DevScalars) * M));
     std::memset(b->hSc, 0, sizeof(DevScalars) * M);
+    BCUDA(b, cudaMalloc(&b->dHold, sizeof(int) * M));
+    BCUDA(b, cudaMemset(b->dHold, 0, sizeof(int) * M));
+    BCUDA(b, cudaMallocHost(&b->hHold, sizeof(int) * M));
+    std::memset(b->hHold, 0, sizeof(int) * M);
+    BCUDA(b, cudaEventCreateWithFlags(&b->hold_ev, cudaEventDisableTiming));
     if (cudaMalloc(&b->dStage, sizeof(double) * 9 * (size_t)c->max_cells) != cudaSuccess)
         return bfail(b, HYPE_ERR_NOMEM, "staging buffer of %lld cells", (long long)c->max_cells);
     b->inst.resize(M);
@@ -614,6 +626,11 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     in.used = true;
     in.bytes = bytes;
     b->in_use += bytes;
+    if (b->hHold[s]) {
+        BCUDA(b, cudaEventSynchronize(b->hold_ev));
+        b->hHold[s] = 0;
+        b->hold_dirty = true;
+    }
     k.members.push_back(s);
     if (k.members.size() == 1) b->dirty = true;
     if ((rc = upload_inst(b, s)) || (rc = rebuild_work(b, in.kind))) return rc;
@@ -660,6 +677,11 @@ int hype_batch_advance(hype_batch *b, int nsteps)
     int rc;
     if (b->dirty && (rc = capture_step(b))) return rc;
     if (!b->exec) { b->timed = false; return HYPE_OK; }
+    if (b->hold_dirty) {
+        BCUDA(b, cudaMemcpyAsync(b->dHold, b->hHold, sizeof(int) * b->inst.size(), cudaMemcpyHostToDevice, b->stream));
+        BCUDA(b, cudaEventRecord(b->hold_ev, b->stream));
+        b->hold_dirty = false;
+    }
     BCUDA(b, cudaEventRecord(b->ev0, b->stream));
     for (int k = 0; k < nsteps; ++k) BCUDA(b, cudaGraphLaunch(b->exec, b->stream));
     BCUDA(b, cudaEventRecord(b->ev1, b->stream));
@@ -695,6 +717,19 @@ int hype_batch_status(const hype_batch *b, int id, hype_instance_status *st)
     st->status = inst_status(b, id);
     st->t = d.t;
     st->dt_next = d.time_step;
+    st->held = b->hHold[id];
+    return HYPE_OK;
+}
+
+int hype_batch_hold(hype_batch *b, int id, int hold)
+{
+    if (!b || id < 0 || id >= (int)b->inst.size() || !b->inst[id].used) return bfail(b, HYPE_ERR_INVALID, "no instance %d", id);
+    const int v = hold ? 1 : 0;
+    if (b->hHold[id] == v) return HYPE_OK;
+    BCUDA(b, cudaSetDevice(b->cfg.device));
+    BCUDA(b, cudaEventSynchronize(b->hold_ev));   // the last upload has read the host array
+    b->hHold[id] = v;
+    b->hold_dirty = true;
     return HYPE_OK;
 }
 

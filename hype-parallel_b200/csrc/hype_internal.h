@@ -32,6 +32,8 @@ struct DevScalars {
     unsigned int err_cell;     // linear index of the first cell that raised an error
     int steps, max_steps;
     int done;                  // set when the run reached t_final or max_steps
+    int hold;                  // host request: skip this instance's steps for now (batch scheduling)
+    int idle;                  // set by begin_step for a step this instance does not take (done or held)
     int pad_;
     double cfl_h;              // CFL*h of the instance (read by the batched step control)
 };
@@ -102,8 +104,9 @@ cudaError_t launch_begin_step(DevScalars *sc, cudaStream_t s);
 cudaError_t launch_end_step(DevScalars *sc, double cfl_h, cudaStream_t s);
 cudaError_t launch_seed_dt(DevScalars *sc, double cfl_h, cudaStream_t s);
 // Batched step control over a member list: members[0] = count, members[1..] =
-// instance indices into sc[]; each instance uses its own sc[k].cfl_h.
-cudaError_t launch_begin_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s);
+// instance indices into sc[]; each instance uses its own sc[k].cfl_h and takes
+// its hold flag from hold[k].
+cudaError_t launch_begin_step_batch(DevScalars *sc, const int *members, const int *hold, int max_members, cudaStream_t s);
 cudaError_t launch_end_step_batch(DevScalars *sc, const int *members, int max_members, cudaStream_t s);
 // u^n = S0 for every member (forward Euler), one pointer pair per instance
 cudaError_t launch_copy_batch(double *const *dst, const double *const *src, const long long *n, const int *members,

@@ -36,6 +36,7 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[HYPE_NOALLOC_MAX_BYTES
 
 constexpr int kMaxDevices = 64;
 constexpr size_t kPlanesOffset = 256;   // DevScalars first, planes after (256-byte aligned)
+static_assert(sizeof(DevScalars) <= kPlanesOffset, "DevScalars must fit ahead of the planes");
 
 std::mutex g_setup_mutex;
 unsigned char *g_scratch_dev[kMaxDevices] = {nullptr};
@@ -46,7 +47,7 @@ __global__ void noalloc_reset_kernel(DevScalars *sc)
     sc->smax = 0ull;
     sc->err = 0u;
     sc->err_cell = 0xffffffffu;
-    sc->steps = 0; sc->max_steps = 0; sc->done = 0; sc->pad_ = 0;
+    sc->steps = 0; sc->max_steps = 0; sc->done = 0; sc->hold = 0; sc->idle = 0; sc->pad_ = 0;
 }
 
 typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,

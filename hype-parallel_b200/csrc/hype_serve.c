@@ -8,9 +8,11 @@
  *      built on the host, uploaded, and its dt seeded by one RHS evaluation);
  *      a request that does not fit waits at the head of the queue until
  *      finished instances free their memory;
- *   2. enqueue k steps of the whole batch (k graph replays, k sized so that
- *      they take about poll_ms of GPU time); while they run, build the
- *      initial state of the next waiting request on the host; then wait;
+ *   2. choose which resident requests step (least remaining work first, up
+ *      to active_cells cells; the others are held), enqueue k steps of the
+ *      batch (k graph replays, k sized so that they take about poll_ms of GPU
+ *      time); while they run, build the initial state of the next waiting
+ *      request on the host; then wait;
  *   3. retire every instance whose time loop ended: copy its state out, hand
  *      it to the sink, free its slot and memory.
  * Instances stop on the device at their own t_final / max_steps, so the k
@@ -70,6 +72,52 @@ void hype_serve_config_default(hype_serve_config *c)
     c->realtime = 1;
     c->autotune = 1;
     c->fetch_results = 1;
+    c->active_cells = 8LL << 20;
+}
+
+typedef struct {
+    double work;     /* cells x remaining steps */
+    int slot;
+    int order;       /* request index: ties go to the earlier arrival */
+    long long cells;
+} pick_t;
+
+static int cmp_pick(const void *a, const void *b)
+{
+    const pick_t *x = (const pick_t *)a, *y = (const pick_t *)b;
+    if (x->work != y->work) return x->work < y->work ? -1 : 1;
+    return x->order - y->order;
+}
+
+/* Least-remaining-work-first: release the resident requests with the least
+ * work left until their cells reach `budget`, hold the others. */
+static void schedule(hype_batch *b, const hype_request *req, const int *req_of, int M, long long budget, pick_t *tmp)
+{
+    int n = 0;
+    for (int s = 0; s < M; ++s) {
+        if (req_of[s] < 0) continue;
+        const hype_request *r = &req[req_of[s]];
+        hype_instance_status st;
+        hype_batch_status(b, s, &st);
+        double rem = (double)(r->max_steps - st.steps);
+        if (r->t_final < 1e300 && st.dt_next > 0.0) {
+            const double by_t = ceil((r->t_final - st.t) / st.dt_next);
+            if (by_t < rem) rem = by_t;
+        }
+        if (rem < 1.0) rem = 1.0;
+        tmp[n].cells = (long long)r->cfg.nx * r->cfg.ny;
+        tmp[n].work = rem * (double)tmp[n].cells;
+        tmp[n].slot = s;
+        tmp[n].order = req_of[s];
+        ++n;
+    }
+    qsort(tmp, (size_t)n, sizeof(pick_t), cmp_pick);
+    long long acc = 0;
+    for (int k = 0; k < n; ++k) {
+        const int run = (k == 0) || acc < budget;
+        if (run) acc += tmp[k].cells;
+        hype_batch_hold(b, tmp[k].slot, !run);
+    }
 }
 
 static int make_initial(const hype_request *r, int index, hype_fill_fn fill, void *ctx, double *U)
@@ -108,11 +156,14 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
     size_t budget = 0;
     hype_batch_info(b, NULL, NULL, NULL, &budget);
     int *req_of = (int *)malloc(sizeof(int) * (size_t)M);
+    pick_t *picks = (pick_t *)malloc(sizeof(pick_t) * (size_t)M);
     /* pinned host staging: initial states in, final states out */
     double *host = NULL, *host_out = NULL;
     const size_t hbytes = sizeof(double) * 9 * (size_t)c->max_cells;
-    if (!req_of || cudaMallocHost((void **)&host, hbytes) != cudaSuccess || cudaMallocHost((void **)&host_out, hbytes) != cudaSuccess) {
+    if (!req_of || !picks || cudaMallocHost((void **)&host, hbytes) != cudaSuccess ||
+        cudaMallocHost((void **)&host_out, hbytes) != cudaSuccess) {
         free(req_of);
+        free(picks);
         if (host) cudaFreeHost(host);
         if (host_out) cudaFreeHost(host_out);
         hype_batch_destroy(b);
@@ -185,7 +236,8 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
             }
             if (ms_per_step < 0.0) steps_per_poll = 1;   /* re-measure the step time */
         }
-        /* 2. k steps of every resident instance; the next waiting request's
+        if (c->active_cells > 0) schedule(b, req, req_of, M, c->active_cells, picks);
+        /* 2. k steps of every released instance; the next waiting request's
          *    initial state is built on the host meanwhile */
         if ((rc = hype_batch_advance(b, steps_per_poll))) break;
         if (next < n && staged != next && (!c->realtime || req[next].arrival_s <= now_s() - t_start) &&
@@ -260,6 +312,7 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
     free(lat);
     free(que);
     free(req_of);
+    free(picks);
     cudaFreeHost(host);
     cudaFreeHost(host_out);
     hype_batch_destroy(b);

@@ -207,7 +207,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
     using QD = Quad<2>;
     constexpr int NV = 6, CELLS = K::CELLS, BW = K::BW, SLOTS = K::SLOTS;
     constexpr unsigned FULL = 0xffffffffu;
-    if (p.sc->done) return;
+    if (p.sc->idle) return;   // finished or held run (set by begin_step; 0 outside a time loop)
 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     unsigned char *rows = smem + 128;

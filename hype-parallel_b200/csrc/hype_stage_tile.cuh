@@ -144,7 +144,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     constexpr int NVH = (NV + 1) / 2;          // variables per half in the reconstruction
     constexpr unsigned FULL = 0xffffffffu;
 
-    if (p.sc->done) return;
+    if (p.sc->idle) return;   // finished or held run (set by begin_step; 0 outside a time loop)
 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw);
     double *rows_s = reinterpret_cast<double *>(smem_raw + 128);

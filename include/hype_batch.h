@@ -51,6 +51,7 @@ typedef struct {
                                by this instance's stages                                  */
     double t;               /* time reached                                               */
     double dt_next;         /* dt the last RHS proposed (Ctx->dt)                         */
+    int held;               /* hype_batch_hold is in force                                */
 } hype_instance_status;
 
 /* max_instances 256, budget 0 (80% of free), max_cells 2048*2048, device 0 */
@@ -88,6 +89,12 @@ HYPE_API int hype_batch_sync(hype_batch *b);
 
 /* Status of an instance as of the last hype_batch_sync (or add). */
 HYPE_API int hype_batch_status(const hype_batch *b, int id, hype_instance_status *st);
+
+/* Holds (hold = 1) or releases an instance: a held instance keeps its state
+ * and time loop but takes no steps, and its tiles cost one flag read per
+ * stage -- a scheduler's way to give the GPU to other instances first.  Takes
+ * effect from the next hype_batch_advance. */
+HYPE_API int hype_batch_hold(hype_batch *b, int id, int hold);
 
 /* Copies an instance's state out (host, Vec layout); waits for queued work. */
 HYPE_API int hype_batch_get_state(hype_batch *b, int id, double *U);

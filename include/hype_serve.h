@@ -58,6 +58,10 @@ typedef struct {
     int autotune;            /* 1: retune the tile shape when the batch has grown
                                 by half since the last tuning                        */
     int fetch_results;       /* 1: copy each final state to the host (sink or not)  */
+    long long active_cells;  /* scheduling: each poll, resident requests step in order
+                                of least remaining work (cells x steps left) until
+                                their cells reach this many; the rest are held.
+                                0 = every resident request steps (processor sharing) */
 } hype_serve_config;
 
 typedef struct {
@@ -79,7 +83,8 @@ typedef int (*hype_fill_fn)(void *ctx, int index, const hype_request *req, doubl
 /* Receives request `index`'s final state (valid during the call only). */
 typedef void (*hype_sink_fn)(void *ctx, int index, const hype_request *req, const double *U, const hype_request_result *res);
 
-/* device 0, 256 slots, budget 0, max_cells 2048*2048, poll 10 ms, realtime, autotune, fetch */
+/* device 0, 256 slots, budget 0, max_cells 2048*2048, poll 10 ms, realtime, autotune, fetch,
+ * active_cells 8*2^20 */
 HYPE_API void hype_serve_config_default(hype_serve_config *c);
 
 /*

@@ -164,3 +164,30 @@ def test_inadmissible_instance_stops_alone(hp):
         b.sync()
         assert b.status(ib)["status"] == hp.ERR_INADMISSIBLE and b.status(ib)["done"] == 1
         check_same(hp, b, ig, good, Ug, 0.0, 1e30, 9)
+
+
+def test_held_instance_waits_and_resumes_unchanged(hp):
+    """A held instance takes no steps (its state and time loop stay as they
+    are) and, once released, ends exactly as a lone run."""
+    ca, cb = kapila(hp, 120, 90), kapila(hp, 90, 70)
+    Ua = hp.initial_state(ca, "shock_bubble", seed=90, nbubbles=2)
+    Ub = hp.initial_state(cb, "shock_bubble", seed=91, nbubbles=1)
+    with hp.Batch(max_instances=4) as b:
+        a = b.add(ca, Ua, 0.0, 1e30, 10)
+        i = b.add(cb, Ub, 0.0, 1e30, 10)
+        b.advance(4)
+        b.sync()
+        b.hold(a)
+        b.advance(5)
+        b.sync()
+        assert b.status(a)["steps"] == 4 and b.status(a)["held"] == 1
+        assert b.status(i)["steps"] == 9
+        U_mid = b.get_state(a)
+        b.advance(3)
+        b.sync()
+        assert b.get_state(a).tobytes() == U_mid.tobytes() and b.status(a)["steps"] == 4
+        b.hold(a, False)
+        b.advance(8)
+        b.sync()
+        check_same(hp, b, a, ca, Ua, 0.0, 1e30, 10)
+        check_same(hp, b, i, cb, Ub, 0.0, 1e30, 10)
