@@ -370,7 +370,8 @@ def serve_leg(hp, args, local_rank, capacity):
         r.arrival_s = t
         t += float(rng.exponential(1.0 / rate))
     res, st = hp.serve(reqs, device=local_rank, hbm_budget=150 * 10 ** 9, max_instances=1024, max_cells=2048 * 2048,
-                       poll_ms=args.serve_poll_ms, realtime=True, active_cells=args.serve_active_cells)
+                       poll_ms=args.serve_poll_ms, realtime=True, active_cells=args.serve_active_cells,
+                       substep_cells=args.serve_substep_cells)
     lat = np.array([r["latency_s"] for r in res])
     by_sys = {}
     for nm, sysid in (("kapila", hp.KAPILA_5EQN), ("bn", hp.BAER_NUNZIATO), ("euler", hp.EULER)):
@@ -380,7 +381,8 @@ def serve_leg(hp, args, local_rank, capacity):
                           "p99_s": float(np.percentile(lat[sel], 99))}
     return {"workload": f"Poisson stream of {n} solves: 70/20/10 kapila5/bn/euler, square grids 64..2048 log-uniform, "
                         "50..2000 steps log-uniform, N=2 SSPRK(4,3), 150 GB HBM budget",
-            "requests": n, "kapila_precision": args.serve_kapila, "active_cells": args.serve_active_cells, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
+            "requests": n, "kapila_precision": args.serve_kapila, "active_cells": args.serve_active_cells,
+            "substep_cells": args.serve_substep_cells, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
             "offered_cell_updates": float(np.sum(work)),
             "p50_s": st["p50_s"], "p90_s": st["p90_s"], "p99_s": st["p99_s"], "max_s": st["max_s"], "mean_s": st["mean_s"],
             "queue_p50_s": st["queue_p50_s"], "queue_p99_s": st["queue_p99_s"],
@@ -535,9 +537,11 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serve-kapila", default="mixed", choices=["mixed", "fp64"], help="precision of Kapila requests")
     ap.add_argument("--serve-poll-ms", type=float, default=10.0)
-    ap.add_argument("--serve-active-cells", type=int, default=8 << 20,
+    ap.add_argument("--serve-active-cells", type=int, default=4 << 20,
                     help="scheduler: cells stepped at once, least remaining work first (0: all resident requests)")
     ap.add_argument("--serve-load", type=float, default=None, help="load factor of the arrival rate (default: seed-drawn)")
+    ap.add_argument("--serve-substep-cells", type=int, default=0,
+                    help="scheduler: a grid of c cells takes up to this/c steps per batch step (0: one)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -88,7 +88,7 @@ class _BatchCfg(ctypes.Structure):
 
 class _InstStatus(ctypes.Structure):
     _fields_ = [("active", ctypes.c_int), ("done", ctypes.c_int), ("steps", ctypes.c_int), ("status", ctypes.c_int),
-                ("t", ctypes.c_double), ("dt_next", ctypes.c_double), ("held", ctypes.c_int)]
+                ("t", ctypes.c_double), ("dt_next", ctypes.c_double), ("held", ctypes.c_int), ("substeps", ctypes.c_int)]
 
 
 class _Request(ctypes.Structure):
@@ -104,7 +104,8 @@ class _Result(ctypes.Structure):
 class _ServeCfg(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("max_instances", ctypes.c_int), ("hbm_budget", ctypes.c_size_t),
                 ("max_cells", ctypes.c_longlong), ("poll_ms", ctypes.c_double), ("realtime", ctypes.c_int),
-                ("autotune", ctypes.c_int), ("fetch_results", ctypes.c_int), ("active_cells", ctypes.c_longlong)]
+                ("autotune", ctypes.c_int), ("fetch_results", ctypes.c_int), ("active_cells", ctypes.c_longlong),
+                ("substep_cells", ctypes.c_longlong)]
 
 
 class _ServeStats(ctypes.Structure):
@@ -178,6 +179,7 @@ def lib() -> ctypes.CDLL:
         L.hype_batch_status.argtypes = [vp, ctypes.c_int, ctypes.POINTER(_InstStatus)]
         L.hype_batch_get_state.argtypes = [vp, ctypes.c_int, _DP]
         L.hype_batch_hold.argtypes = [vp, ctypes.c_int, ctypes.c_int]
+        L.hype_batch_set_substeps.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.hype_batch_set_tiling.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.hype_batch_autotune.argtypes = [vp, ctypes.c_int, IP, IP]
         L.hype_batch_info.argtypes = [vp, IP, IP, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
@@ -426,6 +428,9 @@ class Batch:
     def hold(self, i: int, hold: bool = True) -> None:
         self._check(lib().hype_batch_hold(self._h, i, int(hold)))
 
+    def set_substeps(self, i: int, k: int) -> None:
+        self._check(lib().hype_batch_set_substeps(self._h, i, k))
+
     def get_state(self, i: int) -> np.ndarray:
         c = self.cfgs[i]
         U = np.empty(c.nx * c.ny * c.nvar, dtype=np.float64)
@@ -472,7 +477,7 @@ class Request:
 
 def serve(requests, *, device: int = 0, max_instances: int = 256, hbm_budget: int = 0, max_cells: int = 2048 * 2048,
           poll_ms: float = 10.0, realtime: bool = True, autotune: bool = True, fetch_results: bool = True,
-          active_cells: int | None = None, fill=None, sink=None):
+          active_cells: int | None = None, substep_cells: int | None = None, fill=None, sink=None):
     """Runs hype_serve_run over ``requests`` (sorted by arrival).
 
     fill(index, U0) fills the initial state of IC_CALLBACK requests in place;
@@ -492,6 +497,8 @@ def serve(requests, *, device: int = 0, max_instances: int = 256, hbm_budget: in
     c.poll_ms, c.realtime, c.autotune, c.fetch_results = poll_ms, int(realtime), int(autotune), int(fetch_results)
     if active_cells is not None:
         c.active_cells = active_cells
+    if substep_cells is not None:
+        c.substep_cells = substep_cells
 
     def _fill(_ctx, i, _req, U):
         try:

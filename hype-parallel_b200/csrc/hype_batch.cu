@@ -32,6 +32,7 @@ namespace {
 constexpr int NKIND = 13;              // FP64: 3 systems x 4 orders; 12 = mixed Kapila N = 2
 constexpr int KIND_MIXED = 12;
 constexpr int NBUF = 4;                // U, S0, S1, S2
+constexpr int MAX_SUBSTEPS = 16;       // steps an instance may take per batch step
 
 int kind_of(const hype_config &c) { return c.precision == HYPE_PREC_MIXED ? KIND_MIXED : c.system * 4 + c.order; }
 
@@ -48,6 +49,16 @@ struct Inst {
     double *inlet = nullptr;
     size_t bytes = 0;
     int strips = 1, runs = 1;
+    int substeps = 1;                  // steps per batch step (hype_batch_set_substeps)
+};
+
+// The members taking sub-step j of a batch step (those with substeps > j):
+// their step-control list and the (slot, tile) work-list of the stage launches.
+struct SubList {
+    int2 *dWork = nullptr;
+    int work_cap = 0, nwork = 0;
+    int *dSched = nullptr;             // [4]: item count, next item, blocks finished
+    int *dMembers = nullptr;           // [1 + M]
 };
 
 struct Kind {
@@ -62,11 +73,9 @@ struct Kind {
     MixedParams *dMParams = nullptr;   // [MAX_PLAN][M]
     CUtensorMap *dMaps = nullptr;      // [3][M]
     MixedMaps *dMMaps = nullptr;       // [3][M]
-    int2 *dWork = nullptr;
-    int work_cap = 0, nwork = 0;
+    SubList sub[MAX_SUBSTEPS];
+    int nsub = 1;                      // sub-steps in the captured step (max substeps of the members)
     long long cost = 0;                // cells of all members (autotune report)
-    int *dSched = nullptr;             // [4]
-    int *dMembers = nullptr;           // [1 + M]
     double **dCopyDst = nullptr, **dCopySrc = nullptr;   // forward Euler u = S0, [M]
     long long *dCopyN = nullptr;
 };
@@ -154,6 +163,17 @@ static int kind_blocks_per_sm(const Kind &k, int cells)
     return k.mixed ? mixed_batch_blocks_per_sm(cells) : stage_batch_blocks_per_sm(k.system, k.order, cells);
 }
 
+static int sub_init(hype_batch *b, SubList &l)
+{
+    if (l.dSched) return HYPE_OK;
+    const int M = b->cfg.max_instances;
+    BCUDA(b, pool_alloc(b, &l.dSched, sizeof(int) * 4));
+    BCUDA(b, cudaMemsetAsync(l.dSched, 0, sizeof(int) * 4, b->stream));
+    BCUDA(b, pool_alloc(b, &l.dMembers, sizeof(int) * (1 + M)));
+    BCUDA(b, cudaMemsetAsync(l.dMembers, 0, sizeof(int) * (1 + M), b->stream));
+    return HYPE_OK;
+}
+
 static int kind_init(hype_batch *b, int id, const hype_config &c)
 {
     Kind &k = b->kinds[id];
@@ -174,10 +194,8 @@ static int kind_init(hype_batch *b, int id, const hype_config &c)
         BCUDA(b, pool_alloc(b, &k.dParams, sizeof(StageParams) * MAX_PLAN * M));
         BCUDA(b, pool_alloc(b, &k.dMaps, sizeof(CUtensorMap) * 3 * M));
     }
-    BCUDA(b, pool_alloc(b, &k.dSched, sizeof(int) * 4));
-    BCUDA(b, cudaMemsetAsync(k.dSched, 0, sizeof(int) * 4, b->stream));
-    BCUDA(b, pool_alloc(b, &k.dMembers, sizeof(int) * (1 + M)));
-    BCUDA(b, cudaMemsetAsync(k.dMembers, 0, sizeof(int) * (1 + M), b->stream));
+    int rc;
+    if ((rc = sub_init(b, k.sub[0]))) return rc;
     if (k.copy_back) {
         BCUDA(b, pool_alloc(b, &k.dCopyDst, sizeof(double *) * M));
         BCUDA(b, pool_alloc(b, &k.dCopySrc, sizeof(double *) * M));
@@ -297,51 +315,67 @@ static int upload_inst(hype_batch *b, int s)
     return HYPE_OK;
 }
 
-// Rebuilds the kind's member list and work-list: every (slot, tile) of every
-// member, sorted by estimated tile cost (columns x rows, halos included),
-// longest first, so the persistent blocks finish together.
+// Rebuilds the kind's member lists and work-lists, one per sub-step j (the
+// members with substeps > j): every (slot, tile) of those members, sorted by
+// estimated tile cost (columns x rows, halos included), longest first, so the
+// persistent blocks finish together.
 static int rebuild_work(hype_batch *b, int id)
 {
     Kind &k = b->kinds[id];
     struct Item { long long cost; int2 it; };
-    std::vector<Item> items;
+    int K = 1;
     k.cost = 0;
     for (int s : k.members) {
         const Inst &in = b->inst[s];
         k.cost += (long long)in.cfg.nx * in.cfg.ny;
-        const int halo = k.mixed ? 8 : 6;
-        for (int run = 0; run < in.runs; ++run) {
-            const int H = (int)(((long long)(run + 1) * in.cfg.ny) / in.runs) - (int)(((long long)run * in.cfg.ny) / in.runs);
-            for (int st = 0; st < in.strips; ++st) {
-                const int w = in.cfg.nx / in.strips + 1;
-                items.push_back(Item{(long long)(w + halo) * (H + 6), make_int2(s, run * in.strips + st)});
-            }
-        }
+        if (in.substeps > K) K = in.substeps;
     }
-    std::stable_sort(items.begin(), items.end(), [](const Item &a, const Item &c) { return a.cost > c.cost; });
-    const int n = (int)items.size();
-    if (n > k.work_cap) {
-        int cap = k.work_cap > 0 ? k.work_cap : 1024;
-        while (cap < n) cap *= 2;
-        if (b->exec) {   // the captured graph holds the old pointer
-            BCUDA(b, cudaStreamSynchronize(b->stream));
-            cudaGraphExecDestroy(b->exec);
-            b->exec = nullptr;
-        }
-        pool_free(b, k.dWork);
-        BCUDA(b, pool_alloc(b, &k.dWork, sizeof(int2) * cap));
-        k.work_cap = cap;
+    if (K != k.nsub) {
+        k.nsub = K;
         b->dirty = true;
     }
-    std::vector<int2> w(n);
-    for (int i = 0; i < n; ++i) w[i] = items[i].it;
-    if (n) BCUDA(b, cudaMemcpyAsync(k.dWork, w.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, b->stream));
-    BCUDA(b, cudaMemcpyAsync(k.dSched, &n, sizeof(int), cudaMemcpyHostToDevice, b->stream));
-    std::vector<int> mem(1 + k.members.size());
-    mem[0] = (int)k.members.size();
-    for (size_t i = 0; i < k.members.size(); ++i) mem[1 + i] = k.members[i];
-    BCUDA(b, cudaMemcpyAsync(k.dMembers, mem.data(), sizeof(int) * mem.size(), cudaMemcpyHostToDevice, b->stream));
-    k.nwork = n;
+    int rc;
+    for (int j = 0; j < K; ++j) {
+        SubList &l = k.sub[j];
+        if ((rc = sub_init(b, l))) return rc;
+        std::vector<Item> items;
+        std::vector<int> mem(1, 0);
+        for (int s : k.members) {
+            const Inst &in = b->inst[s];
+            if (in.substeps <= j) continue;
+            mem.push_back(s);
+            const int halo = k.mixed ? 8 : 6;
+            for (int run = 0; run < in.runs; ++run) {
+                const int H = (int)(((long long)(run + 1) * in.cfg.ny) / in.runs) - (int)(((long long)run * in.cfg.ny) / in.runs);
+                for (int st = 0; st < in.strips; ++st) {
+                    const int w = in.cfg.nx / in.strips + 1;
+                    items.push_back(Item{(long long)(w + halo) * (H + 6), make_int2(s, run * in.strips + st)});
+                }
+            }
+        }
+        mem[0] = (int)mem.size() - 1;
+        std::stable_sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.cost > y.cost; });
+        const int n = (int)items.size();
+        if (n > l.work_cap) {
+            int cap = l.work_cap > 0 ? l.work_cap : 1024;
+            while (cap < n) cap *= 2;
+            if (b->exec) {   // the captured graph holds the old pointer
+                BCUDA(b, cudaStreamSynchronize(b->stream));
+                cudaGraphExecDestroy(b->exec);
+                b->exec = nullptr;
+            }
+            pool_free(b, l.dWork);
+            BCUDA(b, pool_alloc(b, &l.dWork, sizeof(int2) * cap));
+            l.work_cap = cap;
+            b->dirty = true;
+        }
+        std::vector<int2> w(n);
+        for (int i = 0; i < n; ++i) w[i] = items[i].it;
+        if (n) BCUDA(b, cudaMemcpyAsync(l.dWork, w.data(), sizeof(int2) * n, cudaMemcpyHostToDevice, b->stream));
+        BCUDA(b, cudaMemcpyAsync(l.dSched, &n, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+        BCUDA(b, cudaMemcpyAsync(l.dMembers, mem.data(), sizeof(int) * mem.size(), cudaMemcpyHostToDevice, b->stream));
+        l.nwork = n;
+    }
     return HYPE_OK;
 }
 
@@ -368,26 +402,32 @@ static int kind_set_tiling(hype_batch *b, int id, int cells, int rows)
 // ---------------------------------------------------------------------------
 // the step graph
 // ---------------------------------------------------------------------------
-static cudaError_t enqueue_kind_stage(hype_batch *b, int id, int st, cudaStream_t s)
+static cudaError_t enqueue_kind_stage(hype_batch *b, int id, int st, cudaStream_t s, int j = 0)
 {
     Kind &k = b->kinds[id];
+    SubList &l = k.sub[j];
     const int M = b->cfg.max_instances;
     const int blocks = b->sms * k.bps;
     const PlanStage &q = k.plan[st];
-    if (k.mixed) return launch_mixed_batch(k.cells, k.dMParams + st * M, k.dMMaps + q.in * M, k.dWork, k.dSched, blocks, s);
-    return launch_stage_batch(k.system, k.order, k.cells, k.dParams + st * M, k.dMaps + q.in * M, k.dWork, k.dSched, blocks, s);
+    if (k.mixed) return launch_mixed_batch(k.cells, k.dMParams + st * M, k.dMMaps + q.in * M, l.dWork, l.dSched, blocks, s);
+    return launch_stage_batch(k.system, k.order, k.cells, k.dParams + st * M, k.dMaps + q.in * M, l.dWork, l.dSched, blocks, s);
 }
 
+// One batch step of a kind: sub-step j steps the members with substeps > j.
 static cudaError_t enqueue_kind_step(hype_batch *b, int id, cudaStream_t s)
 {
     Kind &k = b->kinds[id];
     const int M = b->cfg.max_instances;
     cudaError_t e;
-    if ((e = launch_begin_step_batch(b->dSc, k.dMembers, b->dHold, M, s)) != cudaSuccess) return e;
-    for (int st = 0; st < k.nstage; ++st)
-        if ((e = enqueue_kind_stage(b, id, st, s)) != cudaSuccess) return e;
-    if (k.copy_back && (e = launch_copy_batch(k.dCopyDst, k.dCopySrc, k.dCopyN, k.dMembers, M, b->dSc, s)) != cudaSuccess) return e;
-    return launch_end_step_batch(b->dSc, k.dMembers, M, s);
+    for (int j = 0; j < k.nsub; ++j) {
+        const int *mem = k.sub[j].dMembers;
+        if ((e = launch_begin_step_batch(b->dSc, mem, b->dHold, M, s)) != cudaSuccess) return e;
+        for (int st = 0; st < k.nstage; ++st)
+            if ((e = enqueue_kind_stage(b, id, st, s, j)) != cudaSuccess) return e;
+        if (k.copy_back && (e = launch_copy_batch(k.dCopyDst, k.dCopySrc, k.dCopyN, mem, M, b->dSc, s)) != cudaSuccess) return e;
+        if ((e = launch_end_step_batch(b->dSc, mem, M, s)) != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // Captures one step of every non-empty kind; kinds run on parallel branches.
@@ -479,7 +519,7 @@ int hype_batch_destroy(hype_batch *b)
             if (in.used) free_inst(b, in);
         for (Kind &k : b->kinds) {
             pool_free(b, k.dParams); pool_free(b, k.dMParams); pool_free(b, k.dMaps); pool_free(b, k.dMMaps);
-            pool_free(b, k.dWork); pool_free(b, k.dSched); pool_free(b, k.dMembers);
+            for (SubList &l : k.sub) { pool_free(b, l.dWork); pool_free(b, l.dSched); pool_free(b, l.dMembers); }
             pool_free(b, k.dCopyDst); pool_free(b, k.dCopySrc); pool_free(b, k.dCopyN);
         }
         cudaStreamSynchronize(b->stream);
@@ -718,7 +758,19 @@ int hype_batch_status(const hype_batch *b, int id, hype_instance_status *st)
     st->t = d.t;
     st->dt_next = d.time_step;
     st->held = b->hHold[id];
+    st->substeps = b->inst[id].substeps;
     return HYPE_OK;
+}
+
+int hype_batch_set_substeps(hype_batch *b, int id, int substeps)
+{
+    if (!b || id < 0 || id >= (int)b->inst.size() || !b->inst[id].used) return bfail(b, HYPE_ERR_INVALID, "no instance %d", id);
+    if (substeps < 1 || substeps > MAX_SUBSTEPS) return bfail(b, HYPE_ERR_INVALID, "substeps must be 1..%d", MAX_SUBSTEPS);
+    Inst &in = b->inst[id];
+    if (in.substeps == substeps) return HYPE_OK;
+    BCUDA(b, cudaSetDevice(b->cfg.device));
+    in.substeps = substeps;
+    return rebuild_work(b, in.kind);
 }
 
 int hype_batch_hold(hype_batch *b, int id, int hold)
@@ -800,7 +852,7 @@ int hype_batch_info(const hype_batch *b, int *instances, int *work_items, size_t
     if (!b) return HYPE_ERR_INVALID;
     int n = 0, w = 0;
     for (const Inst &in : b->inst) n += in.used ? 1 : 0;
-    for (const Kind &k : b->kinds) w += k.ready ? k.nwork : 0;
+    for (const Kind &k : b->kinds) w += k.ready ? k.sub[0].nwork : 0;
     if (instances) *instances = n;
     if (work_items) *work_items = w;
     if (bytes_in_use) *bytes_in_use = b->in_use;

@@ -9,7 +9,8 @@
  *      a request that does not fit waits at the head of the queue until
  *      finished instances free their memory;
  *   2. choose which resident requests step (least remaining work first, up
- *      to active_cells cells; the others are held), enqueue k steps of the
+ *      to active_cells cells; the others are held; a small grid takes up to
+ *      substep_cells / cells steps per batch step), enqueue k steps of the
  *      batch (k graph replays, k sized so that they take about poll_ms of GPU
  *      time); while they run, build the initial state of the next waiting
  *      request on the host; then wait;
@@ -72,14 +73,24 @@ void hype_serve_config_default(hype_serve_config *c)
     c->realtime = 1;
     c->autotune = 1;
     c->fetch_results = 1;
-    c->active_cells = 8LL << 20;
+    c->active_cells = 4LL << 20;
+    c->substep_cells = 0;
+}
+
+/* steps per batch step for a grid of `cells` cells: the largest power of two
+ * k <= 16 with k * cells <= substep_cells (at least 1) */
+static int substeps_for(long long cells, long long substep_cells)
+{
+    int k = 1;
+    while (k < 16 && 2LL * k * cells <= substep_cells) k *= 2;
+    return k;
 }
 
 typedef struct {
     double work;     /* cells x remaining steps */
     int slot;
     int order;       /* request index: ties go to the earlier arrival */
-    long long cells;
+    long long cells; /* cells stepped per batch step (grid cells x substeps) */
 } pick_t;
 
 static int cmp_pick(const void *a, const void *b)
@@ -90,7 +101,8 @@ static int cmp_pick(const void *a, const void *b)
 }
 
 /* Least-remaining-work-first: release the resident requests with the least
- * work left until their cells reach `budget`, hold the others. */
+ * work left until the cells they step per batch step reach `budget`, hold
+ * the others. */
 static void schedule(hype_batch *b, const hype_request *req, const int *req_of, int M, long long budget, pick_t *tmp)
 {
     int n = 0;
@@ -105,8 +117,9 @@ static void schedule(hype_batch *b, const hype_request *req, const int *req_of, 
             if (by_t < rem) rem = by_t;
         }
         if (rem < 1.0) rem = 1.0;
-        tmp[n].cells = (long long)r->cfg.nx * r->cfg.ny;
-        tmp[n].work = rem * (double)tmp[n].cells;
+        const long long cells = (long long)r->cfg.nx * r->cfg.ny;
+        tmp[n].cells = cells * (st.substeps > 0 ? st.substeps : 1);
+        tmp[n].work = rem * (double)cells;
         tmp[n].slot = s;
         tmp[n].order = req_of[s];
         ++n;
@@ -201,6 +214,11 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
                 if (st == HYPE_ERR_NOMEM || st == HYPE_ERR_BUSY) {
                     if (running > 0) break;   /* wait for retirements */
                     st = HYPE_ERR_NOMEM;      /* nothing to wait for: it can never fit */
+                }
+                if (st == HYPE_OK && c->substep_cells > 0) {
+                    const int k = substeps_for(cells, c->substep_cells);
+                    if (k > 1) st = hype_batch_set_substeps(b, id, k);
+                    if (st != HYPE_OK) hype_batch_remove(b, id);
                 }
                 if (st == HYPE_OK) {
                     req_of[id] = next;

@@ -7,7 +7,8 @@
  * exactly the arithmetic of a lone hype_solver of the same configuration --
  * and advances all of them with one persistent stage-kernel launch per RK
  * stage and per kind of instance, over a device work-list of (instance, tile)
- * items sorted longest first.  A whole step of the batch is one CUDA graph.
+ * items sorted longest first.  A whole step of the batch is one CUDA graph;
+ * in it an instance takes one step, or several (hype_batch_set_substeps).
  *
  * Instances join and leave between steps (continuous batching): the work-list,
  * member lists and per-instance parameters live in device memory, so adding or
@@ -52,6 +53,7 @@ typedef struct {
     double t;               /* time reached                                               */
     double dt_next;         /* dt the last RHS proposed (Ctx->dt)                         */
     int held;               /* hype_batch_hold is in force                                */
+    int substeps;           /* steps it takes per batch step                              */
 } hype_instance_status;
 
 /* max_instances 256, budget 0 (80% of free), max_cells 2048*2048, device 0 */
@@ -95,6 +97,13 @@ HYPE_API int hype_batch_status(const hype_batch *b, int id, hype_instance_status
  * stage -- a scheduler's way to give the GPU to other instances first.  Takes
  * effect from the next hype_batch_advance. */
 HYPE_API int hype_batch_hold(hype_batch *b, int id, int hold);
+
+/* Steps an instance takes per batch step (1..16, default 1): a small grid
+ * can take several steps while a large one takes one, so that small, long
+ * runs are not paced by the largest member.  Each step is still the
+ * instance's own step, with its own dt and stop tests (an instance never
+ * overruns its t_final or max_steps).  Takes effect from the next advance. */
+HYPE_API int hype_batch_set_substeps(hype_batch *b, int id, int substeps);
 
 /* Copies an instance's state out (host, Vec layout); waits for queued work. */
 HYPE_API int hype_batch_get_state(hype_batch *b, int id, double *U);

@@ -62,6 +62,9 @@ typedef struct {
                                 of least remaining work (cells x steps left) until
                                 their cells reach this many; the rest are held.
                                 0 = every resident request steps (processor sharing) */
+    long long substep_cells; /* a request of c cells takes up to substep_cells / c steps
+                                (a power of two, 1..16) per batch step, so small grids
+                                are not paced by large ones; 0 = one step each        */
 } hype_serve_config;
 
 typedef struct {
@@ -84,7 +87,7 @@ typedef int (*hype_fill_fn)(void *ctx, int index, const hype_request *req, doubl
 typedef void (*hype_sink_fn)(void *ctx, int index, const hype_request *req, const double *U, const hype_request_result *res);
 
 /* device 0, 256 slots, budget 0, max_cells 2048*2048, poll 10 ms, realtime, autotune, fetch,
- * active_cells 8*2^20 */
+ * active_cells 4*2^20, substep_cells 0 */
 HYPE_API void hype_serve_config_default(hype_serve_config *c);
 
 /*

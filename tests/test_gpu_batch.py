@@ -191,3 +191,30 @@ def test_held_instance_waits_and_resumes_unchanged(hp):
         b.sync()
         check_same(hp, b, a, ca, Ua, 0.0, 1e30, 10)
         check_same(hp, b, i, cb, Ub, 0.0, 1e30, 10)
+
+
+def test_substeps_take_several_exact_steps_per_batch_step(hp):
+    """An instance with substeps k takes k of its own steps per batch step and
+    still stops exactly at its max_steps / t_final; results are a lone run's."""
+    cs = [kapila(hp, 60, 50), kapila(hp, 150, 100), kapila(hp, 70, 64, precision=hp.PREC_MIXED)]
+    U = [hp.initial_state(c, "shock_bubble", seed=95 + k, nbubbles=1) for k, c in enumerate(cs)]
+    ce = hp.Config(system=hp.EULER, order=2, nx=40, ny=40, cfl=0.4, gamma1=1.4, gamma2=1.4, pi1=0.0, pi2=0.0)
+    Ue = hp.initial_state(ce, "euler_quadrants", seed=99)
+    with hp.Batch(max_instances=8) as b:
+        a = b.add(cs[0], U[0], 0.0, 1e30, 23)
+        c = b.add(cs[1], U[1], 0.0, 1e30, 6)
+        m = b.add(cs[2], U[2], 0.0, 1e30, 13)
+        e = b.add(ce, Ue, 0.0, 0.02, 100000)
+        b.set_substeps(a, 4)
+        b.set_substeps(m, 3)
+        b.set_substeps(e, 16)
+        b.advance(2)
+        b.sync()
+        assert b.status(a)["steps"] == 8 and b.status(c)["steps"] == 2 and b.status(m)["steps"] == 6
+        assert b.status(a)["substeps"] == 4
+        b.advance(6)
+        b.sync()
+        check_same(hp, b, a, cs[0], U[0], 0.0, 1e30, 23)
+        check_same(hp, b, c, cs[1], U[1], 0.0, 1e30, 6)
+        check_same(hp, b, m, cs[2], U[2], 0.0, 1e30, 13)
+        check_same(hp, b, e, ce, Ue, 0.0, 0.02, 100000)
