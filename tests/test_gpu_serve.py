@@ -53,14 +53,16 @@ def collect(hp, reqs, **kw):
     return res, stats, out
 
 
-@pytest.mark.parametrize("active_cells", [0, 20000])
-def test_each_result_same_alone_and_in_the_mix(hp, active_cells):
+@pytest.mark.parametrize("active_cells,substep_cells", [(0, 0), (20000, 0), (0, 1 << 20)])
+def test_each_result_same_alone_and_in_the_mix(hp, active_cells, substep_cells):
     """active_cells 0: every resident request steps; 20000: the scheduler holds
-    all but the least-remaining-work requests (a few grids' worth of cells)."""
+    all but the least-remaining-work requests (a few grids' worth of cells);
+    substep_cells 2^20: these small grids take 16 steps per batch step."""
     reqs = make_trace(hp, 24, seed=5, spacing_s=0.004)
     sizes = [hp.Batch.instance_bytes(r.cfg) for r in reqs]
     budget = 3 * max(sizes)   # forces waiting for memory
-    res, stats, mixed = collect(hp, reqs, hbm_budget=budget, max_instances=8, poll_ms=2.0, active_cells=active_cells)
+    res, stats, mixed = collect(hp, reqs, hbm_budget=budget, max_instances=8, poll_ms=2.0, active_cells=active_cells,
+                                substep_cells=substep_cells)
     assert stats["completed"] == len(reqs) and stats["failed"] == 0
     assert stats["peak_bytes"] <= budget and stats["peak_instances"] <= 8
     assert stats["peak_instances"] >= 2          # requests overlapped on the device
