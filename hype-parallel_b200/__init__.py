@@ -158,6 +158,12 @@ def lib() -> ctypes.CDLL:
         L.hype_time_stage.argtypes = [vp, ctypes.c_int, _DP]
         L.hype_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.hype_config_default.argtypes = [ctypes.POINTER(_Cfg)]
+        L.hype_get_primitive.argtypes = [vp, _DP]
+        L.hype_solver_config.argtypes = [vp, ctypes.POINTER(_Cfg)]
+        for name in ("hype_write_restart", "hype_read_restart", "hype_write_vts"):
+            getattr(L, name).argtypes = [vp, ctypes.c_char_p]
+        L.hype_solve_monitored.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           ctypes.c_char_p, ctypes.POINTER(ctypes.c_int), _DP, _DP]
         for name in ("hype_ic_shock_bubble",):
             getattr(L, name).argtypes = [ctypes.POINTER(_Cfg), ctypes.c_uint64, ctypes.c_int, _DP]
         for name in ("hype_ic_bn_discs", "hype_ic_euler_quadrants"):
@@ -292,6 +298,32 @@ class Solver:
             raise ValueError("out must be a contiguous float64 array of the state size")
         self._check(lib().hype_get_state(self._h, _ptr(U)))
         return U
+
+    def get_primitive(self) -> np.ndarray:
+        """Primitive variables of the device state (ComputePrimitiveVariables)."""
+        W = np.empty(self.n, dtype=np.float64)
+        self._check(lib().hype_get_primitive(self._h, _ptr(W)))
+        return W
+
+    def write_restart(self, path: str) -> None:
+        self._check(lib().hype_write_restart(self._h, os.fsencode(path)))
+
+    def read_restart(self, path: str) -> int:
+        return lib().hype_read_restart(self._h, os.fsencode(path))
+
+    def write_vts(self, path: str) -> None:
+        self._check(lib().hype_write_vts(self._h, os.fsencode(path)))
+
+    def solve_monitored(self, t0: float, t_final: float, max_steps: int, write_interval: int, restart_interval: int,
+                        directory: str):
+        """hype_solve with MonitorFunction's file schedule; returns (steps, t_end, dt_next)."""
+        steps = ctypes.c_int(0)
+        t = ctypes.c_double(0.0)
+        dt = ctypes.c_double(0.0)
+        self._check(lib().hype_solve_monitored(self._h, t0, t_final, max_steps, write_interval, restart_interval,
+                                               os.fsencode(directory), ctypes.byref(steps), ctypes.byref(t),
+                                               ctypes.byref(dt)))
+        return steps.value, t.value, dt.value
 
     def solve(self, t0: float, t_final: float, max_steps: int, check: bool = True):
         """Returns (steps, t_end, dt_next, status)."""

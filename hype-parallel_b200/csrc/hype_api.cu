@@ -738,6 +738,30 @@ int hype_autotune(hype_solver *s, int reps, int *cells_out, int *waves_out)
     return HYPE_OK;
 }
 
+int hype_solver_config(const hype_solver *s, hype_config *cfg)
+{
+    if (!s || !cfg) return HYPE_ERR_INVALID;
+    *cfg = s->cfg;
+    return HYPE_OK;
+}
+
+int hype_get_primitive(hype_solver *s, double *W)
+{
+    if (!s || !W) return fail(s, HYPE_ERR_INVALID, "null argument");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    const double *planes = s->dU;
+    if (s->mixed) {   // widened to FP64 planes in S0 first
+        CUDA_TRY(s, store_state(s, 0, s->dAosOut));
+        CUDA_TRY(s, launch_aos_to_planes(s->dAosOut, s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream));
+        planes = s->dS0;
+    }
+    const StageParams p = base_params(s);
+    CUDA_TRY(s, launch_cons2prim(s->cfg.system, p.eos, planes, s->dAosOut, s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(W, s->dAosOut, sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return HYPE_OK;
+}
+
 int hype_last_elapsed_ms(const hype_solver *s, double *ms)
 {
     if (!s || !ms) return HYPE_ERR_INVALID;

@@ -159,6 +159,10 @@ cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMa
 cudaError_t launch_aos_to_mixed(const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane, cudaStream_t s);
 cudaError_t launch_mixed_to_aos(const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane, cudaStream_t s);
 
+// hype_io.cu: PDECons2Prim of every cell, planes -> interleaved primitive variables
+cudaError_t launch_cons2prim(int sys, const Eos &eos, const double *planes, double *prim_aos, int nx, int ny, int pitch,
+                             long long plane, cudaStream_t s);
+
 // hype_api.cu, shared with the batch (hype_batch.cu)
 CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, int ny, int nplanes, int pitch, long long plane,
                            int box_w);

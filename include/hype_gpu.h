@@ -154,6 +154,41 @@ HYPE_API int hype_rhs_prim_noalloc(const hype_config *cfg, double t, const doubl
 HYPE_API int hype_set_state(hype_solver *s, const double *U);
 HYPE_API int hype_get_state(hype_solver *s, double *U);
 
+/* Primitive variables of the device state (Vec layout, host memory): what
+ * ComputePrimitiveVariables leaves in Ctx->W (post_process.c:165-200). */
+HYPE_API int hype_get_primitive(hype_solver *s, double *W);
+
+/* The solver's configuration. */
+HYPE_API int hype_solver_config(const hype_solver *s, hype_config *cfg);
+
+/*
+ * The reference's files, from and into the device state:
+ *   hype_write_restart  PETSc binary Vec of the conserved state -- big-endian
+ *                       class id 1211214, length, the doubles in Vec order --
+ *                       as VecView(U) writes restart1/2.bin (post_process.c:47-64),
+ *                       plus the viewer's "<path>.info" (-vecload_block_size nVar);
+ *   hype_read_restart   VecLoad of such a file into the state (hype.c:316-325);
+ *                       the grid must match (HYPE_ERR_INVALID otherwise);
+ *   hype_write_vts      VTK XML structured grid of the primitive variables with
+ *                       the DMDA's cell-centre coordinates and field names, as
+ *                       sol-%08d.vts (post_process.c:25-45, hype.c:388-399), the
+ *                       file HyPE-2D/plot.py reads.
+ */
+HYPE_API int hype_write_restart(hype_solver *s, const char *path);
+HYPE_API int hype_read_restart(hype_solver *s, const char *path);
+HYPE_API int hype_write_vts(hype_solver *s, const char *path);
+
+/*
+ * hype_solve with the reference's output schedule: the files MonitorFunction
+ * writes (post_process.c:12-64) -- sol-%08d.vts every write_interval steps
+ * (step 0 included), restart1.bin when step % restart_interval == 0 and
+ * restart2.bin when (step + 7) % restart_interval == 0 -- and the final
+ * sol-%08d.vts of hype.c:386-399, into directory `dir` (NULL: the current
+ * one).  An interval of 0 writes nothing of that kind.
+ */
+HYPE_API int hype_solve_monitored(hype_solver *s, double t0, double t_final, int max_steps, int write_interval,
+                                  int restart_interval, const char *dir, int *steps_done, double *t_end, double *dt_next);
+
 /*
  * The time loop of HyPE-2D/hype.c:337-384 on the device-resident state: one
  * RHS call at t0 seeds dt (hype.c:343, 356), then SSP-RK steps (N=0 forward
