@@ -152,6 +152,7 @@ def lib() -> ctypes.CDLL:
         L.hype_begin.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
         L.hype_advance.argtypes = [vp, ctypes.c_int]
         L.hype_wait.argtypes = [vp, ctypes.POINTER(ctypes.c_int), _DP, _DP]
+        L.hype_advance_host.argtypes = [vp, _DP, _DP, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _DP, _DP]
         L.hype_totals.argtypes = [vp, ctypes.c_int, _DP, _DP, _DP]
         L.hype_launch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3 + [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
         L.hype_last_elapsed_ms.argtypes = [vp, _DP]
@@ -340,6 +341,21 @@ class Solver:
 
     def advance(self, nsteps: int) -> None:
         self._check(lib().hype_advance(self._h, nsteps))
+
+    def advance_host(self, U_in: np.ndarray, U_out: np.ndarray, nsteps: int = 1):
+        """Host state in, nsteps steps, host state out, copies overlapped with
+        the first and last stages (hype_advance_host); returns (steps, t, dt_next, status)."""
+        for a in (U_in, U_out):
+            if a.size != self.n or a.dtype != np.float64 or not a.flags.c_contiguous:
+                raise ValueError("states must be contiguous float64 arrays of the state size")
+        steps = ctypes.c_int(0)
+        t = ctypes.c_double(0.0)
+        dt = ctypes.c_double(0.0)
+        st = lib().hype_advance_host(self._h, _ptr(U_in), _ptr(U_out), nsteps, ctypes.byref(steps), ctypes.byref(t),
+                                     ctypes.byref(dt))
+        if st not in (OK, ERR_INADMISSIBLE):
+            self._check(st)
+        return steps.value, t.value, dt.value, st
 
     def wait(self):
         steps = ctypes.c_int(0)

@@ -28,6 +28,9 @@ struct hype_solver {
     DevScalars *hSc = nullptr;        // pinned mirror
     CUtensorMap tmU, tmS0, tmS1;
     cudaStream_t stream = nullptr;
+    cudaStream_t cin = nullptr, cout = nullptr;   // host<->device copy streams of the banded calls
+    cudaEvent_t ev_in[8] = {}, ev_done[8] = {};   // per row band: uploaded, computed
+    cudaEvent_t ev_fence = nullptr;               // the compute stream's work so far
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t step_exec = nullptr;
     int cells = STAGE_CELLS;          // tile width of the stage kernel
@@ -232,12 +235,14 @@ static const CUtensorMap &tmap_for(const hype_solver *s, const double *buf)
 }
 
 static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode, double ka, double kb, double kc,
-                         const double *xn, double *out2, int reduce, int out_aos = 0)
+                         const double *xn, double *out2, int reduce, int out_aos = 0, int run0 = 0, int run_count = 0)
 {
     StageParams p = base_params(s);
     p.in = in; p.out = out; p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc; p.xn = xn; p.out2 = out2;
     p.reduce_smax = reduce;
     p.out_aos = out_aos;
+    p.run0 = run0;
+    p.run_count = run_count;
     if (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) return launch_stage_cons(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->stream);
     return launch_stage(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
 }
@@ -338,6 +343,101 @@ static int check_config(const hype_config *c, hype_solver *s)
 }
 
 // ---------------------------------------------------------------------------
+// Banded host calls.  The stages next to a host copy run on a finer row
+// decomposition (up to 8x the runs, at least 8 rows each) grouped into up to
+// 8 bands of rows, launched one band after the other so that each band fills
+// the GPU and finishes early: the host->device copy of later bands overlaps
+// the first stage on earlier ones (band k's stencils read rows of bands
+// k-1..k+1), and the device->host copy of a band overlaps the last stage on
+// the bands after it.  Copies go on their own streams (cin, cout), ordered to
+// the compute stream by events.  Results do not depend on the decomposition.
+// ---------------------------------------------------------------------------
+struct Bands {
+    int n;
+    int runs;     // runs of the banded launches
+    int run[9];   // band k: runs run[k] .. run[k+1]-1
+    int row[9];   //         rows row[k] .. row[k+1]-1 (those runs' own rows)
+    int order[8]; // launch order: band 0 last on a periodic y axis (it reads the last band)
+};
+
+static Bands make_bands(const hype_solver *s)
+{
+    Bands b;
+    const int ny = s->cfg.ny;
+    int runs = 8 * s->runs;
+    if (runs > ny / 8) runs = ny / 8 > s->runs ? ny / 8 : s->runs;
+    if (runs < 1) runs = 1;
+    b.runs = runs;
+    b.n = runs < 8 ? runs : 8;
+    for (int k = 0; k <= b.n; ++k) {
+        b.run[k] = (int)(((long long)k * runs) / b.n);
+        b.row[k] = (int)(((long long)b.run[k] * ny) / runs);
+    }
+    const bool py = s->cfg.bc_bottom == HYPE_BC_PERIODIC && b.n > 1;
+    for (int k = 0; k < b.n; ++k) b.order[k] = py ? (k + 1) % b.n : k;
+    return b;
+}
+
+// the last band whose rows band k's stencils read (the halo is 3 rows, bands are >= 8)
+static int band_needs(const hype_solver *s, const Bands &b, int k)
+{
+    if (k == 0 && s->cfg.bc_bottom == HYPE_BC_PERIODIC) return b.n - 1;
+    return k + 1 < b.n ? k + 1 : b.n - 1;
+}
+
+// the copy streams start after the compute stream's work enqueued so far
+static int fence_copy_streams(hype_solver *s)
+{
+    CUDA_TRY(s, cudaEventRecord(s->ev_fence, s->stream));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->cin, s->ev_fence, 0));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_fence, 0));
+    return HYPE_OK;
+}
+
+// host Vec rows of band k -> planes `dst` (via the staging array); ev_in[k] marks them ready
+static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, double *dst)
+{
+    const size_t row_elems = (size_t)s->cfg.nx * s->nv;
+    const int r0 = b.row[k], nr = b.row[k + 1] - r0;
+    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn + r0 * row_elems, U + r0 * row_elems, sizeof(double) * row_elems * nr,
+                                cudaMemcpyHostToDevice, s->cin));
+    CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, dst, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cin));
+    CUDA_TRY(s, cudaEventRecord(s->ev_in[k], s->cin));
+    return HYPE_OK;
+}
+
+// one stage of `q` over band k's runs of the banded decomposition
+static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanStage &q, int out_aos = 0, double *out = nullptr)
+{
+    const int saved = s->runs;
+    s->runs = b.runs;
+    const cudaError_t e = stage(s, buf_of(s, q.in), out ? out : buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x),
+                                buf_of(s, q.out2), q.reduce, out_aos, b.run[k], b.run[k + 1] - b.run[k]);
+    s->runs = saved;
+    return e;
+}
+
+// First stage of a banded call: uploads of bands 0..n-1 in order, each band
+// launched as soon as the uploads it reads are enqueued (and waited for);
+// `after` runs behind every band launch (e.g. its download).
+template <typename After>
+static int banded_upload_stage(hype_solver *s, const Bands &b, const double *U, double *dst, const PlanStage &q, int out_aos,
+                               double *out, After after)
+{
+    int rc, next = 0;
+    for (int u = 0; u < b.n; ++u) {
+        if ((rc = upload_band(s, b, u, U, dst))) return rc;
+        while (next < b.n && band_needs(s, b, b.order[next]) <= u) {
+            const int k = b.order[next++];
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_in[band_needs(s, b, k)], 0));
+            CUDA_TRY(s, stage_band(s, b, k, q, out_aos, out));
+            if ((rc = after(k))) return rc;
+        }
+    }
+    return HYPE_OK;
+}
+
+// ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
@@ -401,6 +501,13 @@ int hype_destroy(hype_solver *s)
     if (s->hSc) cudaFreeHost(s->hSc);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
+    for (int k = 0; k < 8; ++k) {
+        if (s->ev_in[k]) cudaEventDestroy(s->ev_in[k]);
+        if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
+    }
+    if (s->ev_fence) cudaEventDestroy(s->ev_fence);
+    if (s->cin) { cudaStreamSynchronize(s->cin); cudaStreamDestroy(s->cin); }
+    if (s->cout) { cudaStreamSynchronize(s->cout); cudaStreamDestroy(s->cout); }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return HYPE_OK;
@@ -436,6 +543,13 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(s, cudaEventCreate(&s->ev0));
     CUDA_TRY(s, cudaEventCreate(&s->ev1));
+    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->cin, cudaStreamNonBlocking));
+    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->cout, cudaStreamNonBlocking));
+    for (int k = 0; k < 8; ++k) {
+        CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_in[k], cudaEventDisableTiming));
+        CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming));
+    }
+    CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_fence, cudaEventDisableTiming));
     double **bufs[] = {&s->dU, &s->dS0, &s->dS1};
     for (double **b : bufs) {
         if (cudaMalloc(b, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", state_bytes);
@@ -529,13 +643,40 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
     if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
     if (!s->dSc) return fail(s, HYPE_ERR_INVALID, "solver not created");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
-    const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
-    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
-    CUDA_TRY(s, load_state(s, s->dAosIn, 1));
-    int rc = rhs_common(s, s->dAosOut, dt);
-    if (rc && rc != HYPE_ERR_INADMISSIBLE) return rc;
-    CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    int rc;
+    if (s->mixed) {   // whole-array copies around the mixed kernel
+        const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
+        CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
+        CUDA_TRY(s, load_state(s, s->dAosIn, 1));
+        rc = rhs_common(s, s->dAosOut, dt);
+        if (rc && rc != HYPE_ERR_INADMISSIBLE) return rc;
+        CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+        return rc;
+    }
+    // banded: U's rows stream in while earlier bands compute, RHS rows stream out
+    const Bands b = make_bands(s);
+    const size_t row_elems = (size_t)s->cfg.nx * s->nv;
+    if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
+    const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
+    rc = banded_upload_stage(s, b, U, s->dS0, q, 1, s->dAosOut, [&](int k) -> int {
+        // band k's RHS rows are final: copy them out while later bands compute
+        const int r0 = b.row[k], nr = b.row[k + 1] - r0;
+        CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
+        CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
+        CUDA_TRY(s, cudaMemcpyAsync(RHS + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
+                                    cudaMemcpyDeviceToHost, s->cout));
+        return HYPE_OK;
+    });
+    if (rc) return rc;
+    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
+    if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
+    if (dt) {
+        double smax;
+        const unsigned long long bits = s->hSc->smax;
+        std::memcpy(&smax, &bits, sizeof(smax));
+        *dt = (s->cfg.cfl * s->h) / (2.0 * smax);   // rhs_function_prim.c:620
+    }
     return rc;
 }
 
@@ -616,6 +757,74 @@ int hype_advance(hype_solver *s, int nsteps)
     for (int k = 0; k < nsteps; ++k) CUDA_TRY(s, cudaGraphLaunch(s->step_exec, s->stream));
     CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
     return HYPE_OK;
+}
+
+// One step enqueued by hand (the graph's content), with the first stage's
+// bands waiting for their uploaded rows (upload = U_in) and/or the last
+// stage's bands handed to the copy-out stream (U_out).
+static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_in, double *U_out)
+{
+    PlanStage plan[MAX_PLAN];
+    int copy_back = 0, rc;
+    const int ns = ssp_plan(s->cfg.order, plan, &copy_back);
+    const size_t row_elems = (size_t)s->cfg.nx * s->nv;
+    CUDA_TRY(s, launch_begin_step(s->dSc, s->stream));
+    for (int st = 0; st < ns; ++st) {
+        const PlanStage &q = plan[st];
+        const bool first_in = st == 0 && U_in;
+        const bool last_out = st == ns - 1 && U_out;
+        // band k of the last stage is final: bring its rows to the host while later bands compute
+        auto download = [&](int k) -> int {
+            if (!last_out) return HYPE_OK;
+            const int r0 = b.row[k], nr = b.row[k + 1] - r0;
+            CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
+            CUDA_TRY(s, launch_planes_to_aos_rows(buf_of(s, q.out), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cout));
+            CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
+                                        cudaMemcpyDeviceToHost, s->cout));
+            return HYPE_OK;
+        };
+        if (first_in) {
+            if ((rc = banded_upload_stage(s, b, U_in, buf_of(s, q.in), q, 0, nullptr, download))) return rc;
+        } else if (last_out) {
+            for (int k = 0; k < b.n; ++k) {
+                CUDA_TRY(s, stage_band(s, b, k, q));
+                if ((rc = download(k))) return rc;
+            }
+        } else {
+            CUDA_TRY(s, stage(s, buf_of(s, q.in), buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x), buf_of(s, q.out2),
+                              q.reduce));
+        }
+    }
+    CUDA_TRY(s, launch_end_step(s->dSc, s->cfl_h, s->stream));
+    return HYPE_OK;
+}
+
+int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nsteps, int *steps_done, double *t_end,
+                      double *dt_next)
+{
+    if (!s || !U_in || !U_out || nsteps < 1) return fail(s, HYPE_ERR_INVALID, "bad argument");
+    if (!s->began) return fail(s, HYPE_ERR_INVALID, "hype_begin not called");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    int rc;
+    const bool banded = !s->mixed && s->cfg.order != 0;   // forward Euler's last write is a copy, not a stage
+    if (!banded) {
+        if ((rc = hype_set_state(s, U_in)) || (rc = hype_advance(s, nsteps))) return rc;
+        rc = hype_wait(s, steps_done, t_end, dt_next);
+        if (rc && rc != HYPE_ERR_INADMISSIBLE) return rc;
+        const int rc2 = hype_get_state(s, U_out);
+        return rc ? rc : rc2;
+    }
+    if ((rc = ensure_step_graph(s))) return rc;
+    const Bands b = make_bands(s);
+    if ((rc = fence_copy_streams(s))) return rc;
+    CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
+    if ((rc = enqueue_step_banded(s, b, U_in, nsteps == 1 ? U_out : nullptr))) return rc;
+    for (int k = 1; k + 1 < nsteps; ++k) CUDA_TRY(s, cudaGraphLaunch(s->step_exec, s->stream));
+    if (nsteps > 1 && (rc = enqueue_step_banded(s, b, nullptr, U_out))) return rc;
+    CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
+    return hype_wait(s, steps_done, t_end, dt_next);
 }
 
 int hype_wait(hype_solver *s, int *steps_done, double *t_end, double *dt_next)

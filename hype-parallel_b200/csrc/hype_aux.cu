@@ -7,17 +7,16 @@
 
 namespace hype {
 
-// Interleaved cell-major array (Field{comp[nVar]}, hype.h:68-70) -> planes.
-// One thread per (cell, field); reads and writes are both contiguous in the
-// thread index through a shared-memory tile.
+// Interleaved cell-major array (Field{comp[nVar]}, hype.h:68-70) -> planes,
+// over the cells [cell_begin, cell_end).  One thread per (cell, field); reads
+// and writes are both contiguous in the thread index through a shared-memory tile.
 template <int TILE>
-__global__ void aos_to_planes_kernel(const double *__restrict__ aos, double *__restrict__ planes,
-                                     int nx, int ny, int nv, int pitch, long long plane)
+__global__ void aos_to_planes_kernel(const double *__restrict__ aos, double *__restrict__ planes, int nx, long long cell_begin,
+                                     long long cell_end, int nv, int pitch, long long plane)
 {
     __shared__ double tile[TILE * 9];
-    const long long cell0 = (long long)blockIdx.x * TILE;
-    const long long ncell = (long long)nx * ny;
-    const int ncur = (int)min((long long)TILE, ncell - cell0);
+    const long long cell0 = cell_begin + (long long)blockIdx.x * TILE;
+    const int ncur = (int)min((long long)TILE, cell_end - cell0);
     for (int k = threadIdx.x; k < ncur * nv; k += blockDim.x) tile[k] = aos[cell0 * nv + k];
     __syncthreads();
     for (int k = threadIdx.x; k < ncur * nv; k += blockDim.x) {
@@ -29,13 +28,12 @@ __global__ void aos_to_planes_kernel(const double *__restrict__ aos, double *__r
 }
 
 template <int TILE>
-__global__ void planes_to_aos_kernel(const double *__restrict__ planes, double *__restrict__ aos,
-                                     int nx, int ny, int nv, int pitch, long long plane)
+__global__ void planes_to_aos_kernel(const double *__restrict__ planes, double *__restrict__ aos, int nx, long long cell_begin,
+                                     long long cell_end, int nv, int pitch, long long plane)
 {
     __shared__ double tile[TILE * 9];
-    const long long cell0 = (long long)blockIdx.x * TILE;
-    const long long ncell = (long long)nx * ny;
-    const int ncur = (int)min((long long)TILE, ncell - cell0);
+    const long long cell0 = cell_begin + (long long)blockIdx.x * TILE;
+    const int ncur = (int)min((long long)TILE, cell_end - cell0);
     for (int k = threadIdx.x; k < ncur * nv; k += blockDim.x) {
         const int c = k / ncur, m = k % ncur;
         const long long cell = cell0 + m;
@@ -46,22 +44,36 @@ __global__ void planes_to_aos_kernel(const double *__restrict__ planes, double *
     for (int k = threadIdx.x; k < ncur * nv; k += blockDim.x) aos[cell0 * nv + k] = tile[k];
 }
 
+constexpr int XPOSE_TILE = 256;
+
+cudaError_t launch_aos_to_planes_rows(const double *aos, double *planes, int nx, int row0, int nrows, int nv, int pitch, long long plane,
+                                      cudaStream_t s)
+{
+    const long long c0 = (long long)row0 * nx, c1 = c0 + (long long)nrows * nx;
+    if (c1 <= c0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((c1 - c0 + XPOSE_TILE - 1) / XPOSE_TILE);
+    aos_to_planes_kernel<XPOSE_TILE><<<blocks, 256, 0, s>>>(aos, planes, nx, c0, c1, nv, pitch, plane);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_planes_to_aos_rows(const double *planes, double *aos, int nx, int row0, int nrows, int nv, int pitch, long long plane,
+                                      cudaStream_t s)
+{
+    const long long c0 = (long long)row0 * nx, c1 = c0 + (long long)nrows * nx;
+    if (c1 <= c0) return cudaSuccess;
+    const unsigned blocks = (unsigned)((c1 - c0 + XPOSE_TILE - 1) / XPOSE_TILE);
+    planes_to_aos_kernel<XPOSE_TILE><<<blocks, 256, 0, s>>>(planes, aos, nx, c0, c1, nv, pitch, plane);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_aos_to_planes(const double *aos, double *planes, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s)
 {
-    constexpr int TILE = 256;
-    const long long ncell = (long long)nx * ny;
-    const unsigned blocks = (unsigned)((ncell + TILE - 1) / TILE);
-    aos_to_planes_kernel<TILE><<<blocks, 256, 0, s>>>(aos, planes, nx, ny, nv, pitch, plane);
-    return cudaGetLastError();
+    return launch_aos_to_planes_rows(aos, planes, nx, 0, ny, nv, pitch, plane, s);
 }
 
 cudaError_t launch_planes_to_aos(const double *planes, double *aos, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s)
 {
-    constexpr int TILE = 256;
-    const long long ncell = (long long)nx * ny;
-    const unsigned blocks = (unsigned)((ncell + TILE - 1) / TILE);
-    planes_to_aos_kernel<TILE><<<blocks, 256, 0, s>>>(planes, aos, nx, ny, nv, pitch, plane);
-    return cudaGetLastError();
+    return launch_planes_to_aos_rows(planes, aos, nx, 0, ny, nv, pitch, plane, s);
 }
 
 // dt of the first step from the seeding RHS call (hype.c:343, 356):

@@ -56,6 +56,7 @@ struct StageParams {
     int reduce_smax;            // 1: fold this stage's max wave speed into sc->smax
     const double *inlet;        // [3][ny+6][NV] primitive ghost values for a left inlet (or null)
     int strips, runs;           // tile decomposition: column strips x row runs
+    int run0, run_count;        // grid form: the launch covers runs run0 .. run0+run_count-1 (0: all runs)
 };
 
 // Tile geometry of the stage kernel: a tile is CELLS reconstruction columns
@@ -100,6 +101,11 @@ int ssp_plan(int order, PlanStage *plan, int *copy_back);
 // hype_aux.cu
 cudaError_t launch_aos_to_planes(const double *aos, double *planes, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s);
 cudaError_t launch_planes_to_aos(const double *planes, double *aos, int nx, int ny, int nv, int pitch, long long plane, cudaStream_t s);
+// the same for rows row0 .. row0+nrows-1 only (both arrays are full-grid arrays)
+cudaError_t launch_aos_to_planes_rows(const double *aos, double *planes, int nx, int row0, int nrows, int nv, int pitch, long long plane,
+                                      cudaStream_t s);
+cudaError_t launch_planes_to_aos_rows(const double *planes, double *aos, int nx, int row0, int nrows, int nv, int pitch, long long plane,
+                                      cudaStream_t s);
 cudaError_t launch_begin_step(DevScalars *sc, cudaStream_t s);
 cudaError_t launch_end_step(DevScalars *sc, double cfl_h, cudaStream_t s);
 cudaError_t launch_seed_dt(DevScalars *sc, double cfl_h, cudaStream_t s);

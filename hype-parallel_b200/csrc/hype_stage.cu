@@ -18,7 +18,7 @@ stage_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    stage_tile<SYS, N, CELLS, false>(p, &tmap, blockIdx.x, blockIdx.y, smem_raw, red_s);
+    stage_tile<SYS, N, CELLS, false>(p, &tmap, blockIdx.x, p.run0 + (int)blockIdx.y, smem_raw, red_s);
 }
 
 // Persistent form: the block walks a list of (grid, tile) work items; every grid
@@ -130,7 +130,8 @@ cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap,
     CUtensorMap tm = tmap;
     StageParams pp = p;
     void *args[] = {&tm, &pp};
-    return cudaLaunchKernel(e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
+    const unsigned gy = (unsigned)(p.run_count > 0 ? p.run_count : p.runs);
+    return cudaLaunchKernel(e.single, dim3((unsigned)p.strips, gy, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
 cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,

@@ -17,7 +17,7 @@ stage_cons_kernel(const __grid_constant__ CUtensorMap tmap, const StageParams p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * STAGE_CELLS / 32];
-    stage_tile<SYS, N, STAGE_CELLS, true>(p, &tmap, blockIdx.x, blockIdx.y, smem_raw, red_s);
+    stage_tile<SYS, N, STAGE_CELLS, true>(p, &tmap, blockIdx.x, p.run0 + (int)blockIdx.y, smem_raw, red_s);
 }
 
 struct ConsEntry {
@@ -72,7 +72,8 @@ cudaError_t launch_stage_cons(int sys, int order, const CUtensorMap &tmap, const
     CUtensorMap tm = tmap;
     StageParams pp = p;
     void *args[] = {&tm, &pp};
-    return cudaLaunchKernel(e.fn, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3(2 * STAGE_CELLS, 1, 1), args, e.smem, s);
+    const unsigned gy = (unsigned)(p.run_count > 0 ? p.run_count : p.runs);
+    return cudaLaunchKernel(e.fn, dim3((unsigned)p.strips, gy, 1), dim3(2 * STAGE_CELLS, 1, 1), args, e.smem, s);
 }
 
 }  // namespace hype

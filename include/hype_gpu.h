@@ -207,6 +207,18 @@ HYPE_API int hype_begin(hype_solver *s, double t0, double t_final, int max_steps
 HYPE_API int hype_advance(hype_solver *s, int nsteps);
 HYPE_API int hype_wait(hype_solver *s, int *steps_done, double *t_end, double *dt_next);
 
+/*
+ * Host state in, n steps, host state out: hype_set_state(U_in) +
+ * hype_advance(nsteps) + hype_wait + hype_get_state(U_out), with the copies
+ * overlapped by the computation -- the rows of U_in stream in while the first
+ * stage runs on the rows already there, and the rows of U_out stream out
+ * while the last stage finishes the rows after them.  Needs hype_begin.  U_in
+ * and U_out may be the same array; pinned (page-locked) host memory gives the
+ * overlap its full effect.  Returns what hype_wait returns.
+ */
+HYPE_API int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nsteps, int *steps_done, double *t_end,
+                               double *dt_next);
+
 /* Sums of each conserved variable over the cells (times h^2 when scaled != 0),
  * computed on the device in FP64 with a fixed reduction order; totals has nvar
  * entries.  Also reports min/max of the volume fraction (Kapila, BN). */

@@ -228,3 +228,48 @@ def test_autotuned_tiles_give_identical_bits(hp, orc):
             s.autotune(1)
             R2, dt2, st2 = s.rhs_function_prim(0.0, U2)
             assert st2 == hp.OK and dt2 == dto and R2.tobytes() == Ro.tobytes()
+
+
+@pytest.mark.parametrize("name,nsteps", [("kapila_32x32_bubble_solve", 1), ("kapila_32x32_bubble_solve", 3),
+                                         ("kapila_16x16_solve_N3", 2), ("kapila_24x20_bubble_solve_N1", 2),
+                                         ("bn_20x20_solve", 1), ("euler_32x24_solve", 4), ("kapila_cons_32x32_solve", 2)])
+def test_advance_host_equals_set_advance_get(name, nsteps, hp):
+    """hype_advance_host (copies overlapped with the first and last stages) gives
+    the bits of set_state + advance + wait + get_state."""
+    (_, cfg, kind, seed), t0, tf, nmax = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    pc = cases.to_pkg(cfg)
+    with hp.Solver(pc) as s:
+        s.set_state(U)
+        s.begin(t0, tf, nmax)
+        s.advance(nsteps)
+        ref = (s.wait(), s.get_state())
+    out = np.empty_like(U)
+    with hp.Solver(pc) as s:
+        s.set_state(U)
+        s.begin(t0, tf, nmax)
+        got = s.advance_host(U, out, nsteps)
+    assert got[:3] == ref[0][:3]
+    assert out.tobytes() == ref[1].tobytes()
+
+
+def test_advance_host_large_grid_banded(hp):
+    """A grid large enough for 8 row bands, periodic in y (band 0 reads the last band)."""
+    P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
+    c = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=700, ny=900, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=P, bc_top=P)
+    U = hp.initial_state(c, "shock_bubble", seed=12, nbubbles=3)
+    with hp.Solver(c) as s:
+        s.set_state(U)
+        s.begin(0.0, 1e30, 100)
+        s.advance(2)
+        ref = (s.wait(), s.get_state())
+        R1, dt1, _ = s.rhs_function_prim(0.0, U)
+    out = np.empty_like(U)
+    with hp.Solver(c) as s:
+        assert s.launch_info()["grid"][1] >= 8   # row runs: 8 bands
+        s.set_state(U)
+        s.begin(0.0, 1e30, 100)
+        got = s.advance_host(U, out, 2)
+        R2, dt2, _ = s.rhs_function_prim(0.0, U)
+    assert got[:3] == ref[0][:3] and out.tobytes() == ref[1].tobytes()
+    assert dt1 == dt2 and R1.tobytes() == R2.tobytes()
