@@ -27,6 +27,7 @@ ORACLE_LIB = os.path.join(HERE, "_build", "libhype_oracle.so")
 REF_LIB = {0: os.path.join(HERE, "_ref", "libhype_ref_euler.so"),
            1: os.path.join(HERE, "_ref", "libhype_ref_kapila.so"),
            2: os.path.join(HERE, "_ref", "libhype_ref_bn.so")}
+REF_LIB_VISCOUS = os.path.join(HERE, "_ref", "libhype_ref_kapila_visc.so")   # Kapila built with -DVISCOUS
 
 EULER, KAPILA, BN = 0, 1, 2
 NVAR = {EULER: 4, KAPILA: 6, BN: 9}
@@ -56,6 +57,9 @@ class Config:
     pi2: float = 0.0
     bn_fixed_p2: int = 0
     conservative: int = 0
+    viscous: int = 0          # the VISCOUS build (Kapila, N >= 1)
+    mu1: float = 1.0e-2       # MU_1, MU_2 (hype.h:46-47)
+    mu2: float = 0.0
 
     @property
     def nvar(self) -> int:
@@ -68,7 +72,8 @@ class _HyoConfig(ctypes.Structure):
                 ("y_max", ctypes.c_double), ("cfl", ctypes.c_double),
                 ("bc_left", ctypes.c_int), ("bc_right", ctypes.c_int), ("bc_bottom", ctypes.c_int), ("bc_top", ctypes.c_int),
                 ("gamma1", ctypes.c_double), ("gamma2", ctypes.c_double), ("pi1", ctypes.c_double), ("pi2", ctypes.c_double),
-                ("bn_fixed_p2", ctypes.c_int), ("conservative", ctypes.c_int)]
+                ("bn_fixed_p2", ctypes.c_int), ("conservative", ctypes.c_int), ("viscous", ctypes.c_int),
+                ("mu1", ctypes.c_double), ("mu2", ctypes.c_double)]
 
 
 class _RefConfig(ctypes.Structure):
@@ -76,7 +81,8 @@ class _RefConfig(ctypes.Structure):
                 ("x_min", ctypes.c_double), ("x_max", ctypes.c_double), ("y_min", ctypes.c_double),
                 ("y_max", ctypes.c_double), ("cfl", ctypes.c_double),
                 ("bc_left", ctypes.c_int), ("bc_right", ctypes.c_int), ("bc_bottom", ctypes.c_int), ("bc_top", ctypes.c_int),
-                ("gamma1", ctypes.c_double), ("gamma2", ctypes.c_double), ("pi1", ctypes.c_double), ("pi2", ctypes.c_double)]
+                ("gamma1", ctypes.c_double), ("gamma2", ctypes.c_double), ("pi1", ctypes.c_double), ("pi2", ctypes.c_double),
+                ("mu1", ctypes.c_double), ("mu2", ctypes.c_double)]
 
 
 _DP = ctypes.POINTER(ctypes.c_double)
@@ -95,6 +101,10 @@ def build(ref: bool = False) -> None:
 
 def reference_available() -> bool:
     return all(os.path.exists(p) for p in REF_LIB.values())
+
+
+def viscous_reference_available() -> bool:
+    return os.path.exists(REF_LIB_VISCOUS)
 
 
 class Oracle:
@@ -138,11 +148,14 @@ class Oracle:
 class Reference:
     """The reference's own RHSFunctionPrim/RHSFunction and time loop (oracle/_ref)."""
 
-    def __init__(self, system: int):
-        path = REF_LIB[system]
+    def __init__(self, system: int, viscous: bool = False):
+        if viscous and system != KAPILA:
+            raise ValueError("the reference has a viscous flux for the Kapila system only")
+        path = REF_LIB_VISCOUS if viscous else REF_LIB[system]
         if not os.path.exists(path):
             raise FileNotFoundError(path)
         self.system = system
+        self.viscous = bool(viscous)
         self.lib = ctypes.CDLL(path, mode=os.RTLD_LOCAL | os.RTLD_NOW)
         self.lib.ref_setup.argtypes = [ctypes.POINTER(_RefConfig)]
         self.lib.ref_rhs.argtypes = [ctypes.c_double, _DP, _DP, _DP, ctypes.c_int]
@@ -155,10 +168,12 @@ class Reference:
             raise ValueError("reference library built for another system")
         if cfg.bn_fixed_p2:
             raise ValueError("the reference has only the shipped Baer-Nunziato flux")
+        if bool(cfg.viscous) != self.viscous:
+            raise ValueError("viscous configurations need the VISCOUS build and vice versa")
         rc = _RefConfig(N=cfg.order, nx=cfg.nx, ny=cfg.ny, x_min=cfg.x_min, x_max=cfg.x_max, y_min=cfg.y_min,
                         y_max=cfg.y_max, cfl=cfg.cfl, bc_left=cfg.bc_left, bc_right=cfg.bc_right,
                         bc_bottom=cfg.bc_bottom, bc_top=cfg.bc_top, gamma1=cfg.gamma1, gamma2=cfg.gamma2,
-                        pi1=cfg.pi1, pi2=cfg.pi2)
+                        pi1=cfg.pi1, pi2=cfg.pi2, mu1=cfg.mu1, mu2=cfg.mu2)
         self.lib.ref_setup(ctypes.byref(rc))
         self._cfg = cfg
 

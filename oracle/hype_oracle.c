@@ -233,6 +233,56 @@ static int kap_pad_cons(const eos_t *e, const double *Q)
     return 1;
 }
 
+/* kapila_5eqn.c:377-411: viscous flux in the normal direction from primitive
+ * values V and gradients g[c][dim]; returns the viscous eigenvalue */
+static double kap_visc_prim(const double *V, const double g[][2], double nx, double ny, double mu1, double mu2, double *F)
+{
+    double r2_3 = 2. / 3., r4_3 = 4. / 3.;
+    double phi = V[5];
+    double mu = phi * mu1 + (1.0 - phi) * mu2;
+    double u = V[2], v = V[3];
+    double u_x = g[2][0], u_y = g[2][1], v_x = g[3][0], v_y = g[3][1];
+    double div_v = u_x + v_y;
+    double tau_xx = mu * (2.0 * u_x - r2_3 * div_v);
+    double tau_xy = mu * (u_y + v_x);
+    double tau_yy = mu * (2.0 * v_y - r2_3 * div_v);
+    F[0] = 0.0;
+    F[1] = 0.0;
+    F[2] = -nx * tau_xx - ny * tau_xy;
+    F[3] = -nx * tau_xy - ny * tau_yy;
+    F[4] = -nx * (u * tau_xx + v * tau_xy) - ny * (u * tau_xy + v * tau_yy);
+    F[5] = 0.0;
+    return r4_3 * mu / V[0];
+}
+
+/* kapila_5eqn.c:119-158: the same from conserved values Q and their gradients */
+static double kap_visc_cons(const double *Q, const double g[][2], double nx, double ny, double mu1, double mu2, double *F)
+{
+    double r2_3 = 2. / 3., r4_3 = 4. / 3.;
+    double phi = Q[5];
+    double mu = phi * mu1 + (1.0 - phi) * mu2;
+    double irho = 1.0 / (Q[0] + Q[1]);
+    double u = irho * Q[2];
+    double v = irho * Q[3];
+    double rho_x = g[0][0] + g[1][0];
+    double rho_y = g[0][1] + g[1][1];
+    double u_x = irho * (g[2][0] - u * rho_x);
+    double u_y = irho * (g[2][1] - u * rho_y);
+    double v_x = irho * (g[3][0] - v * rho_x);
+    double v_y = irho * (g[3][1] - v * rho_y);
+    double div_v = u_x + v_y;
+    double tau_xx = mu * (2.0 * u_x - r2_3 * div_v);
+    double tau_xy = mu * (u_y + v_x);
+    double tau_yy = mu * (2.0 * v_y - r2_3 * div_v);
+    F[0] = 0.0;
+    F[1] = 0.0;
+    F[2] = -nx * tau_xx - ny * tau_xy;
+    F[3] = -nx * tau_xy - ny * tau_yy;
+    F[4] = -nx * (u * tau_xx + v * tau_xy) - ny * (u * tau_xy + v * tau_yy);
+    F[5] = 0.0;
+    return r4_3 * mu * irho;
+}
+
 /* ===================================================================== */
 /* Baer-Nunziato, baer_nunziato.c                                         */
 /* ===================================================================== */
@@ -514,6 +564,8 @@ typedef struct {
     void (*ncp)(const eos_t *, const double *, const double *, const double *, double *);
     int (*pad)(const eos_t *, const double *);
     int refl_x[2], refl_y[2];  /* velocity/momentum components negated by a reflective wall (-1: none) */
+    int refl_xv, refl_yv;      /* and the tangential ones the VISCOUS build negates too (-1: none) */
+    double (*visc)(const double *, const double g[][2], double, double, double, double, double *);
 } sys_t;
 
 static int get_sys(const hyo_config *c, sys_t *s)
@@ -525,18 +577,22 @@ static int get_sys(const hyo_config *c, sys_t *s)
         s->nv = 4; s->c2p = eul_cons2prim; s->p2c = eul_prim2cons;
         s->flux = cons ? eul_flux_cons : eul_flux_prim; s->ncp = zero_ncp; s->pad = cons ? eul_pad_cons : eul_pad_prim;
         s->refl_x[0] = 1; s->refl_x[1] = -1; s->refl_y[0] = 2; s->refl_y[1] = -1;   /* rhs_function_prim.c:101-102,230-231 */
+        s->refl_xv = -1; s->refl_yv = -1;   /* no viscous restatement: euler.c:269 writes past nVar */
         return 0;
     case HYO_KAPILA:
         s->nv = 6; s->c2p = kap_cons2prim; s->p2c = kap_prim2cons;
         s->flux = cons ? kap_flux_cons : kap_flux_prim; s->ncp = cons ? kap_ncp_cons : kap_ncp_prim;
         s->pad = cons ? kap_pad_cons : kap_pad_prim;
         s->refl_x[0] = 2; s->refl_x[1] = -1; s->refl_y[0] = 3; s->refl_y[1] = -1;   /* :124-125, :253-254 */
+        s->refl_xv = 3; s->refl_yv = 2;                                             /* :126-127, :255-256 (VISCOUS) */
+        s->visc = cons ? kap_visc_cons : kap_visc_prim;
         return 0;
     case HYO_BN:
         s->nv = 9; s->c2p = bn_cons2prim; s->p2c = bn_prim2cons;
         s->flux = cons ? bn_flux_cons : bn_flux_prim; s->ncp = cons ? bn_ncp_cons : bn_ncp_prim;
         s->pad = cons ? bn_pad_cons : bn_pad_prim;
         s->refl_x[0] = 1; s->refl_x[1] = 5; s->refl_y[0] = 2; s->refl_y[1] = 6;    /* :115-117, :244-246 */
+        s->refl_xv = -1; s->refl_yv = -1;   /* baer_nunziato.c has no viscous flux */
         return 0;
     default:
         return -1;
@@ -740,6 +796,38 @@ static void rec_deg3(const stencil_t *s, double *coeffs)
     coeffs[9] = wt_ratio * u_xyyR4;
 }
 
+/* The unlimited central coefficients u_coeffs that Reconstruct also returns
+ * (reconstruction.c:139-141, 172-174, 195-196, 217, 258-267); the VISCOUS
+ * build takes the face gradients from them.  N = 0 leaves them unset in the
+ * reference, so the viscous path starts at N = 1. */
+static void ucoef(int N, const stencil_t *s, double *uc)
+{
+    const double u_0 = s->c;
+    uc[0] = u_0;
+    if (N == 1) {
+        uc[1] = 0.5 * (s->xp1 - s->xm1);
+        uc[2] = 0.5 * (s->yp1 - s->ym1);
+    } else if (N == 2) {
+        uc[1] = 0.5 * (s->xp1 - s->xm1);
+        uc[3] = 0.5 * (s->xm1 - 2.0 * u_0 + s->xp1);
+        uc[2] = 0.5 * (s->yp1 - s->ym1);
+        uc[4] = 0.5 * (s->ym1 - 2.0 * u_0 + s->yp1);
+        uc[5] = 0.25 * (s->pp - s->pm - s->mp + s->mm);
+    } else if (N == 3) {
+        const double u_ip1 = s->xp1, u_jp1 = s->yp1, u_ip1jp1 = s->pp, u_im1 = s->xm1, u_jm1 = s->ym1, u_ip1jm1 = s->pm;
+        const double u_ip2 = s->xp2, u_jp2 = s->yp2, u_im1jp1 = s->mp, u_im2 = s->xm2, u_jm2 = s->ym2, u_im1jm1 = s->mm;
+        uc[1] = R41_60 * (-u_im1 + u_ip1) + R11_120 * (u_im2 - u_ip2);
+        uc[2] = R41_60 * (-u_jm1 + u_jp1) + R11_120 * (u_jm2 - u_jp2);
+        uc[3] = -u_0 + 0.5 * (u_im1 + u_ip1);
+        uc[4] = -u_0 + 0.5 * (u_jm1 + u_jp1);
+        uc[5] = 0.25 * (u_im1jm1 - u_im1jp1 - u_ip1jm1 + u_ip1jp1);
+        uc[6] = R1_6 * (u_im1 - u_ip1) + R1_12 * (u_ip2 - u_im2);
+        uc[7] = R1_6 * (u_jm1 - u_jp1) + R1_12 * (u_jp2 - u_jm2);
+        uc[8] = 0.25 * (-u_im1jm1 + u_im1jp1 - u_ip1jm1 + u_ip1jp1) + 0.5 * (u_jm1 - u_jp1);
+        uc[9] = 0.5 * (u_im1 - u_ip1) + 0.25 * (u_ip1jp1 - u_im1jm1 - u_im1jp1 + u_ip1jm1);
+    }
+}
+
 /* ===================================================================== */
 /* quadrature tables (hype.c:194-305)                                      */
 /* ===================================================================== */
@@ -750,6 +838,7 @@ typedef struct {
     double phi_face[4][2][MAXDOF];          /* [face L,R,B,T][gp][k] */
     double phi_node[8][MAXDOF];
     double phi_vol[4][MAXDOF], dphi_vol_x[4][MAXDOF], dphi_vol_y[4][MAXDOF];
+    double dphi_face[4][2][2][MAXDOF];      /* [face][gp][dim][k]: gradphiFace_x / _y (hype.c:255-285) */
 } tables_t;
 
 static void make_tables(int N, tables_t *T)
@@ -778,6 +867,10 @@ static void make_tables(int N, tables_t *T)
             T->phi_face[1][q][k] = basis_val(0.5, xf[q], k);
             T->phi_face[2][q][k] = basis_val(xf[q], -0.5, k);
             T->phi_face[3][q][k] = basis_val(xf[q], 0.5, k);
+            basis_grad_val(-0.5, xf[q], k, &T->dphi_face[0][q][0][k], &T->dphi_face[0][q][1][k]);
+            basis_grad_val(0.5, xf[q], k, &T->dphi_face[1][q][0][k], &T->dphi_face[1][q][1][k]);
+            basis_grad_val(xf[q], -0.5, k, &T->dphi_face[2][q][0][k], &T->dphi_face[2][q][1][k]);
+            basis_grad_val(xf[q], 0.5, k, &T->dphi_face[3][q][0][k], &T->dphi_face[3][q][1][k]);
         }
     for (int q = 0; q < T->nnode; ++q)
         for (int k = 0; k < T->ndof; ++k) T->phi_node[q][k] = basis_val(xn[q], yn[q], k);
@@ -811,6 +904,8 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
     (void)t;
     if (get_sys(cfg, &S)) return HYO_ERR_CONFIG;
     if (cfg->order < 0 || cfg->order > 3 || cfg->nx < 1 || cfg->ny < 1) return HYO_ERR_CONFIG;
+    const int visc = cfg->viscous != 0;
+    if (visc && (!S.visc || cfg->order < 1)) return HYO_ERR_CONFIG;
     int bcs[4] = {cfg->bc_left, cfg->bc_right, cfg->bc_bottom, cfg->bc_top};
     for (int k = 0; k < 4; ++k) {
         if (bcs[k] == HYO_BC_WALL || bcs[k] < 0 || bcs[k] > 4) return HYO_ERR_CONFIG;   /* wall: ghosts never set by the reference */
@@ -860,6 +955,7 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
             } else if (bc == HYO_BC_REFLECTIVE) {
                 memcpy(dst, WAT(j, left ? -1 - i : 2 * (nx - 1) - i + 1), sizeof(double) * nv);
                 for (int r = 0; r < 2; ++r) if (S.refl_x[r] >= 0) dst[S.refl_x[r]] = -dst[S.refl_x[r]];
+                if (visc) dst[S.refl_xv] = -dst[S.refl_xv];
             } else if (bc == HYO_BC_INLET) {
                 double x_loc = cfg->x_min + ((double)i + 0.5) * h;
                 double y_loc = cfg->y_min + ((double)j + 0.5) * h;
@@ -878,6 +974,7 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
             } else if (bc == HYO_BC_REFLECTIVE) {
                 memcpy(dst, WAT(bot ? -1 - j : 2 * (ny - 1) - j + 1, i), sizeof(double) * nv);
                 for (int r = 0; r < 2; ++r) if (S.refl_y[r] >= 0) dst[S.refl_y[r]] = -dst[S.refl_y[r]];
+                if (visc) dst[S.refl_yv] = -dst[S.refl_yv];
             }
         }
     }
@@ -887,6 +984,9 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
     const int cw = nx + 2, ch = ny + 2;
     double *C = (double *)calloc((size_t)cw * ch * ndof * nv, sizeof(double));
 #define CAT(j, i) (C + ((size_t)((j) + 1) * cw + (size_t)((i) + 1)) * (size_t)ndof * nv)   /* [k][c] */
+    /* VISCOUS: the unlimited coefficients of every reconstructed cell, [k][c] */
+    double *UC = visc ? (double *)calloc((size_t)cw * ch * ndof * nv, sizeof(double)) : NULL;
+#define UCAT(j, i) (UC + ((size_t)((j) + 1) * cw + (size_t)((i) + 1)) * (size_t)ndof * nv)
     for (int j = -1; j <= ny; ++j)
         for (int i = -1; i <= nx; ++i) {
             if ((j < 0 || j >= ny) && (i < 0 || i >= nx)) continue;
@@ -904,6 +1004,11 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
                 else if (N == 2) rec_deg2(&s, coef);
                 else rec_deg3(&s, coef);
                 for (int k = 0; k < ndof; ++k) cf[k * nv + c] = coef[k];
+                if (visc) {
+                    double uc[MAXDOF];
+                    ucoef(N, &s, uc);
+                    for (int k = 0; k < ndof; ++k) UCAT(j, i)[k * nv + c] = uc[k];
+                }
             }
             /* admissibility at the nodes (rhs_function_prim.c:382-404) */
             int pad = 1;
@@ -935,7 +1040,7 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
     double *Dx = (double *)malloc(sizeof(double) * (size_t)(nx + 1) * ny * nv);
     double *Gy = (double *)malloc(sizeof(double) * (size_t)nx * (ny + 1) * nv);
     double *Ey = (double *)malloc(sizeof(double) * (size_t)nx * (ny + 1) * nv);
-    double s_max_c = 0.0;
+    double s_max_c = 0.0, s_max_v = 0.0;
     int bad = 0;
     for (int dir = 0; dir < 2; ++dir) {
         const double nxv = dir == 0 ? 1.0 : 0.0, nyv = dir == 0 ? 0.0 : 1.0;
@@ -978,9 +1083,33 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
                     }
                     S.ncp(&eos, Vav, gxv, gyv, Dc);
                     if (s > s_max_c) s_max_c = s;
+                    double Fv[MAXV];
+                    if (visc) {
+                        /* rhs_function_prim.c:356-374 (face gradients from u_coeffs) and
+                         * riemann.c:146-186 (ViscRiemannSolver[Prim]: the mean of both sides) */
+                        const double *ul = dir == 0 ? UCAT(j, i - 1) : UCAT(j - 1, i), *ur = UCAT(j, i);
+                        const int fl = dir == 0 ? 1 : 3, fr = dir == 0 ? 0 : 2;
+                        double gL[MAXV][2], gR[MAXV][2], FvL[MAXV], FvR[MAXV];
+                        for (int c = 0; c < nv; ++c)
+                            for (int d = 0; d < 2; ++d) {
+                                double al = 0.0, ar = 0.0;
+                                for (int k = 0; k < ndof; ++k) {
+                                    al += ul[k * nv + c] * T.dphi_face[fl][q][d][k];
+                                    ar += ur[k * nv + c] * T.dphi_face[fr][q][d][k];
+                                }
+                                gL[c][d] = r1_h * al;
+                                gR[c][d] = r1_h * ar;
+                            }
+                        double svl = S.visc(VL, (const double(*)[2])gL, nxv, nyv, cfg->mu1, cfg->mu2, FvL);
+                        double svr = S.visc(VR, (const double(*)[2])gR, nxv, nyv, cfg->mu1, cfg->mu2, FvR);
+                        double sv = (svl < svr) ? svr : svl;
+                        for (int c = 0; c < nv; ++c) Fv[c] = 0.5 * (FvR[c] + FvL[c]);
+                        if (sv > s_max_v) s_max_v = sv;
+                    }
                     for (int c = 0; c < nv; ++c) {
                         Flux[c] += T.wf[q] * Fc[c];
                         NCP[c] += T.wf[q] * Dc[c];
+                        if (visc) Flux[c] += T.wf[q] * Fv[c];
                     }
                 }
                 double *fo = (dir == 0 ? Fx + ((size_t)j * (nx + 1) + i) * nv : Gy + ((size_t)j * nx + i) * nv);
@@ -1019,8 +1148,12 @@ int hyo_rhs(const hyo_config *cfg, double t, const double *U, double *RHS, doubl
         }
 #undef CAT
 #undef WAT
-    free(W); free(C); free(Fx); free(Dx); free(Gy); free(Ey);
-    if (dt_out) *dt_out = (cfg->cfl * h) / (2.0 * s_max_c);   /* rhs_function_prim.c:620 */
+#undef UCAT
+    free(W); free(C); free(UC); free(Fx); free(Dx); free(Gy); free(Ey);
+    if (dt_out) {
+        if (visc) *dt_out = (cfg->cfl * h) / (2.0 * (s_max_c + (r1_h * s_max_v) * 2.0));   /* rhs_function_prim.c:617 */
+        else *dt_out = (cfg->cfl * h) / (2.0 * s_max_c);                                 /* rhs_function_prim.c:620 */
+    }
     return bad ? HYO_ERR_INADMISSIBLE : HYO_OK;
 }
 

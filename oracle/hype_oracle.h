@@ -29,6 +29,8 @@ typedef struct {
     double gamma1, gamma2, pi1, pi2;
     int bn_fixed_p2;     /* 0: Baer-Nunziato flux pressure as the reference has it (p2 = alpha1) */
     int conservative;    /* 0: RHSFunctionPrim, 1: RHSFunction (reconstruct conserved variables) */
+    int viscous;         /* 1: the VISCOUS build of the reference (Kapila, N >= 1): viscous face fluxes */
+    double mu1, mu2;     /* MU_1, MU_2 (hype.h:46-47) */
 } hyo_config;
 
 /* status codes */

@@ -10,8 +10,9 @@
  *   - the PDE system (#define EULER / KAPILA_5EQN / BAER_NUNZIATO) and nVar
  *     come from the command line (hype.h:33-37 hard-codes KAPILA_5EQN, 6);
  *   - the stiffened-gas constants GAMMA_1, GAMMA_2, PI_1, PI_2 (hype.h:42-45,
- *     `static const` there) are run-time globals set by the driver, so the
- *     EOS of each config (e.g. PI_1 = 6e8) needs no rebuild.  Expressions in
+ *     `static const` there) and the viscosities MU_1, MU_2 (hype.h:46-47) are
+ *     run-time globals set by the driver, so the EOS of each config (e.g.
+ *     PI_1 = 6e8) needs no rebuild.  Expressions in
  *     the sources evaluate identically: a constant folded at compile time and
  *     the same IEEE operation at run time round the same way;
  *   - PETSc comes from petsc_mini.h (one rank).
@@ -31,8 +32,7 @@
 #define DIM 2
 
 extern PetscReal GAMMA_1, GAMMA_2, PI_1, PI_2;
-static const PetscReal MU_1 = 1.0e-2;
-static const PetscReal MU_2 = 0.0;
+extern PetscReal MU_1, MU_2;   /* hype.h:46-47 (1.0e-2, 0.0): run-time like the EOS constants */
 static const PetscReal G_A  = 9.8;
 
 static const PetscReal prs_floor = 1.0e-12;

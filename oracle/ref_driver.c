@@ -18,6 +18,7 @@
 #include <setjmp.h>
 
 PetscReal GAMMA_1 = 1.4, GAMMA_2 = 1.4, PI_1 = 0.0, PI_2 = 0.0;
+PetscReal MU_1 = 1.0e-2, MU_2 = 0.0;
 
 /* Symbols that hype.h declares but the chosen PDE file does not define (they
  * are only reached from code paths the oracle does not take: inlet BCs for
@@ -44,6 +45,7 @@ typedef struct {
     double cfl;
     int bc_left, bc_right, bc_bottom, bc_top;   /* enum bndry_type values */
     double gamma1, gamma2, pi1, pi2;
+    double mu1, mu2;          /* MU_1, MU_2: read by the VISCOUS build only */
 } ref_cfg;
 
 static AppCtx Ctx;
@@ -59,7 +61,10 @@ void ref_teardown(void)
     if (!g_ready) return;
     VecDestroy(&U); VecDestroy(&RHS); VecDestroy(&Ctx.W); VecDestroy(&Ctx.localU);
     TSDestroy(&ts_rhs);
-    free5d(Ctx.u_bnd); free3d(Ctx.F); free3d(Ctx.G); free3d(Ctx.D); free3d(Ctx.E);
+    free5d(Ctx.u_bnd); free3d(Ctx.F);
+#ifdef VISCOUS
+    free6d(Ctx.u_bnd_grad);
+#endif free3d(Ctx.G); free3d(Ctx.D); free3d(Ctx.E);
     free3d(Ctx.phiFace); free2d(Ctx.phiNode); free2d(Ctx.phiVol);
     free2d(Ctx.gradphiVol_x); free2d(Ctx.gradphiVol_y);
     free3d(Ctx.gradphiFace_x); free3d(Ctx.gradphiFace_y);
@@ -73,6 +78,7 @@ int ref_setup(const ref_cfg *cfg)
 {
     ref_teardown();
     GAMMA_1 = cfg->gamma1; GAMMA_2 = cfg->gamma2; PI_1 = cfg->pi1; PI_2 = cfg->pi2;
+    MU_1 = cfg->mu1; MU_2 = cfg->mu2;
     memset(&Ctx, 0, sizeof(Ctx));
     Ctx.N = cfg->N;
     Ctx.x_min = cfg->x_min; Ctx.x_max = cfg->x_max; Ctx.y_min = cfg->y_min; Ctx.y_max = cfg->y_max;
@@ -117,6 +123,9 @@ int ref_setup(const ref_cfg *cfg)
     PetscInt xs, ys, xm, ym;
     DMDAGetCorners(da, &xs, &ys, NULL, &xm, &ym, NULL);
     Ctx.u_bnd = allocate5d(ym + 2, xm + 2, nVar, 4, Ctx.Ngp_Face);
+#ifdef VISCOUS
+    Ctx.u_bnd_grad = allocate6d(ym + 2, xm + 2, nVar, 4, Ctx.Ngp_Face, DIM);   /* hype.c:238-240 */
+#endif
     Ctx.F = allocate3d(ym, xm + 1, nVar);
     Ctx.G = allocate3d(ym + 1, xm, nVar);
     Ctx.D = allocate3d(ym, xm + 1, nVar);

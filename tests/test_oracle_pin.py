@@ -105,3 +105,30 @@ def test_oracle_conservative_path_vs_live_reference(orc):
         R2, dt2, s2 = orc.rhs(cfg, U)
         assert s1 == 0 and s2 == 0
         assert dt1 == dt2 and R1.tobytes() == R2.tobytes()
+
+
+@pytest.mark.skipif(not O.viscous_reference_available(), reason="oracle/_ref not built (needs the reference sources)")
+@pytest.mark.parametrize("conservative", [0, 1])
+@pytest.mark.parametrize("order", [1, 2, 3])
+def test_oracle_viscous_vs_live_reference(conservative, order, orc):
+    """The VISCOUS build of the reference (Kapila; hype.h:36 leaves it off):
+    face gradients from the unlimited coefficients, ViscRiemannSolver[Prim],
+    tangential reflection at walls and the viscous dt."""
+    T, R, P, I = O.TRANSMISSIVE, O.REFLECTIVE, O.PERIODIC, O.INLET
+    ref = O.Reference(O.KAPILA, viscous=True)
+    for bcs, kind, mu in (((R, R, R, R), "rough", (0.3, 0.05)), ((T, T, P, P), "bubble", (1e-2, 0.0)),
+                          ((R, T, R, T), "bubble", (2.0, 0.5)), ((I, T, R, R), "rough", (0.1, 0.0))):
+        ext = dict(x_min=0.0, x_max=2.0, y_min=-1.0, y_max=0.6) if bcs[0] == I else {}
+        cfg = O.Config(system=O.KAPILA, order=order, nx=23, ny=17, bc_left=bcs[0], bc_right=bcs[1], bc_bottom=bcs[2],
+                       bc_top=bcs[3], conservative=conservative, viscous=1, mu1=mu[0], mu2=mu[1], **cases.KAPILA_EOS, **ext)
+        U = cases.state(cfg, kind, 5 + order)
+        ref.setup(cfg)
+        R1, dt1, s1 = ref.rhs(U)
+        R2, dt2, s2 = orc.rhs(cfg, U)
+        assert (s1 == 0) == (s2 == 0)
+        if s1 == 0:
+            assert dt1 == dt2 and R1.tobytes() == R2.tobytes()
+        if kind == "bubble":
+            U1, n1, t1, d1, st1 = ref.solve(U, 0.0, 1.0, 3)
+            U2, n2, t2, d2, st2 = orc.solve(cfg, U, 0.0, 1.0, 3)
+            assert st1 == 0 and st2 == 0 and (n1, t1, d1) == (n2, t2, d2) and U1.tobytes() == U2.tobytes()
