@@ -31,6 +31,7 @@ BC_WALL, BC_INLET, BC_PERIODIC, BC_REFLECTIVE, BC_TRANSMISSIVE = 0, 1, 2, 3, 4
 PREC_FP64, PREC_MIXED = 0, 1
 FLAG_BN_FIX_P2 = 1
 FLAG_CONSERVATIVE = 2
+FLAG_VISCOUS = 4
 NVAR = {EULER: 4, KAPILA_5EQN: 6, BAER_NUNZIATO: 9}
 
 
@@ -46,7 +47,8 @@ class _Cfg(ctypes.Structure):
                 ("y_max", ctypes.c_double), ("cfl", ctypes.c_double),
                 ("bc_left", ctypes.c_int), ("bc_right", ctypes.c_int), ("bc_bottom", ctypes.c_int), ("bc_top", ctypes.c_int),
                 ("gamma1", ctypes.c_double), ("gamma2", ctypes.c_double), ("pi1", ctypes.c_double), ("pi2", ctypes.c_double),
-                ("precision", ctypes.c_int), ("flags", ctypes.c_uint), ("device", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("flags", ctypes.c_uint), ("device", ctypes.c_int),
+                ("mu1", ctypes.c_double), ("mu2", ctypes.c_double)]
 
 
 @dataclasses.dataclass
@@ -72,6 +74,8 @@ class Config:
     precision: int = PREC_FP64
     flags: int = 0
     device: int = 0
+    mu1: float = 1.0e-2      # MU_1, MU_2 (hype.h:46-47), read with FLAG_VISCOUS
+    mu2: float = 0.0
 
     @property
     def nvar(self) -> int:

@@ -166,6 +166,8 @@ static StageParams base_params(const hype_solver *s)
     p.eos.fix_p2 = (s->cfg.flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
     p.r1_h = s->r1_h;
     p.cfl_h = s->cfl_h;
+    p.mu1 = s->cfg.mu1;
+    p.mu2 = s->cfg.mu2;
     p.sc = s->dSc;
     p.inlet = s->dInlet;
     p.kb = 1.0;
@@ -206,7 +208,13 @@ static int set_tiling(hype_solver *s, int cells, int waves = 1)
         if (s->step_exec) { cudaGraphExecDestroy(s->step_exec); s->step_exec = nullptr; }
         return HYPE_OK;
     }
-    if (cfg->flags & HYPE_FLAG_CONSERVATIVE) {   // the conservative kernels come in 128-column tiles only
+    if (cfg->flags & HYPE_FLAG_VISCOUS) {   // the viscous kernels come in 128-column tiles only
+        cells = STAGE_CELLS;
+        s->cells = cells;
+        const bool cons = (cfg->flags & HYPE_FLAG_CONSERVATIVE) != 0;
+        CUDA_TRY(s, stage_visc_configure(cfg->order, cons));
+        s->bps = stage_visc_blocks_per_sm(cfg->order, cons);
+    } else if (cfg->flags & HYPE_FLAG_CONSERVATIVE) {   // the conservative kernels come in 128-column tiles only
         cells = STAGE_CELLS;
         s->cells = cells;
         CUDA_TRY(s, stage_cons_configure(cfg->system, cfg->order));
@@ -243,6 +251,8 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
     p.out_aos = out_aos;
     p.run0 = run0;
     p.run_count = run_count;
+    if (s->cfg.flags & HYPE_FLAG_VISCOUS)
+        return launch_stage_visc(s->cfg.order, (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) != 0, tmap_for(s, in), p, s->stream);
     if (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) return launch_stage_cons(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->stream);
     return launch_stage(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
 }
@@ -337,8 +347,12 @@ static int check_config(const hype_config *c, hype_solver *s)
         return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for N = 2 without inlet boundaries");
     if (c->precision == HYPE_PREC_MIXED && (c->flags & HYPE_FLAG_CONSERVATIVE))
         return fail(s, HYPE_ERR_INVALID, "the conservative-variable path is FP64 only");
-    if (c->flags & ~(HYPE_FLAG_BN_FIX_P2 | HYPE_FLAG_CONSERVATIVE))
+    if (c->flags & ~(HYPE_FLAG_BN_FIX_P2 | HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS))
         return fail(s, HYPE_ERR_INVALID, "unknown flags 0x%x", c->flags);
+    if ((c->flags & HYPE_FLAG_VISCOUS) &&
+        (c->system != HYPE_KAPILA_5EQN || c->order < 1 || c->precision != HYPE_PREC_FP64))
+        return fail(s, HYPE_ERR_INVALID, "the viscous path exists for the Kapila system, N = 1..3, FP64 "
+                                         "(the reference's other systems have no usable viscous flux; N = 0 has no gradients)");
     return HYPE_OK;
 }
 
@@ -458,6 +472,7 @@ void hype_config_default(hype_config *c)
     c->precision = HYPE_PREC_FP64;
     c->flags = 0;
     c->device = 0;
+    c->mu1 = 1.0e-2; c->mu2 = 0.0;      // hype.h:46-47
 }
 
 int hype_nvar(int system)
@@ -586,6 +601,19 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     return set_tiling(s, s->mixed ? MIXED_CELLS : STAGE_CELLS);
 }
 
+// dt of the last RHS: CFL h / (2 s_max) (rhs_function_prim.c:620), or
+// CFL h / (2 (s_max + (s_max_v / h) 2)) for a viscous solver (:617); the two
+// agree bit for bit when s_max_v and r1h_v are 0
+static double host_dt(const hype_solver *s)
+{
+    double smax, smaxv;
+    const unsigned long long b0 = s->hSc->smax, b1 = s->hSc->smax_v;
+    std::memcpy(&smax, &b0, sizeof(smax));
+    std::memcpy(&smaxv, &b1, sizeof(smaxv));
+    if (!(s->cfg.flags & HYPE_FLAG_VISCOUS)) return (s->cfg.cfl * s->h) / (2.0 * smax);
+    return (s->cfg.cfl * s->h) / (2.0 * (smax + (s->r1_h * smaxv) * 2.0));
+}
+
 static int read_scalars(hype_solver *s)
 {
     CUDA_TRY(s, cudaMemcpyAsync(s->hSc, s->dSc, sizeof(DevScalars), cudaMemcpyDeviceToHost, s->stream));
@@ -604,6 +632,7 @@ static int reset_scalars(hype_solver *s)
 {
     std::memset(s->hSc, 0, sizeof(DevScalars));
     s->hSc->err_cell = 0xffffffffu;
+    s->hSc->r1h_v = (s->cfg.flags & HYPE_FLAG_VISCOUS) ? s->r1_h : 0.0;
     CUDA_TRY(s, cudaMemcpyAsync(s->dSc, s->hSc, sizeof(DevScalars), cudaMemcpyHostToDevice, s->stream));
     return HYPE_OK;
 }
@@ -629,10 +658,7 @@ static int rhs_common(hype_solver *s, double *dRHS_aos, double *dt)
     else CUDA_TRY(s, stage(s, s->dS0, dRHS_aos, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
     if ((rc = read_scalars(s))) return rc;
     if (dt) {
-        double smax;
-        const unsigned long long bits = s->hSc->smax;
-        std::memcpy(&smax, &bits, sizeof(smax));
-        *dt = (s->cfg.cfl * s->h) / (2.0 * smax);   // rhs_function_prim.c:620
+        *dt = host_dt(s);
     }
     return HYPE_OK;
 }
@@ -672,10 +698,7 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
     CUDA_TRY(s, cudaStreamSynchronize(s->cout));
     if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
     if (dt) {
-        double smax;
-        const unsigned long long bits = s->hSc->smax;
-        std::memcpy(&smax, &bits, sizeof(smax));
-        *dt = (s->cfg.cfl * s->h) / (2.0 * smax);   // rhs_function_prim.c:620
+        *dt = host_dt(s);
     }
     return rc;
 }

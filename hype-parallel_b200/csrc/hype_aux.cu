@@ -76,13 +76,23 @@ cudaError_t launch_planes_to_aos(const double *planes, double *aos, int nx, int 
     return launch_planes_to_aos_rows(planes, aos, nx, 0, ny, nv, pitch, plane, s);
 }
 
-// dt of the first step from the seeding RHS call (hype.c:343, 356):
-// dt = CFL h / (2 s_max)  (rhs_function_prim.c:620)
-__global__ void seed_dt_kernel(DevScalars *sc, double cfl_h)
+// dt from the last RHS's maxima: CFL h / (2 s_max) (rhs_function_prim.c:620),
+// or, for a viscous solver, CFL h / (2 (s_max + (s_max_v / h) 2))
+// (rhs_function_prim.c:617).  Both in one expression: r1h_v = 0 makes the
+// viscous term an exact +0, and s_max + 0 = s_max.
+__device__ __forceinline__ double next_dt(const DevScalars *sc, double cfl_h)
 {
     const double smax = __longlong_as_double((long long)sc->smax);
-    sc->time_step = cfl_h / (2.0 * smax);
+    const double smaxv = __longlong_as_double((long long)sc->smax_v);
+    return cfl_h / (2.0 * (smax + (sc->r1h_v * smaxv) * 2.0));
+}
+
+// dt of the first step from the seeding RHS call (hype.c:343, 356)
+__global__ void seed_dt_kernel(DevScalars *sc, double cfl_h)
+{
+    sc->time_step = next_dt(sc, cfl_h);
     sc->smax = 0ull;
+    sc->smax_v = 0ull;
 }
 
 // Start of a step: the monitor hands TS the last RHS's dt; TS stops at
@@ -101,14 +111,14 @@ __device__ __forceinline__ void begin_step(DevScalars *sc)
     if (sc->t + dt > sc->t_final) dt = sc->t_final - sc->t;
     sc->dt = dt;
     sc->smax = 0ull;
+    sc->smax_v = 0ull;
 }
 
 // End of a step: the last stage's RHS set Ctx->dt for the next step.
 __device__ __forceinline__ void end_step(DevScalars *sc, double cfl_h)
 {
     if (sc->idle) return;
-    const double smax = __longlong_as_double((long long)sc->smax);
-    sc->time_step = cfl_h / (2.0 * smax);
+    sc->time_step = next_dt(sc, cfl_h);
     sc->t = sc->t + sc->dt;
     sc->steps = sc->steps + 1;
 }

@@ -504,7 +504,8 @@ const char *hype_batch_last_error(const hype_batch *b) { return b ? b->err : "nu
 
 size_t hype_batch_instance_bytes(const hype_config *cfg)
 {
-    if (!cfg || validate_config(cfg, nullptr, 0) != HYPE_OK || (cfg->flags & HYPE_FLAG_CONSERVATIVE)) return 0;
+    if (!cfg || validate_config(cfg, nullptr, 0) != HYPE_OK || (cfg->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS)))
+        return 0;
     return state_bytes(*cfg);
 }
 
@@ -605,8 +606,9 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     char msg[256];
     int rc = validate_config(cfg, msg, sizeof(msg));
     if (rc) return bfail(b, rc, "%s", msg);
-    if (cfg->flags & HYPE_FLAG_CONSERVATIVE)
-        return bfail(b, HYPE_ERR_INVALID, "batches run the primitive-variable path (HYPE_FLAG_CONSERVATIVE is for solvers)");
+    if (cfg->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS))
+        return bfail(b, HYPE_ERR_INVALID, "batches run the inviscid primitive-variable path "
+                                          "(HYPE_FLAG_CONSERVATIVE and HYPE_FLAG_VISCOUS are for solvers)");
     if ((long long)cfg->nx * cfg->ny > b->cfg.max_cells)
         return bfail(b, HYPE_ERR_INVALID, "grid %dx%d exceeds the batch's max_cells (%lld)", cfg->nx, cfg->ny, (long long)b->cfg.max_cells);
     int s = -1;

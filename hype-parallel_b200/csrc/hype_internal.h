@@ -28,6 +28,8 @@ struct DevScalars {
     double t_final;
     double time_step;          // dt proposed by the last RHS (MonitorFunction / Ctx->dt)
     unsigned long long smax;   // bit pattern of max wave speed of the RHS being reduced
+    unsigned long long smax_v; // bit pattern of max viscous eigenvalue (viscous solvers)
+    double r1h_v;              // 1/h for viscous solvers, 0 otherwise: dt = CFL h / (2 (smax + (r1h_v smax_v) 2))
     unsigned int err;          // ERR_* bits
     unsigned int err_cell;     // linear index of the first cell that raised an error
     int steps, max_steps;
@@ -57,6 +59,7 @@ struct StageParams {
     const double *inlet;        // [3][ny+6][NV] primitive ghost values for a left inlet (or null)
     int strips, runs;           // tile decomposition: column strips x row runs
     int run0, run_count;        // grid form: the launch covers runs run0 .. run0+run_count-1 (0: all runs)
+    double mu1, mu2;            // viscous solvers: MU_1, MU_2 (hype.h:46-47)
 };
 
 // Tile geometry of the stage kernel: a tile is CELLS reconstruction columns
@@ -74,6 +77,10 @@ int stage_batch_blocks_per_sm(int sys, int order, int cells);   // resident bloc
 cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
                                const int2 *work, int *sched, int blocks, cudaStream_t s);
+// the VISCOUS build (Kapila, N = 1..3, primitive or conservative): 128-column tiles, grid form
+cudaError_t stage_visc_configure(int order, bool cons);
+int stage_visc_blocks_per_sm(int order, bool cons);
+cudaError_t launch_stage_visc(int order, bool cons, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 // conservative-variable path (RHSFunction): 128-column tiles, grid form
 cudaError_t stage_cons_configure(int sys, int order);
 int stage_cons_blocks_per_sm(int sys, int order);

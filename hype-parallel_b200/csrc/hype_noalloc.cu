@@ -45,6 +45,8 @@ __global__ void noalloc_reset_kernel(DevScalars *sc)
 {
     sc->dt = 0.0; sc->t = 0.0; sc->t_final = 0.0; sc->time_step = 0.0;
     sc->smax = 0ull;
+    sc->smax_v = 0ull;
+    sc->r1h_v = 0.0;
     sc->err = 0u;
     sc->err_cell = 0xffffffffu;
     sc->steps = 0; sc->max_steps = 0; sc->done = 0; sc->hold = 0; sc->idle = 0; sc->pad_ = 0;
@@ -74,7 +76,7 @@ int check(const hype_config *c)
     if (c->order < 0 || c->order > 3 || c->nx < 3 || c->ny < 3) return HYPE_ERR_INVALID;
     if (!(c->x_max > c->x_min) || !(c->y_max > c->y_min) || !(c->cfl > 0.0)) return HYPE_ERR_INVALID;
     if (c->precision != HYPE_PREC_FP64) return HYPE_ERR_INVALID;
-    if (c->flags & HYPE_FLAG_CONSERVATIVE) return HYPE_ERR_INVALID;
+    if (c->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS)) return HYPE_ERR_INVALID;
     const int bcs[4] = {c->bc_left, c->bc_right, c->bc_bottom, c->bc_top};
     for (int k = 0; k < 4; ++k)   // inlet needs a per-call host table; wall is never filled by the reference
         if (bcs[k] != HYPE_BC_PERIODIC && bcs[k] != HYPE_BC_REFLECTIVE && bcs[k] != HYPE_BC_TRANSMISSIVE) return HYPE_ERR_INVALID;

@@ -94,6 +94,11 @@ struct Quad {
     static constexpr double phi_vol(int q, int k) { return basis_c(xv(q), yv(q), k); }
     static constexpr double dphi_vol_x(int q, int k) { return basis_gx_c(xv(q), yv(q), k); }
     static constexpr double dphi_vol_y(int q, int k) { return basis_gy_c(xv(q), yv(q), k); }
+    // gradphiFace_x / _y (hype.c:255-285), d = 0 (x) or 1 (y)
+    static constexpr double dphi_face(int f, int q, int d, int k)
+    {
+        return d == 0 ? basis_gx_c(face_x(f, q), face_y(f, q), k) : basis_gy_c(face_x(f, q), face_y(f, q), k);
+    }
 };
 
 // Accumulate sum_k c[k]*phi(k) from 0.0 in ascending k, as the reference's
@@ -128,6 +133,7 @@ template <int SYS> struct System;
 template <> struct System<SYS_KAPILA> {
     static constexpr int NV = 6;
     static constexpr int RX0 = 2, RX1 = -1, RY0 = 3, RY1 = -1;   // rhs_function_prim.c:124-125, 253-254
+    static constexpr int RXV = 3, RYV = 2;                         // tangential, VISCOUS only: :126-127, :255-256
     // kapila_5eqn.c:14-35
     __device__ __forceinline__ static void cons2prim(const Eos &e, const double *Q, double *V)
     {
@@ -223,6 +229,61 @@ template <> struct System<SYS_KAPILA> {
         if (a_sq < PRS_FLOOR) return false;
         if (alpha_1 < 0.0 || alpha_1 > 1.0) return false;
         return true;
+    }
+
+    // ---- viscous fluxes (the VISCOUS build, hype.h:36) ----
+    // kapila_5eqn.c:377-411: from primitive values V and gradients g[c][dim]
+    // (only u, v: g[2], g[3] are read); returns the viscous eigenvalue
+    template <int DIR>
+    __device__ __forceinline__ static double visc_prim(const double *V, const double (*g)[2], double mu1, double mu2, double *F)
+    {
+        constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
+        const double r2_3 = 2. / 3., r4_3 = 4. / 3.;
+        double phi = V[5];
+        double mu = phi * mu1 + (1.0 - phi) * mu2;
+        double u = V[2];
+        double v = V[3];
+        double u_x = g[2][0], u_y = g[2][1], v_x = g[3][0], v_y = g[3][1];
+        double div_v = u_x + v_y;
+        double tau_xx = mu * (2.0 * u_x - r2_3 * div_v);
+        double tau_xy = mu * (u_y + v_x);
+        double tau_yy = mu * (2.0 * v_y - r2_3 * div_v);
+        F[0] = 0.0;
+        F[1] = 0.0;
+        F[2] = -nx * tau_xx - ny * tau_xy;
+        F[3] = -nx * tau_xy - ny * tau_yy;
+        F[4] = -nx * (u * tau_xx + v * tau_xy) - ny * (u * tau_xy + v * tau_yy);
+        F[5] = 0.0;
+        return r4_3 * mu / V[0];
+    }
+    // kapila_5eqn.c:119-158: from conserved values Q and their gradients (g[0..3] read)
+    template <int DIR>
+    __device__ __forceinline__ static double visc_cons(const double *Q, const double (*g)[2], double mu1, double mu2, double *F)
+    {
+        constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
+        const double r2_3 = 2. / 3., r4_3 = 4. / 3.;
+        double phi = Q[5];
+        double mu = phi * mu1 + (1.0 - phi) * mu2;
+        double irho = 1.0 / (Q[0] + Q[1]);
+        double u = irho * Q[2];
+        double v = irho * Q[3];
+        double rho_x = g[0][0] + g[1][0];
+        double rho_y = g[0][1] + g[1][1];
+        double u_x = irho * (g[2][0] - u * rho_x);
+        double u_y = irho * (g[2][1] - u * rho_y);
+        double v_x = irho * (g[3][0] - v * rho_x);
+        double v_y = irho * (g[3][1] - v * rho_y);
+        double div_v = u_x + v_y;
+        double tau_xx = mu * (2.0 * u_x - r2_3 * div_v);
+        double tau_xy = mu * (u_y + v_x);
+        double tau_yy = mu * (2.0 * v_y - r2_3 * div_v);
+        F[0] = 0.0;
+        F[1] = 0.0;
+        F[2] = -nx * tau_xx - ny * tau_xy;
+        F[3] = -nx * tau_xy - ny * tau_yy;
+        F[4] = -nx * (u * tau_xx + v * tau_xy) - ny * (u * tau_xy + v * tau_yy);
+        F[5] = 0.0;
+        return r4_3 * mu * irho;
     }
 
     // ---- conservative-variable path (RHSFunction, rhs_function.c) ----
@@ -723,6 +784,50 @@ template <> struct Recon<3> {
         coeffs[7] = wt_ratio * u_yyyR4;
         coeffs[8] = wt_ratio * u_xxyR4;
         coeffs[9] = wt_ratio * u_xyyR4;
+    }
+};
+
+// The unlimited central coefficients (u_coeffs) Reconstruct returns beside
+// the WENO ones (reconstruction.c:139-141, 172-174, 195-196, 217, 258-267);
+// the VISCOUS build takes face gradients from them.  N = 0: the reference
+// leaves them unset, so the viscous path starts at N = 1.
+template <int N> struct UCoef;
+template <> struct UCoef<1> {
+    __device__ __forceinline__ static void run(const Stencil &s, double *uc)
+    {
+        uc[0] = s.c;
+        uc[1] = 0.5 * (s.xp1 - s.xm1);
+        uc[2] = 0.5 * (s.yp1 - s.ym1);
+    }
+};
+template <> struct UCoef<2> {
+    __device__ __forceinline__ static void run(const Stencil &s, double *uc)
+    {
+        const double u_0 = s.c;
+        uc[0] = u_0;
+        uc[1] = 0.5 * (s.xp1 - s.xm1);
+        uc[3] = 0.5 * (s.xm1 - 2.0 * u_0 + s.xp1);
+        uc[2] = 0.5 * (s.yp1 - s.ym1);
+        uc[4] = 0.5 * (s.ym1 - 2.0 * u_0 + s.yp1);
+        uc[5] = 0.25 * (s.pp - s.pm - s.mp + s.mm);
+    }
+};
+template <> struct UCoef<3> {
+    __device__ __forceinline__ static void run(const Stencil &s, double *uc)
+    {
+        const double u_0 = s.c;
+        const double u_ip1 = s.xp1, u_jp1 = s.yp1, u_ip1jp1 = s.pp, u_im1 = s.xm1, u_jm1 = s.ym1, u_ip1jm1 = s.pm;
+        const double u_ip2 = s.xp2, u_jp2 = s.yp2, u_im1jp1 = s.mp, u_im2 = s.xm2, u_jm2 = s.ym2, u_im1jm1 = s.mm;
+        uc[0] = u_0;
+        uc[1] = R41_60 * (-u_im1 + u_ip1) + R11_120 * (u_im2 - u_ip2);
+        uc[2] = R41_60 * (-u_jm1 + u_jp1) + R11_120 * (u_jm2 - u_jp2);
+        uc[3] = -u_0 + 0.5 * (u_im1 + u_ip1);
+        uc[4] = -u_0 + 0.5 * (u_jm1 + u_jp1);
+        uc[5] = 0.25 * (u_im1jm1 - u_im1jp1 - u_ip1jm1 + u_ip1jp1);
+        uc[6] = R1_6 * (u_im1 - u_ip1) + R1_12 * (u_ip2 - u_im2);
+        uc[7] = R1_6 * (u_jm1 - u_jp1) + R1_12 * (u_jp2 - u_jm2);
+        uc[8] = 0.25 * (-u_im1jm1 + u_im1jp1 - u_ip1jm1 + u_ip1jp1) + 0.5 * (u_jm1 - u_jp1);
+        uc[9] = 0.5 * (u_im1 - u_ip1) + 0.25 * (u_ip1jp1 - u_im1jm1 - u_im1jp1 + u_ip1jm1);
     }
 };
 

@@ -84,6 +84,32 @@ __device__ __forceinline__ double face_val(const double *cf, int q)
     return v;
 }
 
+// Gradient component D (0: x, 1: y) of one variable at Gauss point q of face
+// F from its unlimited coefficients uc: sum_k uc[k] gradphiFace_D(F, q, k) from
+// 0.0 in ascending k (rhs_function_prim.c:362-369), before the 1/h factor.
+// Zero basis gradients are dropped as in face_val.
+template <int N, int F, int D>
+__device__ __forceinline__ double face_grad(const double *uc, int q)
+{
+    using QD = Quad<N>;
+    double v = 0.0;
+    static_for<QD::NDOF>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        constexpr double p0 = QD::dphi_face(F, 0, D, k);
+        constexpr double p1 = QD::dphi_face(F, QD::NFGP > 1 ? 1 : 0, D, k);
+        if constexpr (p0 == p1) {
+            if constexpr (p0 != 0.0) {
+                if constexpr (p0 == 1.0) v = v + uc[k];
+                else v = v + uc[k] * p0;
+            }
+        } else {
+            const double p = q ? p1 : p0;
+            v = v + uc[k] * p;
+        }
+    });
+    return v;
+}
+
 // one face Gauss point with n = e_x (DIR 0) or e_y (DIR 1): riemann.c:112-140
 // (RiemannSolverPrim, VL/VR primitive) or, for the conservative path,
 // riemann.c:52-105 (RiemannSolver, VL/VR conserved)
@@ -132,7 +158,12 @@ __device__ __forceinline__ double riemann_gp(const Eos &eos, const double *VL, c
 // CONS: the conservative-variable RHS (RHSFunction, rhs_function.c:12-625):
 // no conversion of the staged rows, PDECheckPAD / PDEFlux / PDENCP on
 // conserved values, and a PAD fallback that keeps only the cell mean.
-template <int SYS, int N, int CELLS_, bool CONS>
+// VISC: the reference's VISCOUS build (Kapila, N >= 1): walls also negate the
+// tangential velocity, every face Gauss point adds the mean of the two sides'
+// viscous fluxes (riemann.c:146-186) with gradients taken from the unlimited
+// coefficients (rhs_function_prim.c:356-374), and the viscous eigenvalue
+// maximum goes to DevScalars.smax_v for the dt (rhs_function_prim.c:617).
+template <int SYS, int N, int CELLS_, bool CONS, bool VISC = false>
 __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorMap *tmap, int strip, int run,
                                            unsigned char *smem_raw, double *red_s)
 {
@@ -151,6 +182,11 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     double *coef_s = rows_s + (size_t)SLOTS * K::SLOT_STRIDE;   // [k-1][c][cell]; later [F|D][c][cell]
     double *yt_s = coef_s + K::COEF_ELEMS;                      // [q][c][cell]
     double *carry_s = yt_s + K::YT_ELEMS;                       // [ncp|t1|gb|eb][c][cell]
+    // VISC: gradients of the variables the viscous flux reads (primitive u, v;
+    // conserved a1r1, a2r2, ru, rv) at the top face, kept for the row above:
+    // [q][g][d][cell], right behind the carries
+    constexpr int NG = CONS ? 4 : 2, G0 = CONS ? 0 : 2;
+    double *ygt_s = carry_s + K::CARRY_ELEMS;
 
     const int t = threadIdx.x;
     const int m = t >> 1;            // cell of this thread's pair
@@ -192,7 +228,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     auto cidx = [&](int k1, int c, int cell) { return (k1 * NV + c) * CELLS + cell; };         // coef_s index, k1 = k-1
     auto carry = [&](int which, int c) -> double & { return carry_s[(which * NV + c) * CELLS + m]; };
 
-    double smax_loc = 0.0;
+    double smax_loc = 0.0, smaxv_loc = 0.0;
     bool bad = false;
     unsigned bad_cell = 0xffffffffu;
 
@@ -265,11 +301,13 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     } else if (side_bc == BC_REFLECTIVE) {
                         if (S::RX0 >= 0) V[S::RX0] = -V[S::RX0];
                         if (S::RX1 >= 0) V[S::RX1] = -V[S::RX1];
+                        if constexpr (VISC) V[S::RXV] = -V[S::RXV];
                     }
                 }
                 if (yrefl) {
                     if (S::RY0 >= 0) V[S::RY0] = -V[S::RY0];
                     if (S::RY1 >= 0) V[S::RY1] = -V[S::RY1];
+                    if constexpr (VISC) V[S::RYV] = -V[S::RYV];
                 }
 #pragma unroll
                 for (int c = 0; c < NV; ++c) rp[c * BW + cc] = V[c];
@@ -303,6 +341,19 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
             cf[0] = w_0[c * BW + cell + 3];
 #pragma unroll
             for (int k = 1; k < NDOF; ++k) cf[k] = coef_s[cidx(k - 1, c, cell)];
+        };
+        // VISC: unlimited coefficients of variable c of the cell `cell` of row r, from the ring rows
+        auto load_uc = [&](int c, int cell, double *uc) {
+            if constexpr (VISC) {
+                const int col = cell + 3;
+                Stencil st;
+                const double *a0 = w_0 + c * BW + col;
+                st.c = a0[0];
+                st.xm2 = a0[-2]; st.xm1 = a0[-1]; st.xp1 = a0[1]; st.xp2 = a0[2];
+                st.ym2 = w_m2[c * BW + col]; st.ym1 = w_m1[c * BW + col]; st.yp1 = w_p1[c * BW + col]; st.yp2 = w_p2[c * BW + col];
+                st.pp = w_p1[c * BW + col + 1]; st.pm = w_m1[c * BW + col + 1]; st.mp = w_p1[c * BW + col - 1]; st.mm = w_m1[c * BW + col - 1];
+                UCoef<N>::run(st, uc);
+            }
         };
         // admissibility at the nodes (rhs_function_prim.c:382-404), nodes split between the pair
         bool ok = true;
@@ -365,7 +416,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
         {
             double G[NV], E[NV];
             const bool doit = owned && in_rows;
-            double Fq[NV], Dq[NV];
+            double Fq[NV], Dq[NV], Vq[NV];
             if (doit) {
                 double VL[NV], VR[NV];
 #pragma unroll
@@ -379,21 +430,54 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 smax_loc = fmax(smax_loc, s);
 #pragma unroll
                 for (int c = 0; c < NV; ++c) { Fq[c] = QD::wf(0) * Fq[c]; Dq[c] = QD::wf(0) * Dq[c]; }
+                if constexpr (VISC) {
+                    double gL[NV][2], gR[NV][2];
+#pragma unroll
+                    for (int g = 0; g < NG; ++g) {
+                        const int c = G0 + g;
+                        double uc[NDOF];
+                        load_uc(c, m, uc);
+                        gR[c][0] = r1_h * face_grad<N, 2, 0>(uc, q);
+                        gR[c][1] = r1_h * face_grad<N, 2, 1>(uc, q);
+                        gL[c][0] = ygt_s[((q * NG + g) * 2 + 0) * CELLS + m];
+                        gL[c][1] = ygt_s[((q * NG + g) * 2 + 1) * CELLS + m];
+                    }
+                    double FvL[NV], FvR[NV];
+                    double svl, svr;
+                    if constexpr (CONS) {
+                        svl = S::template visc_cons<1>(VL, gL, p.mu1, p.mu2, FvL);
+                        svr = S::template visc_cons<1>(VR, gR, p.mu1, p.mu2, FvR);
+                    } else {
+                        svl = S::template visc_prim<1>(VL, gL, p.mu1, p.mu2, FvL);
+                        svr = S::template visc_prim<1>(VR, gR, p.mu1, p.mu2, FvR);
+                    }
+                    smaxv_loc = fmax(smaxv_loc, (svl < svr) ? svr : svl);
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) Vq[c] = QD::wf(0) * (0.5 * (FvR[c] + FvL[c]));
+                }
             } else {
 #pragma unroll
-                for (int c = 0; c < NV; ++c) { Fq[c] = 0.0; Dq[c] = 0.0; }
+                for (int c = 0; c < NV; ++c) { Fq[c] = 0.0; Dq[c] = 0.0; Vq[c] = 0.0; }
             }
-            // Flux = 0.0; Flux += w F(q0); Flux += w F(q1)   (rhs_function_prim.c:548-577)
+            // Flux = 0.0; Flux += w F(q0); Flux += w F(q1)   (rhs_function_prim.c:548-577),
+            // VISC: Flux += w Fv(q) after each Gauss point's convective part
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
                 if constexpr (NFGP > 1) {
                     const double fo = __shfl_xor_sync(FULL, Fq[c], 1), d_o = __shfl_xor_sync(FULL, Dq[c], 1);
                     const double f0 = h ? fo : Fq[c], f1 = h ? Fq[c] : fo;
                     const double d0 = h ? d_o : Dq[c], d1 = h ? Dq[c] : d_o;
-                    G[c] = (0.0 + f0) + f1;
+                    if constexpr (VISC) {
+                        const double vo = __shfl_xor_sync(FULL, Vq[c], 1);
+                        const double v0 = h ? vo : Vq[c], v1 = h ? Vq[c] : vo;
+                        G[c] = (((0.0 + f0) + v0) + f1) + v1;
+                    } else {
+                        G[c] = (0.0 + f0) + f1;
+                    }
                     E[c] = (0.0 + d0) + d1;
                 } else {
-                    G[c] = 0.0 + Fq[c];
+                    if constexpr (VISC) G[c] = (0.0 + Fq[c]) + Vq[c];
+                    else G[c] = 0.0 + Fq[c];
                     E[c] = 0.0 + Dq[c];
                 }
             }
@@ -454,6 +538,15 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 double cf[NDOF];
                 load_cf(c, m, cf);
                 yt_s[(q * NV + c) * CELLS + m] = face_val<N, 3>(cf, q);
+            }
+            if constexpr (VISC) {
+#pragma unroll
+                for (int g = 0; g < NG; ++g) {
+                    double uc[NDOF];
+                    load_uc(G0 + g, m, uc);
+                    ygt_s[((q * NG + g) * 2 + 0) * CELLS + m] = r1_h * face_grad<N, 3, 0>(uc, q);
+                    ygt_s[((q * NG + g) * 2 + 1) * CELLS + m] = r1_h * face_grad<N, 3, 1>(uc, q);
+                }
             }
         }
 
@@ -528,7 +621,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
         double Fx[NV], Dx[NV];
         {
             const bool doit = xface && full_row;
-            double Fq[NV], Dq[NV];
+            double Fq[NV], Dq[NV], Vq[NV];
             if (doit) {
                 double VL[NV], VR[NV];
 #pragma unroll
@@ -543,10 +636,36 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 smax_loc = fmax(smax_loc, s);
 #pragma unroll
                 for (int c = 0; c < NV; ++c) { Fq[c] = QD::wf(0) * Fq[c]; Dq[c] = QD::wf(0) * Dq[c]; }
+                if constexpr (VISC) {
+                    double gL[NV][2], gR[NV][2];
+#pragma unroll
+                    for (int g = 0; g < NG; ++g) {
+                        const int c = G0 + g;
+                        double ul[NDOF], ur[NDOF];
+                        load_uc(c, m - 1, ul);
+                        load_uc(c, m, ur);
+                        gL[c][0] = r1_h * face_grad<N, 1, 0>(ul, q);
+                        gL[c][1] = r1_h * face_grad<N, 1, 1>(ul, q);
+                        gR[c][0] = r1_h * face_grad<N, 0, 0>(ur, q);
+                        gR[c][1] = r1_h * face_grad<N, 0, 1>(ur, q);
+                    }
+                    double FvL[NV], FvR[NV];
+                    double svl, svr;
+                    if constexpr (CONS) {
+                        svl = S::template visc_cons<0>(VL, gL, p.mu1, p.mu2, FvL);
+                        svr = S::template visc_cons<0>(VR, gR, p.mu1, p.mu2, FvR);
+                    } else {
+                        svl = S::template visc_prim<0>(VL, gL, p.mu1, p.mu2, FvL);
+                        svr = S::template visc_prim<0>(VR, gR, p.mu1, p.mu2, FvR);
+                    }
+                    smaxv_loc = fmax(smaxv_loc, (svl < svr) ? svr : svl);
+#pragma unroll
+                    for (int c = 0; c < NV; ++c) Vq[c] = QD::wf(0) * (0.5 * (FvR[c] + FvL[c]));
+                }
                 if (bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);
             } else {
 #pragma unroll
-                for (int c = 0; c < NV; ++c) { Fq[c] = 0.0; Dq[c] = 0.0; }
+                for (int c = 0; c < NV; ++c) { Fq[c] = 0.0; Dq[c] = 0.0; Vq[c] = 0.0; }
             }
 #pragma unroll
             for (int c = 0; c < NV; ++c) {
@@ -554,10 +673,17 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     const double fo = __shfl_xor_sync(FULL, Fq[c], 1), d_o = __shfl_xor_sync(FULL, Dq[c], 1);
                     const double f0 = h ? fo : Fq[c], f1 = h ? Fq[c] : fo;
                     const double d0 = h ? d_o : Dq[c], d1 = h ? Dq[c] : d_o;
-                    Fx[c] = (0.0 + f0) + f1;
+                    if constexpr (VISC) {
+                        const double vo = __shfl_xor_sync(FULL, Vq[c], 1);
+                        const double v0 = h ? vo : Vq[c], v1 = h ? Vq[c] : vo;
+                        Fx[c] = (((0.0 + f0) + v0) + f1) + v1;
+                    } else {
+                        Fx[c] = (0.0 + f0) + f1;
+                    }
                     Dx[c] = (0.0 + d0) + d1;
                 } else {
-                    Fx[c] = 0.0 + Fq[c];
+                    if constexpr (VISC) Fx[c] = (0.0 + Fq[c]) + Vq[c];
+                    else Fx[c] = 0.0 + Fq[c];
                     Dx[c] = 0.0 + Dq[c];
                 }
             }
@@ -597,6 +723,20 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
 #pragma unroll
             for (int w = 1; w < K::NT / 32; ++w) b = fmax(b, red_s[w]);
             if (b > 0.0) atomicMax(&p.sc->smax, (unsigned long long)__double_as_longlong(b));
+        }
+        if constexpr (VISC) {   // the same for the viscous eigenvalue
+            __syncthreads();
+            double mv = smaxv_loc;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) mv = fmax(mv, __shfl_xor_sync(FULL, mv, o));
+            if ((t & 31) == 0) red_s[t >> 5] = mv;
+            __syncthreads();
+            if (t == 0) {
+                double b = red_s[0];
+#pragma unroll
+                for (int w = 1; w < K::NT / 32; ++w) b = fmax(b, red_s[w]);
+                if (b > 0.0) atomicMax(&p.sc->smax_v, (unsigned long long)__double_as_longlong(b));
+            }
         }
     }
     for (int k = t; k < SLOTS; k += K::NT) mbar_inval(&bars[k]);

@@ -71,6 +71,10 @@ static void glue_config(const AppCtx *Ctx, int conservative, hype_config *c)
     c->pi1 = PI_1; c->pi2 = PI_2;
     c->precision = HYPE_PREC_FP64;
     c->flags = conservative ? HYPE_FLAG_CONSERVATIVE : 0u;
+#ifdef VISCOUS
+    c->flags |= HYPE_FLAG_VISCOUS;   /* the tree's VISCOUS build (hype.h:36) */
+    c->mu1 = MU_1; c->mu2 = MU_2;
+#endif
     c->device = dev ? atoi(dev) : 0;
 }
 

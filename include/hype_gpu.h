@@ -66,6 +66,11 @@ extern "C" {
                                      RHSFunction (rhs_function.c:12-625), which hype.c uses
                                      when Ctx.ReconsPrimitive is false (hype.c:341-352).
                                      FP64 solvers only (not mixed, batch or no-alloc).      */
+#define HYPE_FLAG_VISCOUS     4u  /* the reference's VISCOUS build (hype.h:36, off there by
+                                     default): viscous face fluxes with viscosities mu1/mu2
+                                     (rhs_function_prim.c:356-374, riemann.c:146-186,
+                                     kapila_5eqn.c:119-158, 377-411) and the viscous dt.
+                                     Kapila, N = 1..3, FP64 solvers only.                    */
 
 /*
  * Run-time form of the reference's compile-time and AppCtx parameters:
@@ -76,6 +81,7 @@ extern "C" {
  *   cfl                    AppCtx.CFL
  *   bc_*                   AppCtx.LeftBoundary ... (hype.c:46-49)
  *   gamma1..pi2            GAMMA_1, GAMMA_2, PI_1, PI_2 (hype.h:42-45)
+ *   mu1, mu2               MU_1, MU_2 (hype.h:46-47), with HYPE_FLAG_VISCOUS
  */
 typedef struct {
     int system;
@@ -88,6 +94,7 @@ typedef struct {
     int precision;
     unsigned flags;
     int device;           /* CUDA device ordinal */
+    double mu1, mu2;      /* MU_1, MU_2 (hype.h:46-47): phase viscosities, read with HYPE_FLAG_VISCOUS */
 } hype_config;
 
 typedef struct hype_solver hype_solver;

@@ -27,7 +27,8 @@ def to_pkg(cfg: O.Config) -> "hp.Config":
                      y_min=cfg.y_min, y_max=cfg.y_max, cfl=cfg.cfl, bc_left=cfg.bc_left, bc_right=cfg.bc_right,
                      bc_bottom=cfg.bc_bottom, bc_top=cfg.bc_top, gamma1=cfg.gamma1, gamma2=cfg.gamma2, pi1=cfg.pi1,
                      pi2=cfg.pi2, precision=hp.PREC_FP64,
-                     flags=(hp.FLAG_BN_FIX_P2 if cfg.bn_fixed_p2 else 0) | (hp.FLAG_CONSERVATIVE if cfg.conservative else 0))
+                     flags=(hp.FLAG_BN_FIX_P2 if cfg.bn_fixed_p2 else 0) | (hp.FLAG_CONSERVATIVE if cfg.conservative else 0)
+                     | (hp.FLAG_VISCOUS if cfg.viscous else 0), mu1=cfg.mu1, mu2=cfg.mu2)
 
 
 def kapila_rough(cfg: O.Config, seed: int) -> np.ndarray:
@@ -127,6 +128,17 @@ RHS_CASES = [
     _b("bn_cons_16x16", 16, 16, seed=30, conservative=1),
     _b("bn_cons_13x21_periodic_N1", 13, 21, order=1, bcs=(P, P, R, R), seed=31, conservative=1),
     _b("bn_cons_12x10_N3", 12, 10, order=3, bcs=(R, R, T, T), seed=32, conservative=1),
+    # the reference's VISCOUS build (Kapila, N >= 1)
+    _k("kapila_visc_24x20_walls", 24, 20, bcs=(R, R, R, R), seed=40, viscous=1, mu1=0.3, mu2=0.05),
+    _k("kapila_visc_37x23_rough", 37, 23, bcs=(R, T, R, R), kind="rough", seed=41, viscous=1, mu1=0.05, mu2=0.01),
+    _k("kapila_visc_19x17_N1", 19, 17, order=1, bcs=(T, T, P, P), kind="rough", seed=42, viscous=1),
+    _k("kapila_visc_15x13_N3", 15, 13, order=3, bcs=(R, T, P, P), seed=43, viscous=1, mu1=2.0, mu2=0.5),
+    _k("kapila_visc_18x14_inlet", 18, 14, bcs=(I, T, R, R), kind="rough", seed=44, x_min=0.0, x_max=2.0, y_min=-1.0,
+       y_max=0.5556, viscous=1, mu1=0.1),
+    _k("kapila_visc_251x7_three_strips", 251, 7, bcs=(R, R, T, T), seed=45, viscous=1, mu1=0.2, mu2=0.02),
+    _k("kapila_visc_cons_24x20_walls", 24, 20, bcs=(R, R, R, R), seed=46, conservative=1, viscous=1, mu1=0.3, mu2=0.05),
+    _k("kapila_visc_cons_19x17_N1", 19, 17, order=1, kind="rough", seed=47, conservative=1, viscous=1),
+    _k("kapila_visc_cons_15x13_N3", 15, 13, order=3, bcs=(R, T, P, P), seed=48, conservative=1, viscous=1, mu1=2.0, mu2=0.5),
 ]
 
 # Multi-step solve cases (hype.c time loop)
@@ -140,6 +152,8 @@ SOLVE_CASES = [
     (_k("kapila_cons_32x32_solve", 32, 32, seed=33, conservative=1), 0.0, 1.0, 8),
     (_e("euler_cons_32x24_solve", 32, 24, bcs=(T, T, R, R), seed=34, conservative=1), 0.0, 0.05, 1000),
     (_b("bn_cons_20x20_solve", 20, 20, bcs=(R, R, R, R), seed=35, conservative=1), 0.0, 1.0, 4),
+    (_k("kapila_visc_32x32_solve", 32, 32, bcs=(T, T, R, R), seed=49, viscous=1, mu1=0.5, mu2=0.1), 0.0, 1.0, 6),
+    (_k("kapila_visc_cons_24x24_solve", 24, 24, bcs=(P, P, P, P), seed=50, conservative=1, viscous=1, mu1=0.5), 0.0, 1.0, 4),
 ]
 
 

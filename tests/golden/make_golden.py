@@ -33,7 +33,8 @@ def sha(a: np.ndarray) -> str:
 def main():
     if not O.reference_available():
         raise SystemExit("oracle/_ref is not built: run `make -C oracle ref` where the reference sources exist")
-    refs = {s: O.Reference(s) for s in (O.EULER, O.KAPILA, O.BN)}
+    refs = {(s, 0): O.Reference(s) for s in (O.EULER, O.KAPILA, O.BN)}
+    refs[(O.KAPILA, 1)] = O.Reference(O.KAPILA, viscous=True)
     out = {"generator": "tests/golden/make_golden.py", "rhs": {}, "solve": {}}
     arrays = {}
     keep = {"kapila_16x16_bubble", "euler_16x16", "bn_16x16"}
@@ -50,7 +51,7 @@ def main():
             R, dt, st = O.Oracle().rhs(cfg, U)
             src = "oracle(conservative N=0: reference writes past nDOF)"
         else:
-            ref = refs[cfg.system]
+            ref = refs[(cfg.system, cfg.viscous)]
             ref.setup(cfg)
             R, dt, st = ref.rhs(U)
             src = "reference"
@@ -62,7 +63,7 @@ def main():
         print(f"{name:40s} status={st} dt={dt:.6e}")
     for (name, cfg, kind, seed), t0, tf, nmax in cases.SOLVE_CASES:
         U = cases.state(cfg, kind, seed)
-        ref = refs[cfg.system]
+        ref = refs[(cfg.system, cfg.viscous)]
         ref.setup(cfg)
         Ue, steps, te, dtn, st = ref.solve(U, t0, tf, nmax)
         out["solve"][name] = {"config": cases.config_to_dict(cfg), "kind": kind, "seed": seed, "t0": t0, "t_final": tf,

@@ -68,7 +68,10 @@ def test_config_defaults_follow_reference_main(hp):
     (dict(precision=1, system=2), "Kapila"),
     (dict(precision=1, order=1), "N = 2"),
     (dict(precision=1, order=2, flags=2), "FP64 only"),
-    (dict(flags=4), "unknown flags"),
+    (dict(flags=8), "unknown flags"),
+    (dict(flags=4, system=2), "viscous"),
+    (dict(flags=4, order=0), "viscous"),
+    (dict(flags=4, precision=1), "viscous"),
 ])
 def test_invalid_configs_rejected_before_device(hp, change, needle):
     cfg = hp.Config(nx=16, ny=16)

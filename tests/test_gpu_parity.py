@@ -90,6 +90,31 @@ def test_rhs_fresh_seeds_conservative_vs_oracle(seed, hp, orc):
             assert R.tobytes() == Ro.tobytes(), describe_diff(R, Ro, cfg.nvar)
 
 
+@pytest.mark.parametrize("seed", range(3))
+def test_rhs_fresh_seeds_viscous_vs_oracle(seed, hp, orc):
+    """The VISCOUS build (Kapila, N = 1..3, primitive and conservative) on random
+    sizes, boundaries and viscosities."""
+    rng = np.random.default_rng(3000 + seed)
+    for cons in (0, 1):
+        for kind in ("rough", "bubble"):
+            nx, ny = int(rng.integers(3, 300)), int(rng.integers(3, 40))
+            order = int(rng.integers(1, 4))
+            bcs = [int(b) for b in rng.choice([O.TRANSMISSIVE, O.REFLECTIVE], 4)]
+            if rng.uniform() < 0.3:
+                bcs[2] = bcs[3] = O.PERIODIC
+            cfg = O.Config(system=O.KAPILA, order=order, nx=nx, ny=ny, bc_left=bcs[0], bc_right=bcs[1], bc_bottom=bcs[2],
+                           bc_top=bcs[3], conservative=cons, viscous=1, mu1=float(rng.uniform(0, 1)),
+                           mu2=float(rng.uniform(0, 0.1)), **cases.KAPILA_EOS)
+            U = cases.state(cfg, kind, seed)
+            Ro, dto, sto = orc.rhs(cfg, U)
+            with hp.Solver(cases.to_pkg(cfg)) as s:
+                R, dt, st = s.rhs_function_prim(0.0, U)
+            assert (st == hp.OK) == (sto == O.OK), (cons, nx, ny, order, bcs)
+            if sto == O.OK:
+                assert dt == dto
+                assert R.tobytes() == Ro.tobytes(), describe_diff(R, Ro, cfg.nvar)
+
+
 @pytest.mark.parametrize("seed", range(4))
 def test_rhs_fresh_seeds_vs_oracle(seed, hp, orc):
     rng = np.random.default_rng(1000 + seed)
