@@ -332,6 +332,26 @@ def bn_leg(hp, args, local_rank):
     return out
 
 
+def group_leg(hp, args, local_rank, U0, U_ref):
+    """The FP64 workload as y-slabs on this GPU (hype_group): the cost of the
+    decomposition (halo rows stored by the stage kernels into the neighbours,
+    per-stage events, one reduction per step) against the single solver, and the
+    final state compared with the single solver's after the same steps."""
+    cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=NX, ny=NY, cfl=0.4, device=local_rank)
+    with hp.Group(cfg, args.group_slabs) as grp:
+        grp.set_state(U0)
+        grp.begin(0.0, 1e30, 1 << 30)
+        grp.advance(max(3, args.warmup))
+        grp.wait()
+        grp.advance(args.steps)
+        _, _, _, st = grp.wait()
+        ms = grp.last_elapsed_ms()
+        same = None if U_ref is None else bool(grp.get_state().tobytes() == U_ref.tobytes())
+    return {"value": NX * NY * args.steps / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / args.steps, "status": st,
+            "slabs": args.group_slabs, "devices": [local_rank] * args.group_slabs,
+            "bitwise_equal_to_single_solver": same}
+
+
 def serve_leg(hp, args, local_rank, capacity):
     """Serving: a Poisson stream of solve requests through the C request loop
     (hype_serve_run) -- 70/20/10 Kapila / Baer-Nunziato / Euler, square grids
@@ -425,7 +445,7 @@ def run_gpu(args, rank, world, local_rank):
     ms = max_over_ranks(solver.last_elapsed_ms(), world)
     cells = NX * NY
     value = replica_throughput(world, cells, args.steps, ms)
-    U_fp64 = solver.get_state() if not args.no_mixed else None
+    U_fp64 = solver.get_state()   # the mixed and y-slab legs compare with it
 
     # dominant kernel: the stage kernel, timed alone (CUDA events, same stream)
     ms_stage = solver.time_stage(20)
@@ -490,6 +510,7 @@ def run_gpu(args, rank, world, local_rank):
                  "rel_error_vs_fp64_after_run": {"fields_L1_Linf": errs, "steps": args.steps + max(3, args.warmup)},
                  "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt"}
 
+    group = None if args.group_slabs <= 1 else group_leg(hp, args, local_rank, U0, U_fp64)
     bn = None if args.no_bn else bn_leg(hp, args, local_rank)
     batched = None if args.no_batch else batch_leg(hp, args, local_rank)
     capacity = batched["batched_mixed"]["value"] if batched else 5e8
@@ -514,7 +535,7 @@ def run_gpu(args, rank, world, local_rank):
             "gpu_launches": args.steps * 6,
             "clocks": clk.summary(),
             "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2},
-            "forms": {"mixed": mixed, "bn1024": bn, "batched": batched, "serving": serving}}
+            "forms": {"mixed": mixed, "bn1024": bn, "batched": batched, "serving": serving, "y_slabs": group}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -531,6 +552,7 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-grids leg")
     ap.add_argument("--no-bn", action="store_true", help="skip the Baer-Nunziato 1024^2 leg")
+    ap.add_argument("--group-slabs", type=int, default=2, help="y-slabs of the decomposed leg on this GPU (<= 1: skip)")
     ap.add_argument("--batch-steps", type=int, default=300, help="steps of the batched-grids leg")
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip)")
     ap.add_argument("--serve-kapila", default="mixed", choices=["mixed", "fp64"], help="precision of Kapila requests")

@@ -164,6 +164,18 @@ def lib() -> ctypes.CDLL:
         L.hype_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.hype_config_default.argtypes = [ctypes.POINTER(_Cfg)]
         L.hype_get_primitive.argtypes = [vp, _DP]
+        L.hype_group_create.argtypes = [ctypes.POINTER(_Cfg), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(vp)]
+        L.hype_group_destroy.argtypes = [vp]
+        L.hype_group_last_error.argtypes = [vp]
+        L.hype_group_last_error.restype = ctypes.c_char_p
+        L.hype_group_slab.argtypes = [vp, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 3
+        L.hype_group_set_state.argtypes = [vp, _DP]
+        L.hype_group_get_state.argtypes = [vp, _DP]
+        L.hype_group_begin.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        L.hype_group_advance.argtypes = [vp, ctypes.c_int]
+        L.hype_group_wait.argtypes = [vp, ctypes.POINTER(ctypes.c_int), _DP, _DP]
+        L.hype_group_solve.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_int), _DP, _DP]
+        L.hype_group_last_elapsed_ms.argtypes = [vp, _DP]
         L.hype_solver_config.argtypes = [vp, ctypes.POINTER(_Cfg)]
         for name in ("hype_write_restart", "hype_read_restart", "hype_write_vts"):
             getattr(L, name).argtypes = [vp, ctypes.c_char_p]
@@ -397,6 +409,102 @@ class Solver:
     def last_elapsed_ms(self) -> float:
         ms = ctypes.c_double(0.0)
         self._check(lib().hype_last_elapsed_ms(self._h, ctypes.byref(ms)))
+        return ms.value
+
+
+class Group:
+    """One grid split into y-slabs (include/hype_group.h): HyPE-2D's DMDA
+    decomposition over ranks, here over the GPUs of one process (`devices`, one
+    per slab; default: all slabs on cfg.device).  Same calls as Solver's time
+    loop; the results equal a Solver's bit for bit."""
+
+    def __init__(self, cfg: Config, nslabs: int, devices=None):
+        self.cfg = cfg
+        self.nslabs = nslabs
+        self._h = ctypes.c_void_p()
+        dev = None
+        if devices is not None:
+            if len(devices) != nslabs:
+                raise ValueError("one device per slab")
+            dev = (ctypes.c_int * nslabs)(*devices)
+        st = lib().hype_group_create(ctypes.byref(cfg.c_struct()), nslabs, dev, ctypes.byref(self._h))
+        if st != OK:
+            msg = lib().hype_group_last_error(self._h).decode() if self._h else lib().hype_status_string(st).decode()
+            lib().hype_group_destroy(self._h)
+            self._h = ctypes.c_void_p()
+            raise HypeError(st, msg)
+
+    def close(self):
+        if self._h:
+            lib().hype_group_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st: int) -> None:
+        if st != OK:
+            raise HypeError(st, lib().hype_group_last_error(self._h).decode())
+
+    @property
+    def n(self) -> int:
+        return self.cfg.nx * self.cfg.ny * self.cfg.nvar
+
+    def last_error(self) -> str:
+        return lib().hype_group_last_error(self._h).decode()
+
+    def slab(self, k: int):
+        """(first global row, rows, device) of slab k."""
+        r0, n, d = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        self._check(lib().hype_group_slab(self._h, k, ctypes.byref(r0), ctypes.byref(n), ctypes.byref(d)))
+        return r0.value, n.value, d.value
+
+    def set_state(self, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        if U.size != self.n:
+            raise ValueError("U has the wrong size")
+        self._check(lib().hype_group_set_state(self._h, _ptr(U)))
+
+    def get_state(self) -> np.ndarray:
+        U = np.empty(self.n, dtype=np.float64)
+        self._check(lib().hype_group_get_state(self._h, _ptr(U)))
+        return U
+
+    def solve(self, t0: float, t_final: float, max_steps: int, check: bool = True):
+        """Returns (steps, t_end, dt_next, status)."""
+        steps = ctypes.c_int(0)
+        t = ctypes.c_double(0.0)
+        dt = ctypes.c_double(0.0)
+        st = lib().hype_group_solve(self._h, t0, t_final, max_steps, ctypes.byref(steps), ctypes.byref(t), ctypes.byref(dt))
+        if check and st not in (OK, ERR_INADMISSIBLE):
+            self._check(st)
+        return steps.value, t.value, dt.value, st
+
+    def begin(self, t0: float, t_final: float, max_steps: int) -> None:
+        self._check(lib().hype_group_begin(self._h, t0, t_final, max_steps))
+
+    def advance(self, nsteps: int) -> None:
+        self._check(lib().hype_group_advance(self._h, nsteps))
+
+    def wait(self):
+        steps = ctypes.c_int(0)
+        t = ctypes.c_double(0.0)
+        dt = ctypes.c_double(0.0)
+        st = lib().hype_group_wait(self._h, ctypes.byref(steps), ctypes.byref(t), ctypes.byref(dt))
+        return steps.value, t.value, dt.value, st
+
+    def last_elapsed_ms(self) -> float:
+        ms = ctypes.c_double(0.0)
+        self._check(lib().hype_group_last_elapsed_ms(self._h, ctypes.byref(ms)))
         return ms.value
 
 

@@ -12,46 +12,26 @@
 #include <vector>
 #include "../../include/hype_gpu.h"
 #include "hype_internal.h"
+#include "hype_solver.h"
 
 using namespace hype;
 
-struct hype_solver {
-    hype_config cfg;
-    int nv = 0;
-    int pitch = 0;
-    long long plane = 0;
-    double h = 0.0, r1_h = 0.0, cfl_h = 0.0;
-    double *dU = nullptr, *dS0 = nullptr, *dS1 = nullptr, *dS2 = nullptr;
-    double *dAosIn = nullptr, *dAosOut = nullptr, *dInlet = nullptr;
-    double *dRed = nullptr;           // reduction scratch
-    DevScalars *dSc = nullptr;
-    DevScalars *hSc = nullptr;        // pinned mirror
-    CUtensorMap tmU, tmS0, tmS1;
-    cudaStream_t stream = nullptr;
-    cudaStream_t cin = nullptr, cout = nullptr;   // host<->device copy streams of the banded calls
-    cudaEvent_t ev_in[8] = {}, ev_done[8] = {};   // per row band: uploaded, computed
-    cudaEvent_t ev_fence = nullptr;               // the compute stream's work so far
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    cudaGraphExec_t step_exec = nullptr;
-    int cells = STAGE_CELLS;          // tile width of the stage kernel
-    int waves = 1;                    // row runs per strip = waves x (SM slots / strips)
-    int sms = 0;
-    int strips = 1, runs = 1;         // tile decomposition of the grid
-    int bps = 0;                      // stage blocks per SM
-    // mixed precision (Kapila N=2): state k = 0 (U), 1 (S0), 2 (S1) as FP32 + FP64 planes
-    bool mixed = false;
-    float *mf[3] = {nullptr, nullptr, nullptr};
-    double *md[3] = {nullptr, nullptr, nullptr};
-    MixedMaps mm[3];
-    bool began = false;
-    double last_ms = 0.0;
-    char err[512] = {0};
-};
 
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
 static int fail(hype_solver *s, int code, const char *fmt, ...)
+{
+    if (s) {
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(s->err, sizeof(s->err), fmt, ap);
+        va_end(ap);
+    }
+    return code;
+}
+
+int hype::solver_fail(hype_solver *s, int code, const char *fmt, ...)
 {
     if (s) {
         va_list ap;
@@ -101,10 +81,12 @@ CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, 
 }
 }  // namespace hype
 
-// 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (cells + 6, 1, nvar).
+// 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (cells + 6, 1, nvar);
+// a slab's map also covers its halo rows and starts row_off rows below row 0.
 static int make_tmap(hype_solver *s, CUtensorMap *m, double *base)
 {
-    CUresult r = encode_planes_map(m, base, false, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, stage_box_width(s->cells));
+    CUresult r = encode_planes_map(m, base - (long long)s->row_off * s->pitch, false, s->cfg.nx, s->cfg.ny + 2 * s->row_off, s->nv,
+                                   s->pitch, s->plane, stage_box_width(s->cells));
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return HYPE_OK;
 }
@@ -171,6 +153,7 @@ static StageParams base_params(const hype_solver *s)
     p.sc = s->dSc;
     p.inlet = s->dInlet;
     p.kb = 1.0;
+    p.row_off = s->row_off;
     return p;
 }
 
@@ -243,7 +226,8 @@ static const CUtensorMap &tmap_for(const hype_solver *s, const double *buf)
 }
 
 static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode, double ka, double kb, double kc,
-                         const double *xn, double *out2, int reduce, int out_aos = 0, int run0 = 0, int run_count = 0)
+                         const double *xn, double *out2, int reduce, int out_aos = 0, int run0 = 0, int run_count = 0,
+                         int push_role = B_NONE)
 {
     StageParams p = base_params(s);
     p.in = in; p.out = out; p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc; p.xn = xn; p.out2 = out2;
@@ -251,6 +235,10 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
     p.out_aos = out_aos;
     p.run0 = run0;
     p.run_count = run_count;
+    if (push_role >= 0 && mode != OUT_RHS) {   // a slab's state output: edge rows to the neighbours' halos
+        p.push_lo = s->nb_lo[push_role]; p.push_plane_lo = s->nb_plane_lo; p.push_shift_lo = s->nb_shift_lo;
+        p.push_hi = s->nb_hi[push_role]; p.push_plane_hi = s->nb_plane_hi; p.push_shift_hi = s->nb_shift_hi;
+    }
     if (s->cfg.flags & HYPE_FLAG_VISCOUS)
         return launch_stage_visc(s->cfg.order, (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) != 0, tmap_for(s, in), p, s->stream);
     if (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) return launch_stage_cons(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->stream);
@@ -289,6 +277,18 @@ static double *buf_of(hype_solver *s, int b)
     }
 }
 
+double *hype::solver_buf(hype_solver *s, int role) { return buf_of(s, role); }
+double *hype::solver_alloc_base(const hype_solver *s, double *buf) { return buf ? buf - (long long)s->row_off * s->pitch : nullptr; }
+
+cudaError_t hype::solver_stage(hype_solver *s, const PlanStage &q)
+{
+    return stage(s, buf_of(s, q.in), buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x), buf_of(s, q.out2), q.reduce, 0, 0, 0,
+                 q.out);
+}
+
+// hype.c:343's seeding RHS of u: S1 takes the (unused) RHS planes
+cudaError_t hype::solver_seed_rhs(hype_solver *s) { return stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1); }
+
 // One SSP-RK step on the device state: the stage list of ssp_plan between the
 // step-control kernels.  The mixed state has the same buffer roles (U, S0, S1).
 static cudaError_t enqueue_step(hype_solver *s)
@@ -305,7 +305,8 @@ static cudaError_t enqueue_step(hype_solver *s)
         if (e != cudaSuccess) return e;
     }
     if (copy_back &&
-        (e = cudaMemcpyAsync(s->dU, s->dS0, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream)) != cudaSuccess)
+        (e = cudaMemcpyAsync(solver_alloc_base(s, s->dU), solver_alloc_base(s, s->dS0), sizeof(double) * (size_t)s->plane * s->nv,
+                             cudaMemcpyDeviceToDevice, s->stream)) != cudaSuccess)
         return e;
     return launch_end_step(s->dSc, s->cfl_h, s->stream);
 }
@@ -509,7 +510,8 @@ int hype_destroy(hype_solver *s)
     cudaSetDevice(dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
     if (s->step_exec) cudaGraphExecDestroy(s->step_exec);
-    double *bufs[] = {s->dU, s->dS0, s->dS1, s->dS2, s->dAosIn, s->dAosOut, s->dInlet, s->dRed};
+    double *bufs[] = {solver_alloc_base(s, s->dU), solver_alloc_base(s, s->dS0), solver_alloc_base(s, s->dS1),
+                      solver_alloc_base(s, s->dS2), s->dAosIn, s->dAosOut, s->dInlet, s->dRed};
     for (double *b : bufs) if (b) cudaFree(b);
     for (int k = 0; k < 3; ++k) { if (s->mf[k]) cudaFree(s->mf[k]); if (s->md[k]) cudaFree(s->md[k]); }
     if (s->dSc) cudaFree(s->dSc);
@@ -528,16 +530,16 @@ int hype_destroy(hype_solver *s)
     return HYPE_OK;
 }
 
-int hype_create(const hype_config *cfg, hype_solver **out)
+}  // extern "C"
+
+// Device buffers, streams and descriptors of a checked configuration.  row_off > 0
+// makes a y-slab: every plane carries row_off halo rows below and above the slab's
+// rows; `inlet` replaces the inlet table computed from cfg (a slab's rows of the
+// whole grid's table).
+static int create_common(hype_solver *s, const hype_config *cfg, int row_off, const std::vector<double> *inlet)
 {
-    if (!out) return HYPE_ERR_INVALID;
-    *out = nullptr;
-    hype_solver *s = new (std::nothrow) hype_solver();
-    if (!s) return HYPE_ERR_NOMEM;
-    int rc = check_config(cfg, s);
-    if (rc) { *out = s; return rc; }   // caller reads hype_last_error, then destroys
     s->cfg = *cfg;
-    *out = s;
+    s->row_off = row_off;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
         return fail(s, HYPE_ERR_NO_DEVICE, "CUDA device %d not available", cfg->device);
@@ -549,12 +551,12 @@ int hype_create(const hype_config *cfg, hype_solver **out)
 
     s->nv = hype_nvar(cfg->system);
     s->pitch = s->mixed ? ((cfg->nx + 31) & ~31) : ((cfg->nx + 15) & ~15);   // 128-byte rows
-    s->plane = (long long)s->pitch * cfg->ny;
+    s->plane = (long long)s->pitch * (cfg->ny + 2 * row_off);
     s->h = (cfg->x_max - cfg->x_min) / (double)cfg->nx;   // hype.c:57
     s->r1_h = 1. / s->h;                                  // rhs_function_prim.c:26
     s->cfl_h = cfg->cfl * s->h;                           // rhs_function_prim.c:620
     const size_t state_bytes = sizeof(double) * (size_t)s->plane * s->nv;
-    const size_t aos_bytes = sizeof(double) * (size_t)cfg->nx * cfg->ny * s->nv;
+    const size_t aos_bytes = sizeof(double) * (size_t)cfg->nx * (cfg->ny + 2 * row_off) * s->nv;
     CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(s, cudaEventCreate(&s->ev0));
     CUDA_TRY(s, cudaEventCreate(&s->ev1));
@@ -565,14 +567,13 @@ int hype_create(const hype_config *cfg, hype_solver **out)
         CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming));
     }
     CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_fence, cudaEventDisableTiming));
-    double **bufs[] = {&s->dU, &s->dS0, &s->dS1};
+    double **bufs[] = {&s->dU, &s->dS0, &s->dS1, &s->dS2};
+    const long long off = (long long)row_off * s->pitch;   // the buffers point at row 0
     for (double **b : bufs) {
+        if (b == &s->dS2 && cfg->order != 3) continue;
         if (cudaMalloc(b, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", state_bytes);
         CUDA_TRY(s, cudaMemset(*b, 0, state_bytes));
-    }
-    if (cfg->order == 3) {
-        if (cudaMalloc(&s->dS2, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc failed");
-        CUDA_TRY(s, cudaMemset(s->dS2, 0, state_bytes));
+        *b += off;
     }
     if (s->mixed) {
         for (int k = 0; k < 3; ++k) {
@@ -591,7 +592,8 @@ int hype_create(const hype_config *cfg, hype_solver **out)
     CUDA_TRY(s, cudaMallocHost(&s->hSc, sizeof(DevScalars)));
     if (cfg->bc_left == HYPE_BC_INLET) {
         std::vector<double> tab;
-        inlet_table(*cfg, s->h, tab);
+        if (inlet) tab = *inlet;
+        else inlet_table(*cfg, s->h, tab);
         if (cfg->flags & HYPE_FLAG_CONSERVATIVE) inlet_to_conserved(*cfg, tab);
         CUDA_TRY(s, cudaMalloc(&s->dInlet, sizeof(double) * tab.size()));
         CUDA_TRY(s, cudaMemcpy(s->dInlet, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice));
@@ -599,6 +601,51 @@ int hype_create(const hype_config *cfg, hype_solver **out)
 
     s->sms = prop.multiProcessorCount;
     return set_tiling(s, s->mixed ? MIXED_CELLS : STAGE_CELLS);
+}
+
+int hype::create_slab(const hype_config *global, int row0, int rows, bool halo_lo, bool halo_hi, hype_solver **out)
+{
+    if (!out) return HYPE_ERR_INVALID;
+    *out = nullptr;
+    hype_solver *s = new (std::nothrow) hype_solver();
+    if (!s) return HYPE_ERR_NOMEM;
+    *out = s;
+    int rc = check_config(global, s);
+    if (rc) return rc;
+    if (global->precision != HYPE_PREC_FP64) return fail(s, HYPE_ERR_INVALID, "y-slabs are implemented for the FP64 kernels");
+    if (rows < 3 || row0 < 0 || row0 + rows > global->ny) return fail(s, HYPE_ERR_INVALID, "bad slab rows %d..%d", row0, row0 + rows - 1);
+    hype_config c = *global;
+    c.ny = rows;
+    const double hy = (global->y_max - global->y_min) / (double)global->ny;   // the slab's extent (informative)
+    c.y_min = global->y_min + (double)row0 * hy;
+    c.y_max = global->y_min + (double)(row0 + rows) * hy;
+    if (halo_lo) c.bc_bottom = BC_HALO;
+    if (halo_hi) c.bc_top = BC_HALO;
+    s->row0 = row0;
+    if (global->bc_left != HYPE_BC_INLET) return create_common(s, &c, 3, nullptr);
+    // the slab's ghost-extended rows -3 .. rows+2 are rows row0-3 .. row0+rows+2 of the whole table
+    std::vector<double> whole, tab;
+    const double h = (global->x_max - global->x_min) / (double)global->nx;
+    const int nv = hype_nvar(global->system);
+    inlet_table(*global, h, whole);
+    tab.assign((size_t)3 * (rows + 6) * nv, 0.0);
+    for (int g = 0; g < 3; ++g)
+        std::memcpy(&tab[(size_t)g * (rows + 6) * nv], &whole[((size_t)g * (global->ny + 6) + row0) * nv], sizeof(double) * (rows + 6) * nv);
+    return create_common(s, &c, 3, &tab);
+}
+
+extern "C" {
+
+int hype_create(const hype_config *cfg, hype_solver **out)
+{
+    if (!out) return HYPE_ERR_INVALID;
+    *out = nullptr;
+    hype_solver *s = new (std::nothrow) hype_solver();
+    if (!s) return HYPE_ERR_NOMEM;
+    *out = s;
+    const int rc = check_config(cfg, s);
+    if (rc) return rc;   // caller reads hype_last_error, then destroys
+    return create_common(s, cfg, 0, nullptr);
 }
 
 // dt of the last RHS: CFL h / (2 s_max) (rhs_function_prim.c:620), or
@@ -932,7 +979,8 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
         CUDA_TRY(s, cudaMemcpyAsync(s->mf[1], s->mf[0], sizeof(float) * 4 * (size_t)s->plane, cudaMemcpyDeviceToDevice, s->stream));
         CUDA_TRY(s, cudaMemcpyAsync(s->md[1], s->md[0], sizeof(double) * 2 * (size_t)s->plane, cudaMemcpyDeviceToDevice, s->stream));
     } else {
-        CUDA_TRY(s, cudaMemcpyAsync(s->dS0, s->dU, sizeof(double) * (size_t)s->plane * s->nv, cudaMemcpyDeviceToDevice, s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(solver_alloc_base(s, s->dS0), solver_alloc_base(s, s->dU), sizeof(double) * (size_t)s->plane * s->nv,
+                                    cudaMemcpyDeviceToDevice, s->stream));
     }
     CUDA_TRY(s, one());   // warm
     CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
@@ -1002,3 +1050,6 @@ int hype_last_elapsed_ms(const hype_solver *s, double *ms)
 }
 
 }  // extern "C"
+
+int hype::solver_reset_scalars(hype_solver *s) { return reset_scalars(s); }
+int hype::solver_read_scalars(hype_solver *s) { return read_scalars(s); }

@@ -60,6 +60,14 @@ struct StageParams {
     int strips, runs;           // tile decomposition: column strips x row runs
     int run0, run_count;        // grid form: the launch covers runs run0 .. run0+run_count-1 (0: all runs)
     double mu1, mu2;            // viscous solvers: MU_1, MU_2 (hype.h:46-47)
+    // y-slab of a decomposed grid: the planes carry row_off halo rows below row 0 and above
+    // row ny-1 (the tensor map starts at row -row_off); rows 0..2 and ny-3..ny-1 of a state
+    // output are also stored into the neighbouring slabs' halo rows, at row + push_shift
+    // of planes push_lo / push_hi (null: no neighbour on that side)
+    int row_off;
+    int push_shift_lo, push_shift_hi;
+    long long push_plane_lo, push_plane_hi;
+    double *push_lo, *push_hi;
 };
 
 // Tile geometry of the stage kernel: a tile is CELLS reconstruction columns

@@ -16,7 +16,10 @@ namespace hype {
 
 enum : int { SYS_EULER = 0, SYS_KAPILA = 1, SYS_BN = 2 };
 // HyPE-2D/hype.h:76 enum bndry_type
-enum : int { BC_WALL = 0, BC_INLET = 1, BC_PERIODIC = 2, BC_REFLECTIVE = 3, BC_TRANSMISSIVE = 4 };
+enum : int { BC_WALL = 0, BC_INLET = 1, BC_PERIODIC = 2, BC_REFLECTIVE = 3, BC_TRANSMISSIVE = 4,
+             // internal: a y-slab edge inside the grid; its ghost rows are the neighbouring
+             // slab's rows, kept in the slab's own halo rows (rows -3..-1 or ny..ny+2)
+             BC_HALO = 5 };
 
 // error bits reported through the device error word
 enum : unsigned { ERR_INADMISSIBLE_FACE = 1u, ERR_NONFINITE = 2u, ERR_TMA_TIMEOUT = 4u, ERR_BAD_LAUNCH = 8u };

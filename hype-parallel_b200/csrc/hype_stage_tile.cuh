@@ -241,7 +241,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::ROW_BYTES);
-                tma_load_3d(row_ptr(row), tmap, xs, src, 0, bar);
+                tma_load_3d(row_ptr(row), tmap, xs, src + p.row_off, 0, bar);   // the map starts row_off rows below row 0
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {
@@ -274,7 +274,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                         for (int c = 0; c < NV; ++c) Q[c] = rp[c * BW + (gm - xs)];
                     } else {
 #pragma unroll
-                        for (int c = 0; c < NV; ++c) Q[c] = p.in[(size_t)c * p.plane + (size_t)src * p.pitch + gm];
+                        for (int c = 0; c < NV; ++c) Q[c] = p.in[(long long)c * p.plane + (long long)src * p.pitch + gm];
                     }
                 }
                 __syncthreads();
@@ -520,6 +520,11 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                             o = 15.0 * w1 + (-5.0) * w;
                         }
                         p.out[(size_t)c * p.plane + gidx] = o;
+                        // a y-slab's edge rows are the neighbours' halo rows: store them there too
+                        if (p.push_lo && jo < 3)
+                            p.push_lo[(long long)c * p.push_plane_lo + (long long)(jo + p.push_shift_lo) * p.pitch + i] = o;
+                        if (p.push_hi && jo >= p.ny - 3)
+                            p.push_hi[(long long)c * p.push_plane_hi + (long long)(jo + p.push_shift_hi) * p.pitch + i] = o;
                     }
                 }
 #pragma unroll

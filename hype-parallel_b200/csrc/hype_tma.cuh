@@ -44,15 +44,18 @@ __device__ __forceinline__ void mbar_inval(uint64_t *bar)
 }
 
 // Ghost source index along one axis (rhs_function_prim.c:75-315 and the DMDA
-// periodic wrap): transmissive copies the edge cell, reflective mirrors.
+// periodic wrap): transmissive copies the edge cell, reflective mirrors; a
+// slab edge (BC_HALO) reads its halo rows as they are.
 __device__ __forceinline__ int map_axis(int g, int n, int bc_lo, int bc_hi)
 {
     if (g < 0) {
+        if (bc_lo == BC_HALO) return g;
         if (bc_lo == BC_PERIODIC || bc_hi == BC_PERIODIC) return g + n;
         if (bc_lo == BC_REFLECTIVE) return -1 - g;
         return 0;   // transmissive (inlet columns are replaced after conversion)
     }
     if (g >= n) {
+        if (bc_hi == BC_HALO) return g;
         if (bc_lo == BC_PERIODIC || bc_hi == BC_PERIODIC) return g - n;
         if (bc_hi == BC_REFLECTIVE) return 2 * (n - 1) - g + 1;
         return n - 1;

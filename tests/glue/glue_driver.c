@@ -10,6 +10,9 @@
 #include <string.h>
 
 PetscReal GAMMA_1 = 1.4, GAMMA_2 = 1.4, PI_1 = 0.0, PI_2 = 0.0;
+PetscReal MU_1 = 1.0e-2, MU_2 = 0.0;   /* hype.h:46-47; read by the VISCOUS build */
+
+void glue_set_mu(double mu1, double mu2) { MU_1 = mu1; MU_2 = mu2; }
 
 PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx);
 PetscErrorCode RHSFunction(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx);

@@ -92,6 +92,32 @@ def test_valid_config_without_gpu_reports_no_device(hp):
     assert ei.value.status in (hp.ERR_NO_DEVICE, hp.ERR_CUDA)
 
 
+@pytest.mark.parametrize("change,nslabs,needle", [
+    (dict(), 0, "nslabs"),
+    (dict(ny=12), 5, "ny/3"),
+    (dict(precision=1, order=2), 2, "FP64"),
+    (dict(nx=2), 1, "3x3"),
+])
+def test_group_rejects_before_device(hp, change, nslabs, needle):
+    """y-slab groups: 1..ny/3 slabs of an FP64 configuration, checked before any device call."""
+    cfg = hp.Config(nx=16, ny=16)
+    for k, v in change.items():
+        setattr(cfg, k, v)
+    with pytest.raises(hp.HypeError) as ei:
+        hp.Group(cfg, nslabs)
+    assert ei.value.status == hp.ERR_INVALID
+    assert needle.lower() in str(ei.value).lower()
+
+
+def test_group_without_gpu_reports_no_device(hp):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(hp.HypeError) as ei:
+        hp.Group(hp.Config(nx=16, ny=16), 2)
+    assert ei.value.status == hp.ERR_NO_DEVICE
+
+
 def test_initial_states_deterministic_and_admissible(hp):
     c = hp.Config(nx=64, ny=48)
     a = hp.initial_state(c, "shock_bubble", seed=3, nbubbles=4)

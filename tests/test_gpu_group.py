@@ -1,0 +1,140 @@
+"""One grid split into y-slabs (include/hype_group.h) against the reference's bits.
+
+HyPE-2D decomposes its grid over MPI ranks with a DMDA (hype.c:108-122) and
+refreshes 3 ghost rows per rank before every RHS (rhs_function_prim.c:44-45);
+dt is the global minimum (rhs_function_prim.c:620-623).  A decomposed run must
+give the same bits as the undecomposed one.  Here every solve case of the golden
+file is rerun with its rows split over 2 and 3 slabs, against the reference's
+hashes.  Larger and uneven splits, every system, order and path, and periodic,
+inlet and reflective edges are checked against a lone Solver.  The slabs share
+the test's one GPU.  Their kernels never wait on each other inside a launch:
+the ordering is events between streams.
+"""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import cases
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_outputs.json")))
+T, R, P, I = O.TRANSMISSIVE, O.REFLECTIVE, O.PERIODIC, O.INLET
+
+
+def sha(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float64).tobytes()).hexdigest()
+
+
+@pytest.mark.parametrize("nslabs", [2, 3])
+@pytest.mark.parametrize("name", sorted(GOLDEN["solve"]))
+def test_group_solve_equals_reference(name, nslabs, hp):
+    g = GOLDEN["solve"][name]
+    (_, cfg, kind, seed), t0, tf, nmax = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    with hp.Group(cases.to_pkg(cfg), nslabs) as grp:
+        grp.set_state(U)
+        steps, te, dtn, st = grp.solve(t0, tf, nmax)
+        Ue = grp.get_state()
+    if g["status"] != 0:
+        assert st == hp.ERR_INADMISSIBLE
+        return
+    assert st == hp.OK
+    assert steps == g["steps"]
+    assert float(te).hex() == g["t_end"]
+    assert float(dtn).hex() == g["dt_next"]
+    assert sha(Ue) == g["sha_U_end"]
+
+
+def lone(hp, pcfg, U, t0, tf, nmax):
+    with hp.Solver(pcfg) as s:
+        s.set_state(U)
+        k, t, dt, st = s.solve(t0, tf, nmax)
+        return k, t, dt, st, s.get_state()
+
+
+GROUP_CASES = [
+    # (case, nslabs, steps)
+    (cases._k("kapila_64x50_uneven", 64, 50, bcs=(T, T, R, R), seed=70), 3, 12),          # 17 + 17 + 16 rows
+    (cases._k("kapila_48x40_periodic4", 48, 40, bcs=(P, P, P, P), kind="rough", seed=71), 4, 8),
+    (cases._k("kapila_40x24_periodic2", 40, 24, bcs=(T, R, P, P), seed=72), 2, 8),        # both neighbours are one slab
+    (cases._k("kapila_30x9_min_rows", 30, 9, bcs=(R, T, R, T), kind="rough", seed=73), 3, 6),   # 3 rows a slab
+    (cases._k("kapila_36x30_inlet", 36, 30, bcs=(I, T, R, R), kind="rough", seed=74, x_min=0.0, x_max=2.0,
+              y_min=-1.0, y_max=1.0), 3, 6),
+    (cases._k("kapila_32x33_N0", 32, 33, order=0, bcs=(T, T, R, R), seed=75), 3, 10),
+    (cases._k("kapila_32x31_N1", 32, 31, order=1, bcs=(R, R, T, T), kind="rough", seed=76), 5, 10),
+    (cases._k("kapila_24x27_N3", 24, 27, order=3, bcs=(T, T, P, P), seed=77), 3, 3),
+    (cases._k("kapila_cons_40x30", 40, 30, bcs=(T, T, R, R), seed=78, conservative=1), 3, 8),
+    (cases._k("kapila_visc_40x30", 40, 30, bcs=(T, T, R, R), seed=79, viscous=1, mu1=0.5, mu2=0.1), 3, 6),
+    (cases._k("kapila_visc_cons_30x28_N3", 30, 28, order=3, bcs=(R, T, P, P), seed=80, conservative=1, viscous=1,
+              mu1=2.0, mu2=0.5), 4, 3),
+    (cases._b("bn_40x36_fixed", 40, 36, bcs=(T, T, R, R), seed=81, fixed=1), 3, 8),
+    (cases._b("bn_cons_30x30_N3", 30, 30, order=3, bcs=(P, P, P, P), seed=82, conservative=1), 2, 3),
+    (cases._e("euler_48x40_N1", 48, 40, order=1, bcs=(T, T, R, R), seed=83), 6, 100000),   # to t_final (MATCHSTEP)
+    (cases._e("euler_cons_40x32", 40, 32, bcs=(R, R, P, P), seed=84, conservative=1), 4, 100000),
+]
+
+
+@pytest.mark.parametrize("case,nslabs,nmax", GROUP_CASES, ids=[c[0][0] for c in GROUP_CASES])
+def test_group_equals_lone_solver(case, nslabs, nmax, hp):
+    _, cfg, kind, seed = case
+    tf = 0.02 if cfg.system == O.EULER else 1.0
+    U = cases.state(cfg, kind, seed)
+    pcfg = cases.to_pkg(cfg)
+    k1, t1, dt1, st1, U1 = lone(hp, pcfg, U, 0.0, tf, nmax)
+    with hp.Group(pcfg, nslabs) as grp:
+        rows = [grp.slab(k) for k in range(nslabs)]
+        assert [r[0] for r in rows] == list(np.cumsum([0] + [r[1] for r in rows])[:-1])
+        assert sum(r[1] for r in rows) == cfg.ny and max(r[1] for r in rows) - min(r[1] for r in rows) <= 1
+        grp.set_state(U)
+        k2, t2, dt2, st2 = grp.solve(0.0, tf, nmax)
+        U2 = grp.get_state()
+    assert st1 == st2 == hp.OK
+    assert (k1, t1.hex(), dt1.hex()) == (k2, t2.hex(), dt2.hex())
+    assert U1.tobytes() == U2.tobytes(), float(np.abs(U1 - U2).max())
+
+
+def test_group_one_slab_and_split_runs(hp):
+    """nslabs = 1 is the lone solver; begin / advance / wait in chunks equals one solve."""
+    _, cfg, kind, seed = cases._k("kapila_40x36", 40, 36, bcs=(T, T, R, R), seed=85)
+    U = cases.state(cfg, kind, seed)
+    pcfg = cases.to_pkg(cfg)
+    k1, t1, dt1, st1, U1 = lone(hp, pcfg, U, 0.0, 1.0, 9)
+    with hp.Group(pcfg, 1) as grp:
+        grp.set_state(U)
+        assert grp.solve(0.0, 1.0, 9)[:3] == (k1, t1, dt1)
+        assert grp.get_state().tobytes() == U1.tobytes()
+    with hp.Group(pcfg, 3) as grp:
+        grp.set_state(U)
+        grp.begin(0.0, 1.0, 9)
+        for n in (2, 3, 4, 5):           # the last chunk runs past max_steps: no extra step
+            grp.advance(n)
+        k, t, dt, st = grp.wait()
+        assert (k, t, dt, st) == (k1, t1, dt1, hp.OK)
+        assert grp.get_state().tobytes() == U1.tobytes()
+        assert grp.last_elapsed_ms() > 0.0
+
+
+def test_group_stops_with_the_reference_error(hp):
+    """The Baer-Nunziato phase-2 pressure as written (V[8], baer_nunziato.c:271)
+    makes these states inadmissible after some steps: the slabs stop at the
+    same step as the lone solver, with the same first cell."""
+    _, cfg, kind, seed = cases._b("bn_48x45_bug", 48, 45, bcs=(T, T, T, T), seed=86)
+    U = cases.state(cfg, kind, seed)
+    pcfg = cases.to_pkg(cfg)
+    with hp.Solver(pcfg) as s:
+        s.set_state(U)
+        k1, t1, dt1, st1 = s.solve(0.0, 1.0, 400)
+        msg1 = hp.lib().hype_last_error(s._h).decode()
+    if st1 != hp.ERR_INADMISSIBLE:
+        pytest.skip("this state did not become inadmissible within 400 steps")
+    with hp.Group(pcfg, 3) as grp:
+        grp.set_state(U)
+        k2, t2, dt2, st2 = grp.solve(0.0, 1.0, 400)
+        assert st2 == hp.ERR_INADMISSIBLE
+        assert (k1, t1) == (k2, t2)
+        assert grp.last_error() == msg1

@@ -18,20 +18,23 @@ import oracle as O
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GLUE = os.path.join(ROOT, "tests", "glue")
-LIBNAME = {O.EULER: "euler", O.KAPILA: "kapila", O.BN: "bn"}
+# (system, viscous) -> library; "kapila_visc" is the glue compiled with VISCOUS defined
+LIBNAME = {(O.EULER, 0): "euler", (O.KAPILA, 0): "kapila", (O.BN, 0): "bn", (O.KAPILA, 1): "kapila_visc"}
 
 
 @pytest.fixture(scope="module")
 def glue_libs(hp):
     subprocess.run(["make", "-s", "-C", GLUE], check=True, capture_output=True)
     libs = {}
-    for sysid, nm in LIBNAME.items():
+    for key, nm in LIBNAME.items():
         L = ctypes.CDLL(os.path.join(GLUE, "_build", f"libglue_{nm}.so"))
         DP = ctypes.POINTER(ctypes.c_double)
         IP = ctypes.POINTER(ctypes.c_int)
         L.glue_rhs.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, DP, ctypes.c_double, IP, DP, ctypes.c_int, DP, DP, DP]
         L.glue_rhs.restype = ctypes.c_int
-        libs[sysid] = L
+        if key[1]:
+            L.glue_set_mu.argtypes = [ctypes.c_double, ctypes.c_double]
+        libs[key] = L
     return libs
 
 
@@ -39,6 +42,8 @@ def glue_rhs(L, cfg, U):
     dom = (ctypes.c_double * 4)(cfg.x_min, cfg.x_max, cfg.y_min, cfg.y_max)
     bc = (ctypes.c_int * 4)(cfg.bc_left, cfg.bc_right, cfg.bc_bottom, cfg.bc_top)
     eos = (ctypes.c_double * 4)(cfg.gamma1, cfg.gamma2, cfg.pi1, cfg.pi2)
+    if cfg.viscous:
+        L.glue_set_mu(cfg.mu1, cfg.mu2)
     R = np.empty_like(U)
     dt = ctypes.c_double(0.0)
     DP = ctypes.POINTER(ctypes.c_double)
@@ -57,14 +62,16 @@ def test_glue_without_gpu_returns_an_error(hp, glue_libs):
     if torch.cuda.is_available():
         pytest.skip("a GPU is present")
     cfg = O.Config(system=O.KAPILA, order=2, nx=8, ny=8, **cases.KAPILA_EOS)
-    R, dt, st = glue_rhs(glue_libs[O.KAPILA], cfg, cases.state(cfg, "bubble", 1))
+    R, dt, st = glue_rhs(glue_libs[(O.KAPILA, 0)], cfg, cases.state(cfg, "bubble", 1))
     assert st == hp.ERR_NO_DEVICE
 
 
 GLUE_CASES = ["kapila_37x23_rough_mixed_bc", "kapila_18x14_inlet", "kapila_15x13_N3", "euler_21x19_reflective_N1",
               "bn_16x16", "bn_13x21_periodic_N1",
               # RHSFunction (Ctx.ReconsPrimitive false)
-              "kapila_cons_37x23_rough", "kapila_cons_18x14_inlet", "euler_cons_17x12_periodic_N3", "bn_cons_12x10_N3"]
+              "kapila_cons_37x23_rough", "kapila_cons_18x14_inlet", "euler_cons_17x12_periodic_N3", "bn_cons_12x10_N3",
+              # a tree built with VISCOUS: MU_1, MU_2 from the globals
+              "kapila_visc_37x23_rough", "kapila_visc_15x13_N3", "kapila_visc_cons_24x20_walls"]
 
 
 @pytest.mark.gpu
@@ -74,7 +81,7 @@ def test_glue_rhs_bitwise_vs_oracle(name, hp, orc, glue_libs):
     U = cases.state(cfg, kind, seed)
     Ro, dto, sto = orc.rhs(cfg, U)
     assert sto == O.OK
-    R, dt, st = glue_rhs(glue_libs[cfg.system], cfg, U)
+    R, dt, st = glue_rhs(glue_libs[(cfg.system, int(cfg.viscous))], cfg, U)
     assert st == 0
     assert dt == dto
     assert R.tobytes() == Ro.tobytes()
