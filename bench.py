@@ -397,8 +397,16 @@ def serve_leg(hp, args, local_rank, capacity):
     for nm, sysid in (("kapila", hp.KAPILA_5EQN), ("bn", hp.BAER_NUNZIATO), ("euler", hp.EULER)):
         sel = np.array([r.cfg.system == sysid for r in reqs])
         if sel.any():
+            fails = {}
+            for i in np.nonzero(sel)[0]:
+                if res[i]["status"] != hp.OK:
+                    key = hp.lib().hype_status_string(res[i]["status"]).decode()
+                    fails[key] = fails.get(key, 0) + 1
             by_sys[nm] = {"n": int(sel.sum()), "p50_s": float(np.percentile(lat[sel], 50)),
-                          "p99_s": float(np.percentile(lat[sel], 99))}
+                          "p99_s": float(np.percentile(lat[sel], 99)), "failed": fails}
+    # the first failed requests: which grid, how many steps asked and done
+    failures = [{"i": i, "system": int(r.cfg.system), "side": r.cfg.nx, "steps": r.max_steps, "steps_done": res[i]["steps"],
+                 "status": res[i]["status"]} for i, r in enumerate(reqs) if res[i]["status"] != hp.OK][:40]
     return {"workload": f"Poisson stream of {n} solves: 70/20/10 kapila5/bn/euler, square grids 64..2048 log-uniform, "
                         "50..2000 steps log-uniform, N=2 SSPRK(4,3), 150 GB HBM budget",
             "requests": n, "kapila_precision": args.serve_kapila, "active_cells": args.serve_active_cells,
@@ -409,7 +417,7 @@ def serve_leg(hp, args, local_rank, capacity):
             "value": st["cell_updates_per_s"], "unit": UNIT, "wall_s": st["wall_s"],
             "completed": st["completed"], "failed": st["failed"], "peak_instances": st["peak_instances"],
             "peak_bytes": st["peak_bytes"], "polls": st["polls"], "batch_steps": st["steps_replayed"],
-            "by_system": by_sys}
+            "by_system": by_sys, "failures": failures}
 
 
 def run_gpu(args, rank, world, local_rank):

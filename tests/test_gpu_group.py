@@ -60,13 +60,15 @@ def lone(hp, pcfg, U, t0, tf, nmax):
 GROUP_CASES = [
     # (case, nslabs, steps)
     (cases._k("kapila_64x50_uneven", 64, 50, bcs=(T, T, R, R), seed=70), 3, 12),          # 17 + 17 + 16 rows
-    (cases._k("kapila_48x40_periodic4", 48, 40, bcs=(P, P, P, P), kind="rough", seed=71), 4, 8),
+    (cases._k("kapila_48x40_periodic4", 48, 40, bcs=(P, P, P, P), seed=71), 4, 8),
     (cases._k("kapila_40x24_periodic2", 40, 24, bcs=(T, R, P, P), seed=72), 2, 8),        # both neighbours are one slab
-    (cases._k("kapila_30x9_min_rows", 30, 9, bcs=(R, T, R, T), kind="rough", seed=73), 3, 6),   # 3 rows a slab
-    (cases._k("kapila_36x30_inlet", 36, 30, bcs=(I, T, R, R), kind="rough", seed=74, x_min=0.0, x_max=2.0,
+    (cases._k("kapila_30x9_min_rows", 30, 9, bcs=(R, T, R, T), seed=73), 3, 6),   # 3 rows a slab
+    # a rough field that turns inadmissible: both stop at the same step with the same state
+    (cases._k("kapila_30x9_rough_stops", 30, 9, bcs=(R, T, R, T), kind="rough", seed=73), 3, 6),
+    (cases._k("kapila_36x30_inlet", 36, 30, bcs=(I, T, R, R), seed=74, x_min=0.0, x_max=2.0,
               y_min=-1.0, y_max=1.0), 3, 6),
     (cases._k("kapila_32x33_N0", 32, 33, order=0, bcs=(T, T, R, R), seed=75), 3, 10),
-    (cases._k("kapila_32x31_N1", 32, 31, order=1, bcs=(R, R, T, T), kind="rough", seed=76), 5, 10),
+    (cases._k("kapila_32x31_N1", 32, 31, order=1, bcs=(R, R, T, T), seed=76), 5, 10),
     (cases._k("kapila_24x27_N3", 24, 27, order=3, bcs=(T, T, P, P), seed=77), 3, 3),
     (cases._k("kapila_cons_40x30", 40, 30, bcs=(T, T, R, R), seed=78, conservative=1), 3, 8),
     (cases._k("kapila_visc_40x30", 40, 30, bcs=(T, T, R, R), seed=79, viscous=1, mu1=0.5, mu2=0.1), 3, 6),
@@ -93,7 +95,8 @@ def test_group_equals_lone_solver(case, nslabs, nmax, hp):
         grp.set_state(U)
         k2, t2, dt2, st2 = grp.solve(0.0, tf, nmax)
         U2 = grp.get_state()
-    assert st1 == st2 == hp.OK
+    assert st1 == st2
+    assert st1 == (hp.ERR_INADMISSIBLE if kind == "rough" else hp.OK)
     assert (k1, t1.hex(), dt1.hex()) == (k2, t2.hex(), dt2.hex())
     assert U1.tobytes() == U2.tobytes(), float(np.abs(U1 - U2).max())
 
