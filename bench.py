@@ -38,6 +38,15 @@ PKG_DIR = os.path.join(ROOT, "hype-parallel_b200")
 METRIC = "cell-updates/s FP64 plain vs mixed+batched at L1<=1e-5; serving p50/p99 latency"
 UNIT = "cell-updates/s"
 NX = NY = 2048
+# Algorithmic FP64 operations of one RHS evaluation of this workload (2048^2 Kapila,
+# N = 2, 4-bubble shock-bubble state of seed 0): the reference's arithmetic counted
+# operation by operation (oracle/flops.cpp; tests/test_flops.py recounts it):
+# 8728100905 additions, 10411302998 multiplications, 894672899 divisions and
+# 33570816 square roots, i.e. 4784.5 per cell.
+RHS_FLOPS_2048 = 20067647618
+# the SSPRK(4,3) combinations per cell: three AXPY stages (1 mul + 1 add per field)
+# and the AXPBYPCZ stage (3 mul + 2 add per field), 6 fields
+RK_FLOPS_PER_CELL = 3 * 2 * 6 + 5 * 6
 NBUB = 4
 SEED = 0
 BYTES_PER_CELL_UPDATE = 9 * 6 * 8    # SSPRK(4,3): 5 state reads + 4 state writes of 6 FP64 fields
@@ -461,6 +470,17 @@ def run_gpu(args, rank, world, local_rank):
     achieved = alg_bytes_launch / (ms_stage * 1e-3) / 1e9
     peak, peak_src = peaks()
     totals, amin, amax = solver.totals()
+    # FP64 roofline: the reference's operation count per cell-update against the
+    # measured rate of separately rounded FP64 multiplies and adds
+    flops_cu = 4 * RHS_FLOPS_2048 / (NX * NY) + RK_FLOPS_PER_CELL
+    fp64_peak = hp.fp64_rate(local_rank, 5)
+    fp64 = {"flops_per_cell_update": flops_cu, "achieved_tflops": value / world * flops_cu / 1e12,
+            "peak_tflops": fp64_peak / 1e12, "frac": (value / world * flops_cu) / fp64_peak,
+            "stage_kernel_frac": (NX * NY * RHS_FLOPS_2048 / (NX * NY) / (ms_stage * 1e-3)) / fp64_peak,
+            "peak_source": "hype_fp64_rate: independent FP64 multiply and add chains on every SM, no FMA (as the bit-exact "
+                           "kernels), best of 5 launches",
+            "note": "divisions and square roots count one operation each (213.3 and 8.0 per cell-RHS) but run as "
+                    "multi-instruction sequences on the FP64 pipe"}
 
     # end to end through the C ABI with host buffers: per step the state goes
     # host (pinned) -> device, one SSP-RK step runs, the state comes back.
@@ -534,7 +554,7 @@ def run_gpu(args, rank, world, local_rank):
                        "system": "kapila5", "order": 2, "bubbles": NBUB, "cfl": 0.4, "precision": "fp64-bitexact",
                        "parallelism": f"replicas{world}", "l2": "state 201 MB per buffer > 126 MB L2 (no flush needed)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_src,
+                         "traffic": None, "peak_source": peak_src, "fp64": fp64,
                          "note": "stage kernel alone: 96 B/cell algorithmic (one FP64 state read + one write) per launch; "
                                  "the kernel is FP64-pipe bound, see profiles/"},
             "stage_kernel": {"ms_per_launch": ms_stage, "launch": info, "autotuned_tile": tile},

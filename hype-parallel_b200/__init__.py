@@ -164,6 +164,7 @@ def lib() -> ctypes.CDLL:
         L.hype_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.hype_config_default.argtypes = [ctypes.POINTER(_Cfg)]
         L.hype_get_primitive.argtypes = [vp, _DP]
+        L.hype_fp64_rate.argtypes = [ctypes.c_int, ctypes.c_int, _DP]
         L.hype_group_create.argtypes = [ctypes.POINTER(_Cfg), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(vp)]
         L.hype_group_destroy.argtypes = [vp]
         L.hype_group_last_error.argtypes = [vp]
@@ -410,6 +411,16 @@ class Solver:
         ms = ctypes.c_double(0.0)
         self._check(lib().hype_last_elapsed_ms(self._h, ctypes.byref(ms)))
         return ms.value
+
+
+def fp64_rate(device: int = 0, reps: int = 5) -> float:
+    """Measured rate of separately rounded FP64 multiplies and adds on `device`
+    (hype_fp64_rate): the FP64 roofline of the bit-exact kernels, in ops/s."""
+    r = ctypes.c_double(0.0)
+    st = lib().hype_fp64_rate(device, reps, ctypes.byref(r))
+    if st != OK:
+        raise HypeError(st, lib().hype_status_string(st).decode())
+    return r.value
 
 
 class Group:

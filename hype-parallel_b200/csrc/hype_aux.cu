@@ -3,6 +3,7 @@
 // per-step time-step control that HyPE-2D's MonitorFunction and PETSc TS do on
 // the host (post_process.c:19, hype.c:356-359).  Built with --fmad=false.
 #include <cuda_runtime.h>
+#include <algorithm>
 #include "hype_internal.h"
 
 namespace hype {
@@ -302,3 +303,63 @@ cudaError_t launch_totals(const double *planes, double *red, int nx, int ny, int
 }
 
 }  // namespace hype
+
+// ---------------------------------------------------------------------------
+// FP64 rate: 8 independent chains x = x*m + c per thread, which --fmad=false
+// keeps as one multiply and one add each.  The data-dependent store keeps the
+// chains alive; it never fires for these constants.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int RATE_CHAINS = 8;
+__global__ void __launch_bounds__(256) fp64_rate_kernel(double *sink, int iters, double seed)
+{
+    double x[RATE_CHAINS];
+#pragma unroll
+    for (int k = 0; k < RATE_CHAINS; ++k) x[k] = seed + 1e-3 * k + 1e-9 * threadIdx.x;
+    const double m = 0.999999999, c = 1e-9;
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < RATE_CHAINS; ++k) x[k] = x[k] * m + c;
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < RATE_CHAINS; ++k) s += x[k];
+    if (s == -1.0) sink[0] = s;
+}
+}  // namespace
+
+extern "C" int hype_fp64_rate(int device, int reps, double *ops_per_s)
+{
+    if (!ops_per_s || reps < 1) return HYPE_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return HYPE_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return HYPE_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    double *sink = nullptr;
+    cudaStream_t st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = HYPE_OK;
+    if (cudaMalloc(&sink, sizeof(double)) != cudaSuccess) return HYPE_ERR_NOMEM;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+        cudaEventCreate(&e1) != cudaSuccess)
+        rc = HYPE_ERR_CUDA;
+    const int blocks = sms * 8, threads = 256, iters = 4096;
+    double best = 0.0;
+    for (int r = 0; r <= reps && rc == HYPE_OK; ++r) {   // launch 0 warms up
+        cudaEventRecord(e0, st);
+        fp64_rate_kernel<<<blocks, threads, 0, st>>>(sink, iters, 1.0 + r);
+        cudaEventRecord(e1, st);
+        if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) { rc = HYPE_ERR_CUDA; break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double ops = 2.0 * RATE_CHAINS * (double)iters * blocks * threads;
+        if (r > 0 && ms > 0.f) best = std::max(best, ops / (ms * 1e-3));
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (st) cudaStreamDestroy(st);
+    cudaFree(sink);
+    *ops_per_s = best;
+    return rc;
+}

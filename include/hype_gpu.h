@@ -251,6 +251,13 @@ HYPE_API int hype_autotune(hype_solver *s, int reps, int *cells, int *waves);
  * (CUDA events around the step replays). */
 HYPE_API int hype_last_elapsed_ms(const hype_solver *s, double *ms);
 
+/* The FP64 roofline of the bit-exact kernels, measured on `device`: the rate of
+ * separately rounded FP64 multiplies and adds (the kernels are built without
+ * FMA contraction), from a short kernel of independent multiply-add chains on
+ * every SM, best of `reps` launches timed with CUDA events.  *ops_per_s counts
+ * one per multiply and one per add. */
+HYPE_API int hype_fp64_rate(int device, int reps, double *ops_per_s);
+
 #ifdef __cplusplus
 }
 #endif

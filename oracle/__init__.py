@@ -24,6 +24,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libhype_oracle.so")
+FLOPS_LIB = os.path.join(HERE, "_build", "libhype_oracle_flops.so")   # the oracle with counted operations
 REF_LIB = {0: os.path.join(HERE, "_ref", "libhype_ref_euler.so"),
            1: os.path.join(HERE, "_ref", "libhype_ref_kapila.so"),
            2: os.path.join(HERE, "_ref", "libhype_ref_bn.so")}
@@ -105,6 +106,29 @@ def reference_available() -> bool:
 
 def viscous_reference_available() -> bool:
     return os.path.exists(REF_LIB_VISCOUS)
+
+
+FLOP_KINDS = ("add", "mul", "div", "sqrt", "cmp", "abs", "neg", "trans")
+
+
+def count_rhs_ops(cfg: Config, U: np.ndarray):
+    """The floating-point operations of one oracle RHS evaluation (oracle/flops.cpp):
+    returns (RHS, status, {kind: count}); "flops" = add + mul + div + sqrt."""
+    if not os.path.exists(FLOPS_LIB):
+        subprocess.run(["make", "-s", "-C", HERE, "flops"], check=True)
+    lib = ctypes.CDLL(FLOPS_LIB, mode=os.RTLD_LOCAL | os.RTLD_NOW)
+    lib.hyo_rhs.argtypes = [ctypes.POINTER(_HyoConfig), ctypes.c_double, _DP, _DP, _DP]
+    lib.hyo_flops_read.argtypes = [ctypes.POINTER(ctypes.c_ulonglong)]
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    R = np.empty_like(U)
+    dt = ctypes.c_double(0.0)
+    lib.hyo_flops_reset()
+    st = lib.hyo_rhs(ctypes.byref(Oracle._cfg(cfg)), 0.0, _ptr(U), _ptr(R), ctypes.byref(dt))
+    out = (ctypes.c_ulonglong * 8)()
+    lib.hyo_flops_read(out)
+    counts = dict(zip(FLOP_KINDS, [int(v) for v in out]))
+    counts["flops"] = counts["add"] + counts["mul"] + counts["div"] + counts["sqrt"]
+    return R, st, counts
 
 
 class Oracle:

@@ -1181,8 +1181,8 @@ int hyo_solve(const hyo_config *cfg, double *U, double t0, double t_final, int m
     double dt_ctx, t = t0;
     int steps = 0, rc;
 #define RHS_AT(st, in) do { rc = hyo_rhs(cfg, (st), (in), F, &dt_ctx); if (rc) goto done; } while (0)
+    double time_step;                           /* declared before the first RHS_AT: valid C++ too */
     RHS_AT(t0, U);                              /* hype.c:343 seeds Ctx.dt */
-    double time_step = dt_ctx;
     for (;;) {
         time_step = dt_ctx;                     /* MonitorFunction, post_process.c:19 */
         if (steps >= max_steps || t >= t_final) break;
