@@ -47,6 +47,9 @@ RHS_FLOPS_2048 = 20067647618
 # the SSPRK(4,3) combinations per cell: three AXPY stages (1 mul + 1 add per field)
 # and the AXPBYPCZ stage (3 mul + 2 add per field), 6 fields
 RK_FLOPS_PER_CELL = 3 * 2 * 6 + 5 * 6
+# DRAM bytes of one stage-kernel launch on this workload, from an ncu capture of the
+# kernel (dram__bytes_read.sum + dram__bytes_write.sum: 211,055,616 + 159,402,496)
+STAGE_TRAFFIC_BYTES = 211055616 + 159402496
 NBUB = 4
 SEED = 0
 BYTES_PER_CELL_UPDATE = 9 * 6 * 8    # SSPRK(4,3): 5 state reads + 4 state writes of 6 FP64 fields
@@ -567,7 +570,8 @@ def run_gpu(args, rank, world, local_rank):
                        "system": "kapila5", "order": 2, "bubbles": NBUB, "cfl": 0.4, "precision": "fp64-bitexact",
                        "parallelism": f"replicas{world}", "l2": "state 201 MB per buffer > 126 MB L2 (no flush needed)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_source": peak_src, "fp64": fp64,
+                         "traffic": STAGE_TRAFFIC_BYTES, "traffic_source": "one ncu capture of the stage kernel (profiles/)",
+                         "algorithmic_bytes": alg_bytes_launch, "peak_source": peak_src, "fp64": fp64,
                          "note": "stage kernel alone: 96 B/cell algorithmic (one FP64 state read + one write) per launch; "
                                  "the kernel is FP64-pipe bound, see profiles/"},
             "stage_kernel": {"ms_per_launch": ms_stage, "launch": info, "autotuned_tile": tile},
