@@ -670,7 +670,7 @@ static int read_scalars(hype_solver *s)
     if (s->hSc->err & ERR_INADMISSIBLE_FACE) {
         const unsigned cell = s->hSc->err_cell;
         return fail(s, HYPE_ERR_INADMISSIBLE, "inadmissible face state near cell (i=%u, j=%u)",
-                    cell % (unsigned)s->cfg.nx, cell / (unsigned)s->cfg.nx);
+                    cell % (unsigned)s->cfg.nx, cell / (unsigned)s->cfg.nx + (unsigned)s->row0);
     }
     return HYPE_OK;
 }
@@ -714,6 +714,7 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
 {
     (void)t;
     if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
+    if (s->row_off) return fail(s, HYPE_ERR_INVALID, "a slab solver takes hype_rhs_prim_slab");
     if (!s->dSc) return fail(s, HYPE_ERR_INVALID, "solver not created");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     int rc;
@@ -750,10 +751,44 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
     return rc;
 }
 
+int hype_create_slab(const hype_config *cfg, int row0, int rows, hype_solver **out)
+{
+    if (!cfg) return HYPE_ERR_INVALID;
+    const bool whole = row0 == 0 && rows == cfg->ny;
+    const bool periodic = cfg->bc_bottom == HYPE_BC_PERIODIC;
+    return create_slab(cfg, row0, rows, !whole && (row0 > 0 || periodic), !whole && (row0 + rows < cfg->ny || periodic), out);
+}
+
+int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_stride, double *RHS, double *dt)
+{
+    (void)t;
+    if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
+    if (!s->dSc || s->row_off == 0) return fail(s, HYPE_ERR_INVALID, "not a slab solver (hype_create_slab)");
+    const int nx = s->cfg.nx, rows = s->cfg.ny;
+    if (row_stride < (long long)nx * s->nv) return fail(s, HYPE_ERR_INVALID, "row_stride below nx * nvar");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
+    const int lo = s->cfg.bc_bottom == BC_HALO ? 3 : 0, hi = s->cfg.bc_top == BC_HALO ? 3 : 0;
+    const size_t row_bytes = sizeof(double) * (size_t)nx * s->nv;
+    // the slab's rows and its ghost rows into the staging array (local row -3 first), then planes
+    CUDA_TRY(s, cudaMemcpy2DAsync(s->dAosIn + (size_t)(3 - lo) * nx * s->nv, row_bytes, U - (long long)lo * row_stride,
+                                  sizeof(double) * (size_t)row_stride, row_bytes, (size_t)(rows + lo + hi), cudaMemcpyHostToDevice,
+                                  s->stream));
+    CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dS0), nx, 3 - lo, rows + lo + hi, s->nv, s->pitch,
+                                          s->plane, s->stream));
+    int rc;
+    if ((rc = reset_scalars(s))) return rc;
+    CUDA_TRY(s, stage(s, s->dS0, s->dAosOut, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
+    CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, row_bytes * rows, cudaMemcpyDeviceToHost, s->stream));
+    if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
+    if (dt) *dt = host_dt(s);
+    return rc;
+}
+
 int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRHS, double *dt)
 {
     (void)t;
     if (!s || !dU || !dRHS) return fail(s, HYPE_ERR_INVALID, "null argument");
+    if (s->row_off) return fail(s, HYPE_ERR_INVALID, "a slab solver takes hype_rhs_prim_slab");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     CUDA_TRY(s, load_state(s, dU, 1));
     return rhs_common(s, dRHS, dt);
@@ -762,6 +797,7 @@ int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRH
 int hype_set_state(hype_solver *s, const double *U)
 {
     if (!s || !U) return fail(s, HYPE_ERR_INVALID, "null argument");
+    if (s->row_off) return fail(s, HYPE_ERR_INVALID, "a slab solver has no time loop of its own (hype_group runs slabs)");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
     CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
@@ -801,6 +837,7 @@ static int ensure_step_graph(hype_solver *s)
 int hype_begin(hype_solver *s, double t0, double t_final, int max_steps)
 {
     if (!s) return HYPE_ERR_INVALID;
+    if (s->row_off) return fail(s, HYPE_ERR_INVALID, "a slab solver has no time loop of its own (hype_group runs slabs)");
     if (max_steps < 0) return fail(s, HYPE_ERR_INVALID, "max_steps < 0");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     int rc;

@@ -16,15 +16,22 @@
  * hype.h:305-306:
  *   - RHS is overwritten for every owned cell; U is not modified;
  *   - Ctx->dt is set to CFL*h/(2*s_max) (rhs_function_prim.c:617-623);
- *   - the scratch of AppCtx (W, localU, u_bnd, F, G, D, E) is not touched:
- *     the kernels need none of it.
+ *   - the scratch of AppCtx (W, u_bnd, F, G, D, E) is not touched: the kernels
+ *     need none of it; with several ranks, localU takes the ghosted state, as in
+ *     rhs_function_prim.c:44-45.
+ * Several MPI ranks (a DMDA split in y only, e.g. -da_processors_x 1): each rank's
+ * GPU solver owns its rows (hype_create_slab); DMGlobalToLocal brings the 3 ghost
+ * rows from the neighbouring ranks, hype_rhs_prim_slab computes the rank's RHS and
+ * dt, and Ctx->dt is the MPI_Allreduce(MIN) of the ranks' dt, as in
+ * rhs_function_prim.c:620-623.
  * Differences:
  *   - an inadmissible face state (the reference prints and calls MPI_Abort,
  *     e.g. kapila_5eqn.c:353-357) prints the same kind of message and returns
  *     a non-zero PetscErrorCode, so TS stops through CHKERRQ instead of the
  *     process ending;
- *   - one MPI rank: the whole grid is on this rank's GPU (the DMDA must not
- *     be split); with more ranks the call returns an error.
+ *   - a DMDA split across x as well returns an error (the slabs are whole rows);
+ *   - a failed RHS on any rank makes every rank return the error (a reduction of
+ *     the status), where the reference's failing rank would MPI_Abort.
  * The GPU solver is created on first use and re-created when the AppCtx
  * parameters change (grid, order, CFL, boundaries).  The device is
  * HYPE_DEVICE from the environment, else 0.
@@ -35,9 +42,11 @@
 #include "hype.h"
 #include "hype_gpu.h"
 
-/* one GPU solver per path: [0] primitive, [1] conservative reconstruction */
+/* one GPU solver per path: [0] primitive, [1] conservative reconstruction; with
+ * several ranks, for this rank's rows row0 .. row0+rows-1 */
 static hype_solver *glue_solver[2] = {NULL, NULL};
 static hype_config glue_cfg[2];
+static int glue_row0[2], glue_rows[2];
 
 static int glue_system(void)
 {
@@ -87,55 +96,88 @@ void RHSFunctionPrimFinalize(void)
     }
 }
 
-static PetscErrorCode glue_rhs(int conservative, PetscReal t, Vec U, Vec RHS, AppCtx *Ctx)
+static PetscErrorCode glue_rhs(int conservative, TS ts, PetscReal t, Vec U, Vec RHS, AppCtx *Ctx)
 {
     int size = 1;
     MPI_Comm_size(PETSC_COMM_WORLD, &size);
-    if (size != 1) {
-        fprintf(stderr, "RHSFunction (GPU): one MPI rank only, got %d\n", size);
-        return 1;
-    }
     hype_config c;
     glue_config(Ctx, conservative, &c);
-    if (!glue_solver[conservative] || memcmp(&c, &glue_cfg[conservative], sizeof(c)) != 0) {
+    int row0 = 0, rows = c.ny, st = HYPE_OK;
+    DM da = NULL;
+    PetscInt gxs = 0, gys = 0, gxm = 0, gym = 0;
+    if (size > 1) {   /* this rank's rows of the DMDA (rhs_function_prim.c:36-53) */
+        PetscInt xs, ys, xm, ym;
+        TSGetDM(ts, &da);
+        DMDAGetCorners(da, &xs, &ys, NULL, &xm, &ym, NULL);
+        DMDAGetGhostCorners(da, &gxs, &gys, NULL, &gxm, &gym, NULL);
+        row0 = (int)ys;
+        rows = (int)ym;
+        if (xs != 0 || xm != c.nx) {
+            fprintf(stderr, "RHSFunction (GPU): the DMDA must be split in y only (-da_processors_x 1)\n");
+            st = HYPE_ERR_INVALID;
+        }
+    }
+    if (st == HYPE_OK && (!glue_solver[conservative] || memcmp(&c, &glue_cfg[conservative], sizeof(c)) != 0 ||
+                          glue_row0[conservative] != row0 || glue_rows[conservative] != rows)) {
         hype_destroy(glue_solver[conservative]);
         glue_solver[conservative] = NULL;
         hype_solver *s = NULL;
-        const int st = hype_create(&c, &s);
+        st = size > 1 ? hype_create_slab(&c, row0, rows, &s) : hype_create(&c, &s);
         if (st != HYPE_OK) {
             fprintf(stderr, "RHSFunction (GPU): %s\n", s ? hype_last_error(s) : hype_status_string(st));
             hype_destroy(s);
-            return (PetscErrorCode)st;
+        } else {
+            glue_solver[conservative] = s;
+            glue_cfg[conservative] = c;
+            glue_row0[conservative] = row0;
+            glue_rows[conservative] = rows;
         }
-        glue_solver[conservative] = s;
-        glue_cfg[conservative] = c;
     }
-    const PetscScalar *u = NULL;
-    PetscScalar *r = NULL;
-    PetscErrorCode ierr = VecGetArrayRead(U, &u);
-    if (ierr) return ierr;
-    ierr = VecGetArray(RHS, &r);
-    if (ierr) { VecRestoreArrayRead(U, &u); return ierr; }
     double dt = 0.0;
-    const int st = hype_rhs_prim(glue_solver[conservative], (double)t, (const double *)u, (double *)r, &dt);
-    VecRestoreArray(RHS, &r);
-    VecRestoreArrayRead(U, &u);
-    if (st != HYPE_OK) {
-        fprintf(stderr, "RHSFunction (GPU): %s\n", hype_last_error(glue_solver[conservative]));
-        return (PetscErrorCode)st;
+    if (st == HYPE_OK) {
+        const PetscScalar *u = NULL;
+        PetscScalar *r = NULL;
+        Vec in = size > 1 ? Ctx->localU : U;
+        PetscErrorCode ierr = 0;
+        if (size > 1) {   /* the neighbours' ghost rows (rhs_function_prim.c:44-45) */
+            ierr = DMGlobalToLocalBegin(da, U, INSERT_VALUES, Ctx->localU);
+            if (!ierr) ierr = DMGlobalToLocalEnd(da, U, INSERT_VALUES, Ctx->localU);
+        }
+        if (!ierr) ierr = VecGetArrayRead(in, &u);
+        if (!ierr && (ierr = VecGetArray(RHS, &r)) != 0) VecRestoreArrayRead(in, &u);
+        if (ierr) return ierr;
+        hype_solver *s = glue_solver[conservative];
+        if (size > 1) {
+            const int nv = hype_nvar(c.system);
+            /* cell (0, row0) of the ghosted local array; its rows are gxm records apart */
+            const double *u0 = (const double *)u + ((size_t)(row0 - gys) * gxm + (size_t)(0 - gxs)) * nv;
+            st = hype_rhs_prim_slab(s, (double)t, u0, (long long)gxm * nv, (double *)r, &dt);
+        } else {
+            st = hype_rhs_prim(s, (double)t, (const double *)u, (double *)r, &dt);
+        }
+        VecRestoreArray(RHS, &r);
+        VecRestoreArrayRead(in, &u);
+        if (st != HYPE_OK) fprintf(stderr, "RHSFunction (GPU): %s\n", hype_last_error(s));
     }
+    if (size > 1) {   /* every rank returns the same status; dt is the minimum over ranks */
+        const PetscReal mine = (PetscReal)st, dt_mine = dt;
+        PetscReal worst = mine, dt_all = dt;
+        MPI_Allreduce(&mine, &worst, 1, MPIU_REAL, MPIU_MAX, PETSC_COMM_WORLD);
+        MPI_Allreduce(&dt_mine, &dt_all, 1, MPIU_REAL, MPIU_MIN, PETSC_COMM_WORLD);
+        st = (int)worst;
+        dt = dt_all;
+    }
+    if (st != HYPE_OK) return (PetscErrorCode)st;
     Ctx->dt = dt;   /* rhs_function_prim.c:623, rhs_function.c:622 */
     return 0;
 }
 
 PetscErrorCode RHSFunctionPrim(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
 {
-    (void)ts;
-    return glue_rhs(0, t, U, RHS, (AppCtx *)ctx);
+    return glue_rhs(0, ts, t, U, RHS, (AppCtx *)ctx);
 }
 
 PetscErrorCode RHSFunction(TS ts, PetscReal t, Vec U, Vec RHS, void *ctx)
 {
-    (void)ts;
-    return glue_rhs(1, t, U, RHS, (AppCtx *)ctx);
+    return glue_rhs(1, ts, t, U, RHS, (AppCtx *)ctx);
 }

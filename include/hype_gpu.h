@@ -132,6 +132,24 @@ HYPE_API int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RH
  * VECCUDA array); the call is synchronous. */
 HYPE_API int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRHS, double *dt);
 
+/* One MPI rank's share of a grid decomposed over ranks in y: HyPE-2D's DMDA
+ * (hype.c:108-122) with one rank across x.  The solver owns global rows
+ * row0 .. row0+rows-1 of the grid `cfg` describes (nx, ny, domain and boundaries of
+ * the whole grid).  A side with a neighbouring rank (row0 > 0, row0+rows < ny, or a
+ * periodic y axis when the slab is not the whole grid) takes its 3 ghost rows from
+ * the caller instead of a boundary condition.  FP64 only. */
+HYPE_API int hype_create_slab(const hype_config *cfg, int row0, int rows, hype_solver **out);
+
+/* RHSFunctionPrim (or RHSFunction) on a slab: rhs_function_prim.c:12-626 for one
+ * rank.  U points at the slab's cell (0, 0) in a host array whose rows are
+ * row_stride doubles apart: nx*nvar for a compact array, or the ghosted width times
+ * nvar for a DMDA local vector after DMGlobalToLocal.  Rows -3..-1 and rows..rows+2
+ * are read on the sides with a neighbour; ghost columns are never read.  RHS
+ * receives the slab's rows, compact.  *dt is this slab's CFL h / (2 s_max); the
+ * caller takes the minimum over ranks, as rhs_function_prim.c:620-623 does with
+ * MPI_Allreduce(MIN). */
+HYPE_API int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_stride, double *RHS, double *dt);
+
 /*
  * RHSFunctionPrim for callers that cannot allocate device memory -- for
  * example a plug-in running inside an application or framework whose memory

@@ -20,14 +20,28 @@ void petsc_mini_set_abort_target(jmp_buf *env) { g_abort_env = env; }
 int  petsc_mini_abort_count(void) { return g_abort_count; }
 void petsc_mini_set_quiet(int quiet) { g_quiet = quiet; }
 
+/* Emulation of one rank of a DMDA split over ranks in y (tests of code written for
+ * several ranks, in one process): DMDAs created while it is on own rows ys..ys+ym-1,
+ * their global vectors hold those rows only, and DMGlobalToLocal takes the other
+ * ranks' rows from `full` (the whole grid's global array).  MPI reports the
+ * emulated rank and size; MPI_Allreduce still returns this rank's own values. */
+static int g_emu_size = 1, g_emu_rank = 0;
+static PetscInt g_emu_ys = 0, g_emu_ym = -1;
+static const PetscScalar *g_emu_full = NULL;
+void petsc_mini_emulate_rank(int rank, int size, PetscInt ys, PetscInt ym, const PetscScalar *full)
+{
+    g_emu_rank = rank; g_emu_size = size; g_emu_ys = ys; g_emu_ym = ym; g_emu_full = full;
+    if (size <= 1) { g_emu_rank = 0; g_emu_size = 1; g_emu_ys = 0; g_emu_ym = -1; g_emu_full = NULL; }
+}
+
 int MPI_Allreduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, MPI_Comm c)
 {
     (void)t; (void)op; (void)c;
     memmove(r, s, (size_t)count * sizeof(double));
     return 0;
 }
-int MPI_Comm_size(MPI_Comm c, int *size) { (void)c; *size = 1; return 0; }
-int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = 0; return 0; }
+int MPI_Comm_size(MPI_Comm c, int *size) { (void)c; *size = g_emu_size; return 0; }
+int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = g_emu_rank; return 0; }
 int MPI_Abort(MPI_Comm c, int code)
 {
     (void)c;
@@ -121,6 +135,7 @@ struct _p_DM {
     PetscInt M, N, dof, s;
     DMBoundaryType bx, by;
     PetscInt xs_g, ys_g, xm_g, ym_g;   /* ghost corners */
+    PetscInt ys, ym;                    /* owned rows (all of them on one rank) */
     DM cda;                             /* coordinate DM (dof 2) */
     Vec coords;
     /* one row-pointer table per array handed out (released on restore) */
@@ -137,7 +152,9 @@ PetscErrorCode DMDACreate2d(MPI_Comm c, DMBoundaryType bx, DMBoundaryType by, DM
     int gx = (bx == DM_BOUNDARY_NONE) ? 0 : s;
     int gy = (by == DM_BOUNDARY_NONE) ? 0 : s;
     d->xs_g = -gx; d->xm_g = M + 2 * gx;
-    d->ys_g = -gy; d->ym_g = N + 2 * gy;
+    d->ys = 0; d->ym = N;
+    if (g_emu_ym >= 0) { d->ys = g_emu_ys; d->ym = g_emu_ym; }
+    d->ys_g = d->ys - gy; d->ym_g = d->ym + 2 * gy;
     *da = d;
     return 0;
 }
@@ -152,7 +169,7 @@ PetscErrorCode DMDestroy(DM *da)
     return 0;
 }
 PetscErrorCode DMView(DM da, PetscViewer v) { (void)da; (void)v; return 0; }
-PetscErrorCode DMCreateGlobalVector(DM da, Vec *v) { *v = vec_new(da->M * da->N * da->dof, da, 0); return 0; }
+PetscErrorCode DMCreateGlobalVector(DM da, Vec *v) { *v = vec_new(da->M * da->ym * da->dof, da, 0); return 0; }
 PetscErrorCode DMCreateLocalVector(DM da, Vec *v) { *v = vec_new(da->xm_g * da->ym_g * da->dof, da, 1); return 0; }
 
 static inline PetscInt wrap(PetscInt i, PetscInt n) { PetscInt r = i % n; return r < 0 ? r + n : r; }
@@ -169,7 +186,11 @@ PetscErrorCode DMGlobalToLocalBegin(DM da, Vec g, InsertMode m, Vec l)
             int iin = (i >= 0 && i < da->M);
             if (!iin && da->bx != DM_BOUNDARY_PERIODIC) continue;   /* no source: keep */
             PetscInt is = iin ? i : wrap(i, da->M);
-            const PetscScalar *src = g->a + ((size_t)js * da->M + is) * dof;
+            /* this rank's rows from its global vector, the other ranks' from the emulation's array */
+            const int own = js >= da->ys && js < da->ys + da->ym;
+            if (!own && !g_emu_full) continue;
+            const PetscScalar *src = own ? g->a + ((size_t)(js - da->ys) * da->M + is) * dof
+                                         : g_emu_full + ((size_t)js * da->M + is) * dof;
             PetscScalar *dst = l->a + ((size_t)(j - da->ys_g) * da->xm_g + (i - da->xs_g)) * dof;
             memcpy(dst, src, (size_t)dof * sizeof(PetscScalar));
         }
@@ -181,10 +202,10 @@ PetscErrorCode DMGlobalToLocalEnd(DM da, Vec g, InsertMode m, Vec l) { (void)da;
 PetscErrorCode DMDAGetCorners(DM da, PetscInt *xs, PetscInt *ys, PetscInt *zs, PetscInt *xm, PetscInt *ym, PetscInt *zm)
 {
     if (xs) *xs = 0;
-    if (ys) *ys = 0;
+    if (ys) *ys = da->ys;
     if (zs) *zs = 0;
     if (xm) *xm = da->M;
-    if (ym) *ym = da->N;
+    if (ym) *ym = da->ym;
     if (zm) *zm = 1;
     return 0;
 }
@@ -205,7 +226,7 @@ PetscErrorCode DMDAVecGetArray(DM da, Vec v, void *array)
 {
     PetscInt xs, ys, xm, ym;
     if (v->local) { xs = da->xs_g; ys = da->ys_g; xm = da->xm_g; ym = da->ym_g; }
-    else { xs = 0; ys = 0; xm = v->dm->M; ym = v->dm->N; }
+    else { xs = 0; ys = v->dm->ys; xm = v->dm->M; ym = v->dm->ym; }
     const PetscInt dof = v->dm->dof;
     char **rows = (char **)malloc((size_t)ym * sizeof(char *));
     for (PetscInt r = 0; r < ym; ++r)
@@ -215,7 +236,7 @@ PetscErrorCode DMDAVecGetArray(DM da, Vec v, void *array)
 }
 PetscErrorCode DMDAVecRestoreArray(DM da, Vec v, void *array)
 {
-    PetscInt ys = v->local ? da->ys_g : 0;
+    PetscInt ys = v->local ? da->ys_g : v->dm->ys;
     char **rows = *(char ***)array;
     if (rows) free(rows + ys);
     *(char ***)array = NULL;

@@ -68,6 +68,9 @@ int MPI_Comm_rank(MPI_Comm c, int *rank);
 /* The reference calls MPI_Abort on an inadmissible face state; the stand-in
  * records the event and long-jumps back to the driver (petsc_mini_set_abort_target). */
 int MPI_Abort(MPI_Comm c, int code);
+/* test hook: emulate rank `rank` of `size` owning rows ys..ys+ym-1 of a y-split DMDA,
+ * the other ranks' rows read from `full`; size <= 1 switches it off */
+void petsc_mini_emulate_rank(int rank, int size, PetscInt ys, PetscInt ym, const PetscScalar *full);
 
 /* ---- objects ------------------------------------------------------------ */
 typedef struct _p_Vec         *Vec;

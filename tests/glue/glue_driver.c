@@ -20,6 +20,10 @@ void RHSFunctionPrimFinalize(void);
 
 int glue_nvar(void) { return nVar; }
 
+/* one rank of a y-split DMDA (petsc_mini's emulation): rank `rank` of `size` owns rows
+ * ys .. ys+ym-1; the other ranks' rows come from `full` (the whole grid's state) */
+void glue_emulate(int rank, int size, int ys, int ym, const double *full) { petsc_mini_emulate_rank(rank, size, ys, ym, full); }
+
 int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int bc[4], const double eos[4], int conservative,
              const double *Uin, double *Rout, double *dt)
 {
@@ -41,9 +45,14 @@ int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int b
     DMSetUp(da);
     DMCreateGlobalVector(da, &U);
     VecDuplicate(U, &R);
+    DMCreateLocalVector(da, &Ctx.localU);   /* hype.c keeps it in AppCtx */
+    /* this rank's rows of the state (all of them on one rank) */
+    PetscInt xs, ys, xm, ym;
+    DMDAGetCorners(da, &xs, &ys, NULL, &xm, &ym, NULL);
+    const size_t row = (size_t)nx * nVar;
     PetscScalar *a;
     VecGetArray(U, &a);
-    memcpy(a, Uin, sizeof(double) * (size_t)nx * ny * nVar);
+    memcpy(a, Uin + (size_t)ys * row, sizeof(double) * row * ym);
     VecRestoreArray(U, &a);
     TS ts;
     TSCreate(PETSC_COMM_WORLD, &ts);
@@ -51,12 +60,13 @@ int glue_rhs(int N, int nx, int ny, const double dom[4], double cfl, const int b
     /* hype.c:341-352: ReconsPrimitive picks the RHS function */
     const PetscErrorCode ierr = Ctx.ReconsPrimitive ? RHSFunctionPrim(ts, 0.0, U, R, &Ctx) : RHSFunction(ts, 0.0, U, R, &Ctx);
     VecGetArray(R, &a);
-    memcpy(Rout, a, sizeof(double) * (size_t)nx * ny * nVar);
+    memcpy(Rout + (size_t)ys * row, a, sizeof(double) * row * ym);
     VecRestoreArray(R, &a);
     *dt = Ctx.dt;
     TSDestroy(&ts);
     VecDestroy(&U);
     VecDestroy(&R);
+    VecDestroy(&Ctx.localU);
     DMDestroy(&da);
     return (int)ierr;
 }

@@ -141,3 +141,60 @@ def test_group_stops_with_the_reference_error(hp):
         assert st2 == hp.ERR_INADMISSIBLE
         assert (k1, t1) == (k2, t2)
         assert grp.last_error() == msg1
+
+
+def test_group_full_size(hp):
+    """1024^2 Kapila as 4 slabs: 10 steps, the single solver's bits."""
+    cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=1024, ny=1024, cfl=0.4, bc_bottom=hp.BC_REFLECTIVE,
+                    bc_top=hp.BC_REFLECTIVE)
+    U = hp.initial_state(cfg, "shock_bubble", seed=4, nbubbles=3)
+    k1, t1, dt1, st1, U1 = lone(hp, cfg, U, 0.0, 1e30, 10)
+    with hp.Group(cfg, 4) as grp:
+        grp.set_state(U)
+        k2, t2, dt2, st2 = grp.solve(0.0, 1e30, 10)
+        U2 = grp.get_state()
+    assert st1 == st2 == hp.OK and (k1, t1, dt1) == (k2, t2, dt2)
+    assert U1.tobytes() == U2.tobytes()
+
+
+@pytest.mark.parametrize("name,nranks", [("kapila_37x23_rough_mixed_bc", 3), ("kapila_24x24_periodic", 2),
+                                         ("bn_13x21_periodic_N1", 4), ("kapila_visc_cons_15x13_N3", 2)])
+def test_rhs_prim_slab_reads_only_rows(name, nranks, hp, orc):
+    """hype_rhs_prim_slab on DMDA-style local arrays: owned rows plus 3 ghost rows
+    from the neighbours, 3 ghost columns each side holding NaN (never read), rows
+    (nx + 6) * nvar apart.  The ranks' rows make the reference's RHS bit for bit."""
+    import ctypes
+    _, cfg, kind, seed = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    Ro, dto, _ = orc.rhs(cfg, U)
+    nv, nx, ny = cfg.nvar, cfg.nx, cfg.ny
+    Ug = U.reshape(ny, nx, nv)
+    L = hp.lib()
+    DP = ctypes.POINTER(ctypes.c_double)
+    L.hype_create_slab.argtypes = [ctypes.POINTER(hp._Cfg), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.hype_rhs_prim_slab.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong, DP, DP]
+    periodic = cfg.bc_bottom == O.PERIODIC
+    rows = [ny // nranks + (1 if r < ny % nranks else 0) for r in range(nranks)]
+    R = np.full_like(U, np.nan)
+    dts = []
+    for r in range(nranks):
+        ys, ym = sum(rows[:r]), rows[r]
+        loc = np.full((ym + 6, nx + 6, nv), np.nan)
+        for j in range(-3, ym + 3):
+            g = ys + j
+            if 0 <= g < ny or periodic:
+                loc[j + 3, 3:nx + 3] = Ug[g % ny]
+        h = ctypes.c_void_p()
+        st = L.hype_create_slab(ctypes.byref(cases.to_pkg(cfg).c_struct()), ys, ym, ctypes.byref(h))
+        assert st == hp.OK, L.hype_last_error(h)
+        Rr = np.empty(ym * nx * nv)
+        dt = ctypes.c_double()
+        base = loc.ctypes.data + ((3 * (nx + 6) + 3) * nv) * 8
+        st = L.hype_rhs_prim_slab(h, 0.0, base, (nx + 6) * nv, Rr.ctypes.data_as(DP), ctypes.byref(dt))
+        L.hype_destroy(h)
+        assert st == hp.OK
+        R[ys * nx * nv:(ys + ym) * nx * nv] = Rr
+        dts.append(dt.value)
+    assert R.tobytes() == Ro.tobytes()
+    if not cfg.viscous:
+        assert min(dts) == dto

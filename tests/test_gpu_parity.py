@@ -298,3 +298,25 @@ def test_advance_host_large_grid_banded(hp):
         R2, dt2, _ = s.rhs_function_prim(0.0, U)
     assert got[:3] == ref[0][:3] and out.tobytes() == ref[1].tobytes()
     assert dt1 == dt2 and R1.tobytes() == R2.tobytes()
+
+
+def test_full_size_conservation_periodic(hp):
+    """The 2048^2 Kapila workload on a periodic grid: 20 steps conserve the partial
+    masses and the energy to 1e-12 relative (rounding only), and alpha_1 stays in
+    [0, 1], the bound the reference's admissibility check enforces
+    (kapila_5eqn.c:474).  Near the shock alpha_1 leaves the initial data's
+    [eps, 1 - eps] (eps = 1e-6) by ~1e-8, as the reference's arithmetic does."""
+    cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=2048, ny=2048, cfl=0.4, bc_left=hp.BC_PERIODIC,
+                    bc_right=hp.BC_PERIODIC, bc_bottom=hp.BC_PERIODIC, bc_top=hp.BC_PERIODIC)
+    U = hp.initial_state(cfg, "shock_bubble", seed=3, nbubbles=4)
+    with hp.Solver(cfg) as s:
+        s.set_state(U)
+        tot0, amin0, amax0 = s.totals()
+        steps, te, dtn, st = s.solve(0.0, 1e30, 20)
+        assert st == hp.OK and steps == 20
+        tot1, amin1, amax1 = s.totals()
+    scale = np.abs(U.reshape(-1, 6)).sum(axis=0)
+    for c in (0, 1, 4):
+        assert abs(tot1[c] - tot0[c]) <= 1e-12 * scale[c], (c, tot0[c], tot1[c])
+    assert 0.0 <= amin1 and amax1 <= 1.0, (amin1, amax1)
+    assert amin1 > 0.5e-6 and amax1 < 1 - 1e-9, (amin1, amax1)   # pure phases stay distinct

@@ -85,3 +85,47 @@ def test_glue_rhs_bitwise_vs_oracle(name, hp, orc, glue_libs):
     assert st == 0
     assert dt == dto
     assert R.tobytes() == Ro.tobytes()
+
+
+def split_rows(ny, n):
+    """PETSc's split of ny rows over n ranks: the first ny % n get one more."""
+    rows = [ny // n + (1 if r < ny % n else 0) for r in range(n)]
+    return [(sum(rows[:r]), rows[r]) for r in range(n)]
+
+
+RANK_CASES = [("kapila_37x23_rough_mixed_bc", 3), ("kapila_24x24_periodic", 4), ("kapila_18x14_inlet", 2),
+              ("kapila_15x13_N3", 2), ("bn_13x21_periodic_N1", 3), ("euler_21x19_reflective_N1", 3),
+              ("kapila_cons_37x23_rough", 3), ("kapila_visc_37x23_rough", 3)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nranks", RANK_CASES)
+def test_glue_ranks_bitwise_vs_oracle(name, nranks, hp, orc, glue_libs):
+    """The glue on a DMDA split in y over several ranks (petsc_mini emulates one rank
+    at a time): each rank's RHS rows equal the reference's bit for bit, and the
+    minimum of the ranks' dt (the glue's MPI_Allreduce) is the reference's dt."""
+    _, cfg, kind, seed = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    Ro, dto, sto = orc.rhs(cfg, U)
+    assert sto == O.OK
+    L = glue_libs[(cfg.system, int(cfg.viscous))]
+    L.glue_emulate.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    row = cfg.nx * cfg.nvar
+    R = np.full_like(U, np.nan)
+    dts = []
+    try:
+        for r, (ys, ym) in enumerate(split_rows(cfg.ny, nranks)):
+            L.glue_emulate(r, nranks, ys, ym, U.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+            Rr, dt, st = glue_rhs(L, cfg, U)
+            assert st == 0, (r, st)
+            R[ys * row:(ys + ym) * row] = Rr[ys * row:(ys + ym) * row]
+            dts.append(dt)
+    finally:
+        L.glue_emulate(0, 1, 0, -1, None)
+    assert R.tobytes() == Ro.tobytes()
+    if cfg.viscous:
+        # rhs_function_prim.c:617-623: each rank's dt has its own s_max and s_max_v, so
+        # the minimum over ranks can exceed the one-rank dt
+        assert min(dts) >= dto
+    else:
+        assert min(dts) == dto
