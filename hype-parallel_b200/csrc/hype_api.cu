@@ -866,43 +866,78 @@ int hype_advance(hype_solver *s, int nsteps)
     return HYPE_OK;
 }
 
-// One step enqueued by hand (the graph's content), with the first stage's
-// bands waiting for their uploaded rows (upload = U_in) and/or the last
-// stage's bands handed to the copy-out stream (U_out).
+// One step enqueued by hand (the graph's content) as a wavefront of row bands:
+// band k of stage s reads the rows of bands k-1..k+1 of stage s-1 (3-row stencils,
+// bands of >= 8 rows; bands 0 and n-1 are neighbours on a periodic y axis) and
+// is launched once those are enqueued, stage 0 once the uploads of those bands are
+// (U_in).  Stage s writes a buffer that only stage s-1 (or, for the combination's
+// second operand, the same band of an earlier stage) still reads, so the same
+// dependency covers every overwrite.  Launches go in one stream: after each
+// band's upload every launch that became ready is enqueued, lowest stage first, so
+// all stages run behind the host->device copy, and the last stage's bands go to
+// the copy-out stream as they finish (U_out).  Results equal the unbanded step's.
 static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_in, double *U_out)
 {
     PlanStage plan[MAX_PLAN];
     int copy_back = 0, rc;
     const int ns = ssp_plan(s->cfg.order, plan, &copy_back);
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
-    CUDA_TRY(s, launch_begin_step(s->dSc, s->stream));
-    for (int st = 0; st < ns; ++st) {
+    const bool py = s->cfg.bc_bottom == HYPE_BC_PERIODIC && b.n > 1;
+    bool done[MAX_PLAN][8] = {};
+    auto nbrs = [&](int k, int *out) -> int {   // bands whose rows band k's stencils read
+        int m = 0;
+        out[m++] = k;
+        if (k > 0) out[m++] = k - 1; else if (py) out[m++] = b.n - 1;
+        if (k + 1 < b.n) out[m++] = k + 1; else if (py) out[m++] = 0;
+        return m;
+    };
+    int uploaded = U_in ? 0 : b.n;
+    auto ready = [&](int st, int k) -> bool {
+        int nb[3];
+        const int m = nbrs(k, nb);
+        for (int j = 0; j < m; ++j)
+            if (st == 0 ? nb[j] >= uploaded : !done[st - 1][nb[j]]) return false;
+        return true;
+    };
+    auto launch = [&](int st, int k) -> int {
         const PlanStage &q = plan[st];
-        const bool first_in = st == 0 && U_in;
-        const bool last_out = st == ns - 1 && U_out;
-        // band k of the last stage is final: bring its rows to the host while later bands compute
-        auto download = [&](int k) -> int {
-            if (!last_out) return HYPE_OK;
+        if (st == 0 && U_in) {
+            int nb[3];
+            const int m = nbrs(k, nb);
+            for (int j = 0; j < m; ++j) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_in[nb[j]], 0));
+        }
+        CUDA_TRY(s, stage_band(s, b, k, q));
+        if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
             const int r0 = b.row[k], nr = b.row[k + 1] - r0;
             CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
             CUDA_TRY(s, launch_planes_to_aos_rows(buf_of(s, q.out), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cout));
             CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
                                         cudaMemcpyDeviceToHost, s->cout));
-            return HYPE_OK;
-        };
-        if (first_in) {
-            if ((rc = banded_upload_stage(s, b, U_in, buf_of(s, q.in), q, 0, nullptr, download))) return rc;
-        } else if (last_out) {
-            for (int k = 0; k < b.n; ++k) {
-                CUDA_TRY(s, stage_band(s, b, k, q));
-                if ((rc = download(k))) return rc;
-            }
-        } else {
-            CUDA_TRY(s, stage(s, buf_of(s, q.in), buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x), buf_of(s, q.out2),
-                              q.reduce));
         }
+        done[st][k] = true;
+        return HYPE_OK;
+    };
+    CUDA_TRY(s, launch_begin_step(s->dSc, s->stream));
+    for (int u = 0;; ++u) {
+        if (U_in && u < b.n) {
+            if ((rc = upload_band(s, b, u, U_in, buf_of(s, plan[0].in)))) return rc;
+            uploaded = u + 1;
+        }
+        for (bool progress = true; progress;) {
+            progress = false;
+            for (int st = 0; st < ns; ++st)
+                for (int k = 0; k < b.n; ++k)
+                    if (!done[st][k] && ready(st, k)) {
+                        if ((rc = launch(st, k))) return rc;
+                        progress = true;
+                    }
+        }
+        if (uploaded >= b.n) break;
     }
+    for (int st = 0; st < ns; ++st)
+        for (int k = 0; k < b.n; ++k)
+            if (!done[st][k]) return fail(s, HYPE_ERR_CUDA, "banded step: stage %d band %d never became ready", st, k);
     CUDA_TRY(s, launch_end_step(s->dSc, s->cfl_h, s->stream));
     return HYPE_OK;
 }

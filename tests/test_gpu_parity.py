@@ -300,6 +300,32 @@ def test_advance_host_large_grid_banded(hp):
     assert dt1 == dt2 and R1.tobytes() == R2.tobytes()
 
 
+@pytest.mark.parametrize("order,periodic,nsteps,flags", [(2, False, 1, 0), (3, False, 1, 0), (1, True, 3, 0), (2, True, 1, 0),
+                                                        (2, False, 2, 4), (2, False, 1, 2)])
+def test_advance_host_wavefront(order, periodic, nsteps, flags, hp):
+    """8 row bands, every stage launched band by band behind the upload and the
+    result downloaded band by band (one-step calls do both): the bits of the
+    unbanded step, for N = 1..3, periodic y, the viscous and the conservative paths."""
+    P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
+    yb = P if periodic else hp.BC_REFLECTIVE
+    c = hp.Config(system=hp.KAPILA_5EQN, order=order, nx=640, ny=720, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=yb, bc_top=yb,
+                  flags=flags, mu1=0.3, mu2=0.05)
+    U = hp.initial_state(c, "shock_bubble", seed=30 + order, nbubbles=2)
+    with hp.Solver(c) as s:
+        s.set_state(U)
+        s.begin(0.0, 1e30, 100)
+        s.advance(nsteps)
+        ref = (s.wait(), s.get_state())
+    out = np.empty_like(U)
+    with hp.Solver(c) as s:
+        assert s.launch_info()["grid"][1] >= 8
+        s.set_state(U)
+        s.begin(0.0, 1e30, 100)
+        got = s.advance_host(U, out, nsteps)
+    assert got[3] == hp.OK and got[:3] == ref[0][:3]
+    assert out.tobytes() == ref[1].tobytes()
+
+
 def test_full_size_conservation_periodic(hp):
     """The 2048^2 Kapila workload on a periodic grid: 20 steps conserve the partial
     masses and the energy to 1e-12 relative (rounding only), and alpha_1 stays in
