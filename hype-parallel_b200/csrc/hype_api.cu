@@ -421,14 +421,19 @@ static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, d
     return HYPE_OK;
 }
 
-// one stage of `q` over band k's runs of the banded decomposition
-static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanStage &q, int out_aos = 0, double *out = nullptr)
+// one stage of `q` over band k's runs of the banded decomposition, on stream `on`
+// (the solver's compute stream by default)
+static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanStage &q, int out_aos = 0, double *out = nullptr,
+                              cudaStream_t on = nullptr)
 {
     const int saved = s->runs;
+    cudaStream_t saved_stream = s->stream;
     s->runs = b.runs;
+    if (on) s->stream = on;
     const cudaError_t e = stage(s, buf_of(s, q.in), out ? out : buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x),
                                 buf_of(s, q.out2), q.reduce, out_aos, b.run[k], b.run[k + 1] - b.run[k]);
     s->runs = saved;
+    s->stream = saved_stream;
     return e;
 }
 
@@ -523,6 +528,8 @@ int hype_destroy(hype_solver *s)
         if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
     }
     if (s->ev_fence) cudaEventDestroy(s->ev_fence);
+    for (cudaEvent_t e : s->ev_sb) if (e) cudaEventDestroy(e);
+    if (s->stream2) { cudaStreamSynchronize(s->stream2); cudaStreamDestroy(s->stream2); }
     if (s->cin) { cudaStreamSynchronize(s->cin); cudaStreamDestroy(s->cin); }
     if (s->cout) { cudaStreamSynchronize(s->cout); cudaStreamDestroy(s->cout); }
     if (s->stream) cudaStreamDestroy(s->stream);
@@ -567,6 +574,8 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
         CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming));
     }
     CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_fence, cudaEventDisableTiming));
+    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : s->ev_sb) CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     double **bufs[] = {&s->dU, &s->dS0, &s->dS1, &s->dS2};
     const long long off = (long long)row_off * s->pitch;   // the buffers point at row 0
     for (double **b : bufs) {
@@ -872,10 +881,13 @@ int hype_advance(hype_solver *s, int nsteps)
 // is launched once those are enqueued, stage 0 once the uploads of those bands are
 // (U_in).  Stage s writes a buffer that only stage s-1 (or, for the combination's
 // second operand, the same band of an earlier stage) still reads, so the same
-// dependency covers every overwrite.  Launches go in one stream: after each
-// band's upload every launch that became ready is enqueued, lowest stage first, so
-// all stages run behind the host->device copy, and the last stage's bands go to
-// the copy-out stream as they finish (U_out).  Results equal the unbanded step's.
+// dependency covers every overwrite.  After each band's upload every launch that
+// became ready is enqueued, lowest stage first, so all stages run behind the
+// host->device copy, and the last stage's bands go to the copy-out stream as they
+// finish (U_out).  Even stages run on the compute stream, odd ones on a second
+// stream, each launch waiting for the events of the bands it reads, so that a
+// band's launch fills the SMs that the tail of another leaves idle.  Results equal
+// the unbanded step's.
 static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_in, double *U_out)
 {
     PlanStage plan[MAX_PLAN];
@@ -901,16 +913,18 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
     };
     auto launch = [&](int st, int k) -> int {
         const PlanStage &q = plan[st];
-        if (st == 0 && U_in) {
-            int nb[3];
-            const int m = nbrs(k, nb);
-            for (int j = 0; j < m; ++j) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_in[nb[j]], 0));
+        cudaStream_t on = (st & 1) ? s->stream2 : s->stream;
+        int nb[3];
+        const int m = nbrs(k, nb);
+        for (int j = 0; j < m; ++j) {
+            if (st == 0 && U_in) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_in[nb[j]], 0));
+            if (st > 0) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_sb[(st - 1) * 8 + nb[j]], 0));
         }
-        CUDA_TRY(s, stage_band(s, b, k, q));
+        CUDA_TRY(s, stage_band(s, b, k, q, 0, nullptr, on));
+        CUDA_TRY(s, cudaEventRecord(s->ev_sb[st * 8 + k], on));
         if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
             const int r0 = b.row[k], nr = b.row[k + 1] - r0;
-            CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
-            CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_sb[st * 8 + k], 0));
             CUDA_TRY(s, launch_planes_to_aos_rows(buf_of(s, q.out), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cout));
             CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
                                         cudaMemcpyDeviceToHost, s->cout));
@@ -919,6 +933,8 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
         return HYPE_OK;
     };
     CUDA_TRY(s, launch_begin_step(s->dSc, s->stream));
+    CUDA_TRY(s, cudaEventRecord(s->ev_fence, s->stream));   // the second stream starts behind begin_step
+    CUDA_TRY(s, cudaStreamWaitEvent(s->stream2, s->ev_fence, 0));
     for (int u = 0;; ++u) {
         if (U_in && u < b.n) {
             if ((rc = upload_band(s, b, u, U_in, buf_of(s, plan[0].in)))) return rc;
@@ -938,6 +954,9 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
     for (int st = 0; st < ns; ++st)
         for (int k = 0; k < b.n; ++k)
             if (!done[st][k]) return fail(s, HYPE_ERR_CUDA, "banded step: stage %d band %d never became ready", st, k);
+    for (int k = 0; k < b.n; ++k)   // end_step and everything after it behind both streams
+        for (int st = ns - 2; st < ns; ++st)
+            if (st >= 0) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_sb[st * 8 + k], 0));
     CUDA_TRY(s, launch_end_step(s->dSc, s->cfl_h, s->stream));
     return HYPE_OK;
 }

@@ -23,6 +23,10 @@ struct hype_solver {
     cudaStream_t cin = nullptr, cout = nullptr;   // host<->device copy streams of the banded calls
     cudaEvent_t ev_in[8] = {}, ev_done[8] = {};   // per row band: uploaded, computed
     cudaEvent_t ev_fence = nullptr;               // the compute stream's work so far
+    // banded steps: odd stages on a second compute stream, band k of stage s marked by
+    // ev_sb[s * 8 + k], so that one band's launch fills the tail of another's
+    cudaStream_t stream2 = nullptr;
+    cudaEvent_t ev_sb[hype::MAX_PLAN * 8] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t step_exec = nullptr;
     int cells = hype::STAGE_CELLS;          // tile width of the stage kernel
