@@ -364,7 +364,28 @@ def group_leg(hp, args, local_rank, U0, U_ref):
             "bitwise_equal_to_single_solver": same}
 
 
-def serve_leg(hp, args, local_rank, capacity):
+def euler_rate(hp, local_rank):
+    """FP64 Euler N = 2 at 1024^2 (four-quadrant state), cell-updates/s: the serving
+    mix's third system."""
+    cfg = hp.Config(system=hp.EULER, order=2, nx=1024, ny=1024, cfl=0.4, device=local_rank, gamma1=1.4, gamma2=1.4, pi1=0.0,
+                    pi2=0.0)
+    with hp.Solver(cfg) as s:
+        s.set_state(hp.initial_state(cfg, "euler_quadrants", seed=SEED))
+        s.begin(0.0, 1e30, 1 << 30)
+        s.advance(3)
+        s.wait()
+        s.advance(20)
+        s.wait()
+        return 1024 * 1024 * 20 / (s.last_elapsed_ms() * 1e-3)
+
+
+def mix_capacity(work_share, rates):
+    """Throughput of a request mix whose systems share the GPU in turn: the
+    work-weighted harmonic mean of the systems' own rates."""
+    return 1.0 / sum(work_share[k] / rates[k] for k in work_share)
+
+
+def serve_leg(hp, args, local_rank, rates):
     """Serving: a Poisson stream of solve requests through the C request loop
     (hype_serve_run) -- 70/20/10 Kapila / Baer-Nunziato / Euler, square grids
     with side log-uniform in 64..2048, runs of 50..2000 steps (log-uniform),
@@ -396,6 +417,13 @@ def serve_leg(hp, args, local_rank, capacity):
     rho = float(rng.uniform(0.5, 0.8))
     if args.serve_load is not None:
         rho = args.serve_load
+    # the load factor is of this mix's own capacity (per-system rates measured in this run)
+    share = {k: 0.0 for k in rates}
+    for r, w in zip(reqs, work):
+        share[{hp.KAPILA_5EQN: "kapila", hp.BAER_NUNZIATO: "bn", hp.EULER: "euler"}[r.cfg.system]] += w
+    total = sum(share.values())
+    share = {k: v / total for k, v in share.items()}
+    capacity = mix_capacity(share, rates)
     rate = rho * capacity / float(np.mean(work))
     t = 0.0
     for r in reqs:
@@ -422,6 +450,8 @@ def serve_leg(hp, args, local_rank, capacity):
     return {"workload": f"Poisson stream of {n} solves: 70/20/10 kapila5/bn/euler, square grids 64..2048 log-uniform, "
                         "50..2000 steps log-uniform, N=2 SSPRK(4,3), 150 GB HBM budget",
             "requests": n, "kapila_precision": args.serve_kapila, "active_cells": args.serve_active_cells,
+            "capacity_estimate": capacity, "capacity_from": {"rates": rates, "work_share": share,
+                                                             "rule": "work-weighted harmonic mean of the systems' rates"},
             "substep_cells": args.serve_substep_cells, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
             "offered_cell_updates": float(np.sum(work)),
             "p50_s": st["p50_s"], "p90_s": st["p90_s"], "p99_s": st["p99_s"], "max_s": st["max_s"], "mean_s": st["mean_s"],
@@ -557,8 +587,17 @@ def run_gpu(args, rank, world, local_rank):
     group = None if args.group_slabs <= 1 else group_leg(hp, args, local_rank, U0, U_fp64)
     bn = None if args.no_bn else bn_leg(hp, args, local_rank)
     batched = None if args.no_batch else batch_leg(hp, args, local_rank)
-    capacity = batched["batched_mixed"]["value"] if batched else 5e8
-    serving = None if args.serve_requests <= 0 else serve_leg(hp, args, local_rank, capacity)
+    serving = None
+    if args.serve_requests > 0:
+        # per-system rates of this run: batched Kapila in the requests' precision, BN in
+        # the fixed flux form, Euler measured here (fallbacks when a leg was skipped)
+        kap = None
+        if batched:
+            kap = batched["batched_mixed" if args.serve_kapila == "mixed" else "batched_fp64"]["value"]
+        rates = {"kapila": kap or (value * (2.0 if args.serve_kapila == "mixed" else 1.0)),
+                 "bn": (bn or {}).get("fixed_p2", {}).get("value") or 0.5 * value,
+                 "euler": euler_rate(hp, local_rank)}
+        serving = serve_leg(hp, args, local_rank, rates)
 
     if rank != 0:
         return 0
