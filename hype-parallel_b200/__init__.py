@@ -361,7 +361,7 @@ class Solver:
 
     def advance_host(self, U_in: np.ndarray, U_out: np.ndarray, nsteps: int = 1):
         """Host state in, nsteps steps, host state out, copies overlapped with
-        the first and last stages (hype_advance_host); returns (steps, t, dt_next, status)."""
+        the first and last steps' stages (hype_advance_host); returns (steps, t, dt_next, status)."""
         for a in (U_in, U_out):
             if a.size != self.n or a.dtype != np.float64 or not a.flags.c_contiguous:
                 raise ValueError("states must be contiguous float64 arrays of the state size")

@@ -360,12 +360,14 @@ static int check_config(const hype_config *c, hype_solver *s)
 // ---------------------------------------------------------------------------
 // Banded host calls.  The stages next to a host copy run on a finer row
 // decomposition (up to 8x the runs, at least 8 rows each) grouped into up to
-// 8 bands of rows, launched one band after the other so that each band fills
-// the GPU and finishes early: the host->device copy of later bands overlaps
-// the first stage on earlier ones (band k's stencils read rows of bands
-// k-1..k+1), and the device->host copy of a band overlaps the last stage on
-// the bands after it.  Copies go on their own streams (cin, cout), ordered to
-// the compute stream by events.  Results do not depend on the decomposition.
+// 8 bands of rows, launched band by band so that each band fills the GPU and
+// finishes early: the host->device copy of later bands overlaps the launches on
+// earlier ones (band k's stencils read rows of bands k-1..k+1), and the
+// device->host copy of a band overlaps the launches on the bands after it
+// (hype_rhs_prim: its one RHS launch; hype_advance_host: every stage of the
+// step, enqueue_step_banded).  Copies go on their own streams (cin, cout),
+// ordered to the compute streams by events.  Results do not depend on the
+// decomposition.
 // ---------------------------------------------------------------------------
 struct Bands {
     int n;

@@ -236,8 +236,9 @@ HYPE_API int hype_wait(hype_solver *s, int *steps_done, double *t_end, double *d
  * Host state in, n steps, host state out: hype_set_state(U_in) +
  * hype_advance(nsteps) + hype_wait + hype_get_state(U_out), with the copies
  * overlapped by the computation -- the rows of U_in stream in while the first
- * stage runs on the rows already there, and the rows of U_out stream out
- * while the last stage finishes the rows after them.  Needs hype_begin.  U_in
+ * step's stages run, band of rows by band of rows, on the rows already there,
+ * and the rows of U_out stream out while the last step finishes the rows after
+ * them.  Needs hype_begin.  U_in
  * and U_out may be the same array; pinned (page-locked) host memory gives the
  * overlap its full effect.  Returns what hype_wait returns.
  */

@@ -259,7 +259,7 @@ def test_autotuned_tiles_give_identical_bits(hp, orc):
                                          ("kapila_16x16_solve_N3", 2), ("kapila_24x20_bubble_solve_N1", 2),
                                          ("bn_20x20_solve", 1), ("euler_32x24_solve", 4), ("kapila_cons_32x32_solve", 2)])
 def test_advance_host_equals_set_advance_get(name, nsteps, hp):
-    """hype_advance_host (copies overlapped with the first and last stages) gives
+    """hype_advance_host (copies overlapped with the stages of the first and last steps) gives
     the bits of set_state + advance + wait + get_state."""
     (_, cfg, kind, seed), t0, tf, nmax = cases.case_by_name(name)
     U = cases.state(cfg, kind, seed)
