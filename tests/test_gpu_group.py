@@ -198,3 +198,39 @@ def test_rhs_prim_slab_reads_only_rows(name, nranks, hp, orc):
     assert R.tobytes() == Ro.tobytes()
     if not cfg.viscous:
         assert min(dts) == dto
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_group_random_configurations(seed, hp):
+    """Random grids, slab counts (1 .. ny/3), orders, systems, paths and boundaries:
+    the group's t, steps, dt and state equal the single solver's, bit for bit (or
+    both stop with the same error at the same step)."""
+    rng = np.random.default_rng(500 + seed)
+    for _ in range(4):
+        system = int(rng.choice([O.EULER, O.KAPILA, O.BN]))
+        order = int(rng.integers(0, 4))
+        nx, ny = int(rng.integers(6, 90)), int(rng.integers(6, 60))
+        bcs = [int(b) for b in rng.choice([T, R], 4)]
+        if rng.uniform() < 0.4:
+            bcs[2] = bcs[3] = P
+        if rng.uniform() < 0.3:
+            bcs[0] = bcs[1] = P
+        kw = dict(conservative=int(rng.uniform() < 0.3))
+        if system == O.KAPILA and order >= 1 and rng.uniform() < 0.3:
+            kw.update(viscous=1, mu1=float(rng.uniform(0, 0.5)), mu2=float(rng.uniform(0, 0.1)))
+        if system == O.BN:
+            kw["fixed"] = 1
+        mk = {O.EULER: cases._e, O.KAPILA: cases._k, O.BN: cases._b}[system]
+        _, cfg, kind, sd = mk("random", nx, ny, order=order, bcs=bcs, seed=int(rng.integers(1 << 20)), **kw)
+        U = cases.state(cfg, kind, sd)
+        pcfg = cases.to_pkg(cfg)
+        nslabs = int(rng.integers(1, ny // 3 + 1))
+        tf = 0.01 if system == O.EULER else 1.0
+        k1, t1, dt1, st1, U1 = lone(hp, pcfg, U, 0.0, tf, 6)
+        with hp.Group(pcfg, nslabs) as grp:
+            grp.set_state(U)
+            k2, t2, dt2, st2 = grp.solve(0.0, tf, 6)
+            U2 = grp.get_state()
+        what = (system, order, nx, ny, bcs, kw, nslabs)
+        assert (st1, k1, t1, dt1) == (st2, k2, t2, dt2), what
+        assert U1.tobytes() == U2.tobytes(), what
