@@ -161,13 +161,16 @@ static StageParams base_params(const hype_solver *s)
 // resident blocks each), at least 8 rows per run.  Rebuilds the TMA
 // descriptors, whose box width follows the tile width, and drops the captured
 // step graph (recaptured on the next hype_begin / hype_advance).
-// FP32 (4 planes) and FP64 (2 planes) maps of a mixed state, box (cells + 8, 1, planes)
+// FP32 (4 planes) and FP64 (2 planes) maps of a mixed state, box (cells + 8, 1, planes);
+// a slab's maps also cover its halo rows and start row_off rows below row 0
 static int make_mixed_maps(hype_solver *s, MixedMaps *mm, float *pf, double *pd)
 {
     const int bw = mixed_box_width(s->cells);
-    CUresult r = encode_planes_map(&mm->f, pf, true, s->cfg.nx, s->cfg.ny, 4, s->pitch, s->plane, bw);
+    const long long off = (long long)s->row_off * s->pitch;
+    const int rows = s->cfg.ny + 2 * s->row_off;
+    CUresult r = encode_planes_map(&mm->f, pf - off, true, s->cfg.nx, rows, 4, s->pitch, s->plane, bw);
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP32 planes) failed (%d)", (int)r);
-    r = encode_planes_map(&mm->d, pd, false, s->cfg.nx, s->cfg.ny, 2, s->pitch, s->plane, bw);
+    r = encode_planes_map(&mm->d, pd - off, false, s->cfg.nx, rows, 2, s->pitch, s->plane, bw);
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP64 planes) failed (%d)", (int)r);
     return HYPE_OK;
 }
@@ -248,7 +251,7 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
 // mixed-precision stage: input state k_in, output k_out (or the interleaved
 // FP64 RHS for OUT_RHS), second state k_x
 static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double ka, double kb, double kc, int k_x, int reduce,
-                           double *out_rhs = nullptr)
+                           double *out_rhs = nullptr, bool push = false)
 {
     MixedParams p;
     std::memset(&p, 0, sizeof(p));
@@ -263,6 +266,13 @@ static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double
     p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc;
     p.sc = s->dSc; p.reduce_smax = reduce;
     p.strips = s->strips; p.runs = s->runs;
+    p.row_off = s->row_off;
+    if (push && k_out >= 0 && mode != OUT_RHS) {   // a slab's state output: edge rows to the neighbours' halos
+        p.push_lo_f = s->nbf_lo[k_out]; p.push_lo_d = s->nbd_lo[k_out];
+        p.push_hi_f = s->nbf_hi[k_out]; p.push_hi_d = s->nbd_hi[k_out];
+        p.push_plane_lo = s->nb_plane_lo; p.push_shift_lo = s->nb_shift_lo;
+        p.push_plane_hi = s->nb_plane_hi; p.push_shift_hi = s->nb_shift_hi;
+    }
     return launch_mixed(s->cells, s->mm[k_in], p, s->stream);
 }
 
@@ -282,12 +292,17 @@ double *hype::solver_alloc_base(const hype_solver *s, double *buf) { return buf 
 
 cudaError_t hype::solver_stage(hype_solver *s, const PlanStage &q)
 {
+    if (s->mixed) return stage_m(s, q.in, q.out, q.mode, q.ka, q.kb, q.kc, q.x, q.reduce, nullptr, true);
     return stage(s, buf_of(s, q.in), buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x), buf_of(s, q.out2), q.reduce, 0, 0, 0,
                  q.out);
 }
 
 // hype.c:343's seeding RHS of u: S1 takes the (unused) RHS planes
-cudaError_t hype::solver_seed_rhs(hype_solver *s) { return stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1); }
+cudaError_t hype::solver_seed_rhs(hype_solver *s)
+{
+    if (s->mixed) return stage_m(s, 0, -1, OUT_RHS, 0, 1.0, 0, -1, 1, s->dAosOut);
+    return stage(s, s->dU, s->dS1, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1);
+}
 
 // One SSP-RK step on the device state: the stage list of ssp_plan between the
 // step-control kernels.  The mixed state has the same buffer roles (U, S0, S1).
@@ -520,7 +535,8 @@ int hype_destroy(hype_solver *s)
     double *bufs[] = {solver_alloc_base(s, s->dU), solver_alloc_base(s, s->dS0), solver_alloc_base(s, s->dS1),
                       solver_alloc_base(s, s->dS2), s->dAosIn, s->dAosOut, s->dInlet, s->dRed};
     for (double *b : bufs) if (b) cudaFree(b);
-    for (int k = 0; k < 3; ++k) { if (s->mf[k]) cudaFree(s->mf[k]); if (s->md[k]) cudaFree(s->md[k]); }
+    const long long moff = (long long)s->row_off * s->pitch;
+    for (int k = 0; k < 3; ++k) { if (s->mf[k]) cudaFree(s->mf[k] - moff); if (s->md[k]) cudaFree(s->md[k] - moff); }
     if (s->dSc) cudaFree(s->dSc);
     if (s->hSc) cudaFreeHost(s->hSc);
     if (s->ev0) cudaEventDestroy(s->ev0);
@@ -593,6 +609,8 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
                 return fail(s, HYPE_ERR_NOMEM, "cudaMalloc of the mixed state failed");
             CUDA_TRY(s, cudaMemset(s->mf[k], 0, sizeof(float) * 4 * (size_t)s->plane));
             CUDA_TRY(s, cudaMemset(s->md[k], 0, sizeof(double) * 2 * (size_t)s->plane));
+            s->mf[k] += off;   // row 0 of the slab
+            s->md[k] += off;
         }
     }
     if (cudaMalloc(&s->dAosIn, aos_bytes) != cudaSuccess || cudaMalloc(&s->dAosOut, aos_bytes) != cudaSuccess)
@@ -623,7 +641,6 @@ int hype::create_slab(const hype_config *global, int row0, int rows, bool halo_l
     *out = s;
     int rc = check_config(global, s);
     if (rc) return rc;
-    if (global->precision != HYPE_PREC_FP64) return fail(s, HYPE_ERR_INVALID, "y-slabs are implemented for the FP64 kernels");
     if (rows < 3 || row0 < 0 || row0 + rows > global->ny) return fail(s, HYPE_ERR_INVALID, "bad slab rows %d..%d", row0, row0 + rows - 1);
     hype_config c = *global;
     c.ny = rows;
@@ -784,11 +801,19 @@ int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_
     CUDA_TRY(s, cudaMemcpy2DAsync(s->dAosIn + (size_t)(3 - lo) * nx * s->nv, row_bytes, U - (long long)lo * row_stride,
                                   sizeof(double) * (size_t)row_stride, row_bytes, (size_t)(rows + lo + hi), cudaMemcpyHostToDevice,
                                   s->stream));
-    CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dS0), nx, 3 - lo, rows + lo + hi, s->nv, s->pitch,
-                                          s->plane, s->stream));
     int rc;
-    if ((rc = reset_scalars(s))) return rc;
-    CUDA_TRY(s, stage(s, s->dS0, s->dAosOut, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
+    if (s->mixed) {   // rows -lo .. rows+hi-1 into the mixed state S0 (FP32 and FP64 planes)
+        const size_t row_elems = (size_t)nx * s->nv;
+        CUDA_TRY(s, launch_aos_to_mixed(s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[1] - (long long)lo * s->pitch,
+                                        s->md[1] - (long long)lo * s->pitch, nx, rows + lo + hi, s->pitch, s->plane, s->stream));
+        if ((rc = reset_scalars(s))) return rc;
+        CUDA_TRY(s, stage_m(s, 1, -1, OUT_RHS, 0, 1.0, 0, -1, 1, s->dAosOut));
+    } else {
+        CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dS0), nx, 3 - lo, rows + lo + hi, s->nv, s->pitch,
+                                              s->plane, s->stream));
+        if ((rc = reset_scalars(s))) return rc;
+        CUDA_TRY(s, stage(s, s->dS0, s->dAosOut, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
+    }
     CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, row_bytes * rows, cudaMemcpyDeviceToHost, s->stream));
     if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
     if (dt) *dt = host_dt(s);
@@ -1069,8 +1094,11 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
         return stage(s, s->dS0, s->dS1, OUT_AXPY, 0, 2.0, 0, nullptr, nullptr, 1);
     };
     if (s->mixed) {
-        CUDA_TRY(s, cudaMemcpyAsync(s->mf[1], s->mf[0], sizeof(float) * 4 * (size_t)s->plane, cudaMemcpyDeviceToDevice, s->stream));
-        CUDA_TRY(s, cudaMemcpyAsync(s->md[1], s->md[0], sizeof(double) * 2 * (size_t)s->plane, cudaMemcpyDeviceToDevice, s->stream));
+        const long long moff = (long long)s->row_off * s->pitch;   // whole planes, halo rows included
+        CUDA_TRY(s, cudaMemcpyAsync(s->mf[1] - moff, s->mf[0] - moff, sizeof(float) * 4 * (size_t)s->plane, cudaMemcpyDeviceToDevice,
+                                    s->stream));
+        CUDA_TRY(s, cudaMemcpyAsync(s->md[1] - moff, s->md[0] - moff, sizeof(double) * 2 * (size_t)s->plane, cudaMemcpyDeviceToDevice,
+                                    s->stream));
     } else {
         CUDA_TRY(s, cudaMemcpyAsync(solver_alloc_base(s, s->dS0), solver_alloc_base(s, s->dU), sizeof(double) * (size_t)s->plane * s->nv,
                                     cudaMemcpyDeviceToDevice, s->stream));

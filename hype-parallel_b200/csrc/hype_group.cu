@@ -215,7 +215,6 @@ int hype_group_create(const hype_config *cfg, int nslabs, const int *devices, hy
     int rc = validate_config(cfg, g->err, sizeof(g->err));
     if (rc) return rc;
     g->cfg = *cfg;
-    if (cfg->precision != HYPE_PREC_FP64) return gfail(g, HYPE_ERR_INVALID, "y-slabs are implemented for the FP64 kernels");
     if (nslabs < 1 || nslabs > MAX_SLABS || nslabs > cfg->ny / 3)
         return gfail(g, HYPE_ERR_INVALID, "nslabs must be 1..min(%d, ny/3 = %d) (got %d)", MAX_SLABS, cfg->ny / 3, nslabs);
     int ndev = 0;
@@ -266,6 +265,10 @@ int hype_group_create(const hype_config *cfg, int nslabs, const int *devices, hy
         for (int role = B_U; role <= B_S2; ++role) {
             if (lo >= 0 && nslabs > 1) s->nb_lo[role] = solver_buf(g->slab[lo], role);
             if (hi >= 0 && nslabs > 1) s->nb_hi[role] = solver_buf(g->slab[hi], role);
+        }
+        for (int k3 = 0; k3 < 3 && s->mixed && nslabs > 1; ++k3) {   // mixed states U, S0, S1
+            if (lo >= 0) { s->nbf_lo[k3] = g->slab[lo]->mf[k3]; s->nbd_lo[k3] = g->slab[lo]->md[k3]; }
+            if (hi >= 0) { s->nbf_hi[k3] = g->slab[hi]->mf[k3]; s->nbd_hi[k3] = g->slab[hi]->md[k3]; }
         }
         if (lo >= 0) { s->nb_plane_lo = g->slab[lo]->plane; s->nb_shift_lo = g->rows[lo]; }
         if (hi >= 0) { s->nb_plane_hi = g->slab[hi]->plane; s->nb_shift_hi = -g->rows[k]; }
@@ -330,8 +333,12 @@ int hype_group_set_state(hype_group *g, const double *U)
                                      cudaMemcpyHostToDevice, s->stream));
             r += len;
         }
-        G_TRY(g, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dU), nx, 3 - lo, g->rows[k] + lo + hi, nv, s->pitch, s->plane,
-                                           s->stream));
+        if (s->mixed)
+            G_TRY(g, launch_aos_to_mixed(s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[0] - (long long)lo * s->pitch,
+                                         s->md[0] - (long long)lo * s->pitch, nx, g->rows[k] + lo + hi, s->pitch, s->plane, s->stream));
+        else
+            G_TRY(g, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dU), nx, 3 - lo, g->rows[k] + lo + hi, nv, s->pitch,
+                                               s->plane, s->stream));
     }
     return sync_all(g);
 }
@@ -345,7 +352,8 @@ int hype_group_get_state(hype_group *g, double *U)
     for (int k = 0; k < g->n; ++k) {
         hype_solver *s = g->slab[k];
         G_TRY(g, cudaSetDevice(g->dev[k]));
-        G_TRY(g, launch_planes_to_aos(s->dU, s->dAosOut, nx, g->rows[k], nv, s->pitch, s->plane, s->stream));
+        if (s->mixed) G_TRY(g, launch_mixed_to_aos(s->mf[0], s->md[0], s->dAosOut, nx, g->rows[k], s->pitch, s->plane, s->stream));
+        else G_TRY(g, launch_planes_to_aos(s->dU, s->dAosOut, nx, g->rows[k], nv, s->pitch, s->plane, s->stream));
         G_TRY(g, cudaMemcpyAsync(U + (size_t)g->row0[k] * row_elems, s->dAosOut, sizeof(double) * row_elems * g->rows[k],
                                  cudaMemcpyDeviceToHost, s->stream));
     }

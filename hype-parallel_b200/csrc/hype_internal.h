@@ -159,6 +159,13 @@ struct MixedParams {
     DevScalars *sc;
     int reduce_smax;
     int strips, runs;
+    // y-slab of a decomposed grid, as StageParams: row_off halo rows below and above in
+    // every plane; state rows 0..2 and ny-3..ny-1 also go to the neighbours' halo rows
+    int row_off;
+    int push_shift_lo, push_shift_hi;
+    long long push_plane_lo, push_plane_hi;
+    float *push_lo_f, *push_hi_f;
+    double *push_lo_d, *push_hi_d;
 };
 struct MixedMaps {
     CUtensorMap f;              // FP32 planes: (nx, ny, 4), box (cells + 8, 1, 4)

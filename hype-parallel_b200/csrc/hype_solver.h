@@ -45,6 +45,8 @@ struct hype_solver {
     int row_off = 0;
     int row0 = 0;                     // first global row of the slab
     double *nb_lo[4] = {}, *nb_hi[4] = {};
+    float *nbf_lo[3] = {}, *nbf_hi[3] = {};      // the same for a mixed state: FP32 and FP64 planes
+    double *nbd_lo[3] = {}, *nbd_hi[3] = {};
     long long nb_plane_lo = 0, nb_plane_hi = 0;
     int nb_shift_lo = 0, nb_shift_hi = 0;
     bool began = false;

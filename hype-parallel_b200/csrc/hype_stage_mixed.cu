@@ -263,8 +263,8 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::F_ROW_BYTES + K::D_ROW_BYTES);
-                tma_load_3d(rowf(row), &maps->f, xs, src, 0, bar);
-                tma_load_3d(rowd(row), &maps->d, xs, src, 0, bar);
+                tma_load_3d(rowf(row), &maps->f, xs, src + p.row_off, 0, bar);   // the maps start row_off rows below row 0
+                tma_load_3d(rowd(row), &maps->d, xs, src + p.row_off, 0, bar);
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {
@@ -295,10 +295,10 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                         for (int c = 0; c < 4; ++c) q[c] = rf[c * BW + (gm - xs)];
                         E = rd[gm - xs]; a1 = rd[BW + (gm - xs)];
                     } else {
-                        const size_t gi = (size_t)src * p.pitch + gm;
+                        const long long gi = (long long)src * p.pitch + gm;
 #pragma unroll
-                        for (int c = 0; c < 4; ++c) q[c] = p.in_f[(size_t)c * p.plane + gi];
-                        E = p.in_d[gi]; a1 = p.in_d[(size_t)p.plane + gi];
+                        for (int c = 0; c < 4; ++c) q[c] = p.in_f[(long long)c * p.plane + gi];
+                        E = p.in_d[gi]; a1 = p.in_d[p.plane + gi];
                     }
                 }
                 __syncthreads();
@@ -468,6 +468,17 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                         }
                         if (c < 4) p.out_f[(size_t)c * p.plane + gidx] = (float)o;
                         else p.out_d[(size_t)(c - 4) * p.plane + gidx] = o;
+                        // a y-slab's edge rows are the neighbours' halo rows: store them there too
+                        if (p.push_lo_f && jo < 3) {
+                            const long long at = (long long)(jo + p.push_shift_lo) * p.pitch + i;
+                            if (c < 4) p.push_lo_f[c * p.push_plane_lo + at] = (float)o;
+                            else p.push_lo_d[(c - 4) * p.push_plane_lo + at] = o;
+                        }
+                        if (p.push_hi_f && jo >= p.ny - 3) {
+                            const long long at = (long long)(jo + p.push_shift_hi) * p.pitch + i;
+                            if (c < 4) p.push_hi_f[c * p.push_plane_hi + at] = (float)o;
+                            else p.push_hi_d[(c - 4) * p.push_plane_hi + at] = o;
+                        }
                     }
                 }
 #pragma unroll

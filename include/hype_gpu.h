@@ -137,7 +137,7 @@ HYPE_API int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, do
  * row0 .. row0+rows-1 of the grid `cfg` describes (nx, ny, domain and boundaries of
  * the whole grid).  A side with a neighbouring rank (row0 > 0, row0+rows < ny, or a
  * periodic y axis when the slab is not the whole grid) takes its 3 ghost rows from
- * the caller instead of a boundary condition.  FP64 only. */
+ * the caller instead of a boundary condition.  FP64 or mixed precision. */
 HYPE_API int hype_create_slab(const hype_config *cfg, int row0, int rows, hype_solver **out);
 
 /* RHSFunctionPrim (or RHSFunction) on a slab: rhs_function_prim.c:12-626 for one

@@ -17,7 +17,9 @@
  * exchange.  After each step's last stage, one kernel takes the maximum wave
  * speed over all slabs and gives every slab the same dt.  The result equals a
  * single solver's on the same grid bit for bit: t, the step count and the state.
- * FP64 only: the primitive, conservative and viscous paths, N = 0..3.
+ * Every form of the single solver: FP64 (primitive, conservative and viscous
+ * paths, N = 0..3) and mixed precision, whose stage kernel stores the edge rows
+ * into the neighbours' FP32 and FP64 planes the same way.
  *
  * Calls return HYPE_OK or an HYPE_ERR_* code of hype_gpu.h, with the message in
  * hype_group_last_error.

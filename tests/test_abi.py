@@ -95,11 +95,11 @@ def test_valid_config_without_gpu_reports_no_device(hp):
 @pytest.mark.parametrize("change,nslabs,needle", [
     (dict(), 0, "nslabs"),
     (dict(ny=12), 5, "ny/3"),
-    (dict(precision=1, order=2), 2, "FP64"),
+    (dict(precision=1, order=1), 2, "N = 2"),
     (dict(nx=2), 1, "3x3"),
 ])
 def test_group_rejects_before_device(hp, change, nslabs, needle):
-    """y-slab groups: 1..ny/3 slabs of an FP64 configuration, checked before any device call."""
+    """y-slab groups: 1..ny/3 slabs of a valid configuration, checked before any device call."""
     cfg = hp.Config(nx=16, ny=16)
     for k, v in change.items():
         setattr(cfg, k, v)

@@ -234,3 +234,55 @@ def test_group_random_configurations(seed, hp):
         what = (system, order, nx, ny, bcs, kw, nslabs)
         assert (st1, k1, t1, dt1) == (st2, k2, t2, dt2), what
         assert U1.tobytes() == U2.tobytes(), what
+
+
+@pytest.mark.parametrize("bcy,nslabs,seed", [(R, 3, 0), (P, 4, 1), (T, 2, 2)])
+def test_group_mixed_precision(bcy, nslabs, seed, hp):
+    """The mixed-precision form as y-slabs: the stage kernel stores its edge rows
+    into the neighbours' FP32 and FP64 halo planes; every bit equals the single
+    mixed-precision solver's (the mixed kernel's per-cell arithmetic does not
+    depend on the tiling either)."""
+    cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=96, ny=70, cfl=0.4, precision=hp.PREC_MIXED, bc_bottom=bcy, bc_top=bcy)
+    U = hp.initial_state(cfg, "shock_bubble", seed=90 + seed, nbubbles=2)
+    k1, t1, dt1, st1, U1 = lone(hp, cfg, U, 0.0, 1e30, 12)
+    with hp.Group(cfg, nslabs) as grp:
+        grp.set_state(U)
+        k2, t2, dt2, st2 = grp.solve(0.0, 1e30, 12)
+        U2 = grp.get_state()
+    assert st1 == st2 == hp.OK and (k1, t1, dt1) == (k2, t2, dt2)
+    assert U1.tobytes() == U2.tobytes()
+
+
+def test_rhs_prim_slab_mixed_precision(hp):
+    """hype_rhs_prim_slab on a mixed-precision configuration: the ranks' rows make
+    the single mixed solver's RHS bit for bit, and the least of their dt is its dt."""
+    import ctypes
+    cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=80, ny=45, cfl=0.4, precision=hp.PREC_MIXED, bc_bottom=P, bc_top=P)
+    U = hp.initial_state(cfg, "shock_bubble", seed=95, nbubbles=3)
+    with hp.Solver(cfg) as s:
+        Rf, dtf, st = s.rhs_function_prim(0.0, U)
+    assert st == hp.OK
+    nv, nx, ny = 6, cfg.nx, cfg.ny
+    Ug = U.reshape(ny, nx, nv)
+    L = hp.lib()
+    DP = ctypes.POINTER(ctypes.c_double)
+    L.hype_create_slab.argtypes = [ctypes.POINTER(hp._Cfg), ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+    L.hype_rhs_prim_slab.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong, DP, DP]
+    R = np.full_like(U, np.nan)
+    dts = []
+    for ys, ym in ((0, 15), (15, 15), (30, 15)):
+        loc = np.full((ym + 6, nx + 6, nv), np.nan)
+        for j in range(-3, ym + 3):
+            loc[j + 3, 3:nx + 3] = Ug[(ys + j) % ny]
+        h = ctypes.c_void_p()
+        assert L.hype_create_slab(ctypes.byref(cfg.c_struct()), ys, ym, ctypes.byref(h)) == hp.OK
+        Rr = np.empty(ym * nx * nv)
+        dt = ctypes.c_double()
+        st = L.hype_rhs_prim_slab(h, 0.0, loc.ctypes.data + ((3 * (nx + 6) + 3) * nv) * 8, (nx + 6) * nv, Rr.ctypes.data_as(DP),
+                                  ctypes.byref(dt))
+        L.hype_destroy(h)
+        assert st == hp.OK
+        R[ys * nx * nv:(ys + ym) * nx * nv] = Rr
+        dts.append(dt.value)
+    assert R.tobytes() == Rf.tobytes()
+    assert min(dts) == dtf
