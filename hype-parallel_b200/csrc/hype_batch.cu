@@ -29,12 +29,31 @@ using namespace hype;
 
 namespace {
 
-constexpr int NKIND = 13;              // FP64: 3 systems x 4 orders; 12 = mixed Kapila N = 2
+// kinds: FP64 primitive path 0..11 (3 systems x 4 orders), 12 = mixed Kapila N = 2,
+// conservative path 13..24 (3 systems x 4 orders), viscous Kapila N = 1..3: primitive
+// 25..27, conservative 28..30
+constexpr int NKIND = 31;
 constexpr int KIND_MIXED = 12;
+constexpr int KIND_CONS0 = 13, KIND_VISC0 = 25, KIND_VISC_CONS0 = 28;
 constexpr int NBUF = 4;                // U, S0, S1, S2
 constexpr int MAX_SUBSTEPS = 16;       // steps an instance may take per batch step
 
-int kind_of(const hype_config &c) { return c.precision == HYPE_PREC_MIXED ? KIND_MIXED : c.system * 4 + c.order; }
+int kind_of(const hype_config &c)
+{
+    if (c.precision == HYPE_PREC_MIXED) return KIND_MIXED;
+    const bool cons = (c.flags & HYPE_FLAG_CONSERVATIVE) != 0;
+    if (c.flags & HYPE_FLAG_VISCOUS) return (cons ? KIND_VISC_CONS0 : KIND_VISC0) + c.order - 1;
+    return (cons ? KIND_CONS0 : 0) + c.system * 4 + c.order;
+}
+
+// the persistent kernel family of a kind: -1 the primitive path's, else BATCH_PATH_*
+int path_of_kind(int id)
+{
+    if (id >= KIND_VISC_CONS0) return BATCH_PATH_VISC_CONS;
+    if (id >= KIND_VISC0) return BATCH_PATH_VISC;
+    if (id >= KIND_CONS0) return BATCH_PATH_CONS;
+    return -1;
+}
 
 struct Inst {
     bool used = false;
@@ -64,6 +83,7 @@ struct SubList {
 struct Kind {
     int system = 0, order = 0;
     bool mixed = false;
+    int path = -1;                     // BATCH_PATH_* for the conservative and viscous kinds (128-column tiles)
     bool ready = false;
     int nstage = 0, copy_back = 0;
     PlanStage plan[MAX_PLAN];
@@ -160,6 +180,7 @@ static size_t state_bytes(const hype_config &c)
 // ---------------------------------------------------------------------------
 static int kind_blocks_per_sm(const Kind &k, int cells)
 {
+    if (k.path >= 0) return cells == STAGE_CELLS ? path_batch_blocks_per_sm(k.path, k.system, k.order) : 0;
     return k.mixed ? mixed_batch_blocks_per_sm(cells) : stage_batch_blocks_per_sm(k.system, k.order, cells);
 }
 
@@ -182,7 +203,11 @@ static int kind_init(hype_batch *b, int id, const hype_config &c)
     k.system = c.system;
     k.order = c.order;
     k.mixed = id == KIND_MIXED;
+    k.path = path_of_kind(id);
     k.nstage = ssp_plan(c.order, k.plan, &k.copy_back);
+    // the grid form of a path kind's kernel seeds each instance's dt
+    if (k.path == BATCH_PATH_CONS) BCUDA(b, stage_cons_configure(c.system, c.order));
+    else if (k.path >= 0) BCUDA(b, stage_visc_configure(c.order, k.path == BATCH_PATH_VISC_CONS));
     k.cells = k.mixed ? MIXED_CELLS : STAGE_CELLS;
     k.rows = 64;
     k.bps = kind_blocks_per_sm(k, k.cells);
@@ -238,6 +263,7 @@ static StageParams inst_params(hype_batch *b, const Inst &in, const PlanStage &q
     p.out2 = q.out2 >= 0 ? in.buf[q.out2] : nullptr;
     p.mode = q.mode; p.ka = q.ka; p.kb = q.kb; p.kc = q.kc;
     p.reduce_smax = q.reduce;
+    p.mu1 = c.mu1; p.mu2 = c.mu2;
     return p;
 }
 
@@ -385,6 +411,7 @@ static int kind_set_tiling(hype_batch *b, int id, int cells, int rows)
 {
     Kind &k = b->kinds[id];
     if (!k.ready) return HYPE_OK;
+    if (k.path >= 0) cells = STAGE_CELLS;   // the conservative and viscous kernels come in 128-column tiles
     const int bps = kind_blocks_per_sm(k, cells);
     if (bps < 1) return bfail(b, HYPE_ERR_CUDA, "stage kernel does not fit on an SM with %d-column tiles", cells);
     if (k.cells != cells) b->dirty = true;
@@ -410,6 +437,7 @@ static cudaError_t enqueue_kind_stage(hype_batch *b, int id, int st, cudaStream_
     const int blocks = b->sms * k.bps;
     const PlanStage &q = k.plan[st];
     if (k.mixed) return launch_mixed_batch(k.cells, k.dMParams + st * M, k.dMMaps + q.in * M, l.dWork, l.dSched, blocks, s);
+    if (k.path >= 0) return launch_path_batch(k.path, k.system, k.order, k.dParams + st * M, k.dMaps + q.in * M, l.dWork, l.dSched, blocks, s);
     return launch_stage_batch(k.system, k.order, k.cells, k.dParams + st * M, k.dMaps + q.in * M, l.dWork, l.dSched, blocks, s);
 }
 
@@ -504,8 +532,7 @@ const char *hype_batch_last_error(const hype_batch *b) { return b ? b->err : "nu
 
 size_t hype_batch_instance_bytes(const hype_config *cfg)
 {
-    if (!cfg || validate_config(cfg, nullptr, 0) != HYPE_OK || (cfg->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS)))
-        return 0;
+    if (!cfg || validate_config(cfg, nullptr, 0) != HYPE_OK) return 0;
     return state_bytes(*cfg);
 }
 
@@ -606,9 +633,6 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     char msg[256];
     int rc = validate_config(cfg, msg, sizeof(msg));
     if (rc) return bfail(b, rc, "%s", msg);
-    if (cfg->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS))
-        return bfail(b, HYPE_ERR_INVALID, "batches run the inviscid primitive-variable path "
-                                          "(HYPE_FLAG_CONSERVATIVE and HYPE_FLAG_VISCOUS are for solvers)");
     if ((long long)cfg->nx * cfg->ny > b->cfg.max_cells)
         return bfail(b, HYPE_ERR_INVALID, "grid %dx%d exceeds the batch's max_cells (%lld)", cfg->nx, cfg->ny, (long long)b->cfg.max_cells);
     int s = -1;
@@ -644,6 +668,7 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     std::vector<double> tab;
     if (ok && cfg->bc_left == HYPE_BC_INLET) {
         inlet_table(*cfg, in.h, tab);
+        if (cfg->flags & HYPE_FLAG_CONSERVATIVE) inlet_to_conserved(*cfg, tab);
         ok = pool_alloc(b, &in.inlet, sizeof(double) * tab.size()) == cudaSuccess;
     }
     if (!ok) {
@@ -664,6 +689,7 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     h.err_cell = 0xffffffffu;
     h.t = t0; h.t_final = t_final; h.max_steps = max_steps;
     h.cfl_h = in.cfl_h;
+    h.r1h_v = (cfg->flags & HYPE_FLAG_VISCOUS) ? 1. / in.h : 0.0;   // the viscous dt term (rhs_function_prim.c:617)
     BCUDA(b, cudaMemcpyAsync(&b->dSc[s], &h, sizeof(h), cudaMemcpyHostToDevice, b->stream));
     in.used = true;
     in.bytes = bytes;
@@ -687,7 +713,10 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     } else {
         CUtensorMap tm[3];
         if ((rc = inst_maps(b, k, in, tm, nullptr))) return rc;
-        BCUDA(b, launch_stage(k.system, k.order, k.cells, tm[0], inst_params(b, in, seed), b->stream));
+        const StageParams sp = inst_params(b, in, seed);
+        if (k.path == BATCH_PATH_CONS) BCUDA(b, launch_stage_cons(k.system, k.order, tm[0], sp, b->stream));
+        else if (k.path >= 0) BCUDA(b, launch_stage_visc(k.order, k.path == BATCH_PATH_VISC_CONS, tm[0], sp, b->stream));
+        else BCUDA(b, launch_stage(k.system, k.order, k.cells, tm[0], sp, b->stream));
     }
     BCUDA(b, launch_seed_dt(&b->dSc[s], in.cfl_h, b->stream));
     BCUDA(b, cudaMemcpyAsync(&b->hSc[s], &b->dSc[s], sizeof(DevScalars), cudaMemcpyDeviceToHost, b->stream));
@@ -828,6 +857,7 @@ int hype_batch_autotune(hype_batch *b, int reps, int *cells_out, int *rows_out)
         double best = 1e300;
         for (int c : cand_cells)
             for (int r : cand_rows) {
+                if (k.path >= 0 && c != STAGE_CELLS) continue;
                 if ((rc = kind_set_tiling(b, id, c, r))) return rc;
                 BCUDA(b, enqueue_kind_stage(b, id, 0, b->stream));   // warm
                 BCUDA(b, cudaEventRecord(b->ev0, b->stream));

@@ -93,6 +93,12 @@ cudaError_t launch_stage_visc(int order, bool cons, const CUtensorMap &tmap, con
 cudaError_t stage_cons_configure(int sys, int order);
 int stage_cons_blocks_per_sm(int sys, int order);
 cudaError_t launch_stage_cons(int sys, int order, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
+// persistent (batched) form of the conservative path and of the viscous build: 128-column tiles
+enum : int { BATCH_PATH_CONS = 0, BATCH_PATH_VISC = 1, BATCH_PATH_VISC_CONS = 2 };
+cudaError_t path_batch_configure(int path, int sys, int order);
+int path_batch_blocks_per_sm(int path, int sys, int order);
+cudaError_t launch_path_batch(int path, int sys, int order, const StageParams *inst, const CUtensorMap *tmaps, const int2 *work,
+                              int *sched, int blocks, cudaStream_t s);
 // Strips of a grid: with S = ceil(nx/(cells-4)) strips and even origins
 // 2*floor(s*nx/(2S)), every strip has at most 2*ceil(nx/(2S)) <= cells-4
 // columns and the last one at most nx/S + 2 <= cells-2.

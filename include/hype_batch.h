@@ -9,6 +9,9 @@
  * stage and per kind of instance, over a device work-list of (instance, tile)
  * items sorted longest first.  A whole step of the batch is one CUDA graph;
  * in it an instance takes one step, or several (hype_batch_set_substeps).
+ * Every configuration a solver takes is an instance kind: the FP64 primitive
+ * and conservative paths (HYPE_FLAG_CONSERVATIVE), the VISCOUS build
+ * (HYPE_FLAG_VISCOUS) and mixed precision.
  *
  * Instances join and leave between steps (continuous batching): the work-list,
  * member lists and per-instance parameters live in device memory, so adding or
@@ -111,7 +114,8 @@ HYPE_API int hype_batch_get_state(hype_batch *b, int id, double *U);
 /*
  * Tile shape of the persistent launches: tile width `cells` (64 or 128
  * columns) and about `rows` rows per tile (16..1024), applied to every
- * instance kind.  Rebuilds the work-list and the step graph.
+ * instance kind (the conservative and viscous kinds keep 128 columns).
+ * Rebuilds the work-list and the step graph.
  */
 HYPE_API int hype_batch_set_tiling(hype_batch *b, int cells, int rows);
 

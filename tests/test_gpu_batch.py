@@ -218,3 +218,39 @@ def test_substeps_take_several_exact_steps_per_batch_step(hp):
         check_same(hp, b, c, cs[1], U[1], 0.0, 1e30, 6)
         check_same(hp, b, m, cs[2], U[2], 0.0, 1e30, 13)
         check_same(hp, b, e, ce, Ue, 0.0, 0.02, 100000)
+
+
+def test_conservative_and_viscous_kinds_in_one_batch(hp):
+    """The conservative path (RHSFunction) and the VISCOUS build as batch kinds,
+    beside primitive-path and mixed instances: each equals its lone solver bit
+    for bit (the lone solvers are pinned to the reference in test_gpu_parity.py),
+    with the viscous dt term carried per instance; a tile-shape change keeps them."""
+    T, R, P, I = hp.BC_TRANSMISSIVE, hp.BC_REFLECTIVE, hp.BC_PERIODIC, hp.BC_INLET
+    CONS, VISC = hp.FLAG_CONSERVATIVE, hp.FLAG_VISCOUS
+    specs = [
+        (kapila(hp, 90, 70, flags=CONS), "shock_bubble"),
+        (kapila(hp, 64, 50, order=3, bcs=(T, T, P, P), flags=CONS), "shock_bubble"),
+        (kapila(hp, 60, 44, order=1, flags=VISC, mu1=0.4, mu2=0.05), "shock_bubble"),
+        (kapila(hp, 80, 64, order=2, bcs=(R, R, R, R), flags=VISC | CONS, mu1=0.2), "shock_bubble"),
+        (kapila(hp, 50, 48, order=3, bcs=(T, R, P, P), flags=VISC, mu1=1.0, mu2=0.3), "shock_bubble"),
+        (kapila(hp, 72, 40, bcs=(I, T, R, R), flags=CONS, x_min=0.0, x_max=2.0, y_min=-1.0, y_max=1.0), "shock_bubble"),
+        (hp.Config(system=hp.EULER, order=2, nx=70, ny=60, cfl=0.4, gamma1=1.4, gamma2=1.4, pi1=0.0, pi2=0.0, flags=CONS),
+         "euler_quadrants"),
+        (hp.Config(system=hp.BAER_NUNZIATO, order=1, nx=56, ny=56, cfl=0.4, flags=CONS | hp.FLAG_BN_FIX_P2), "bn_discs"),
+        (kapila(hp, 100, 60), "shock_bubble"),
+        (kapila(hp, 96, 64, precision=hp.PREC_MIXED), "shock_bubble"),
+    ]
+    runs = []
+    with hp.Batch(max_instances=16) as b:
+        for n, (cfg, ic) in enumerate(specs):
+            U0 = hp.initial_state(cfg, ic, seed=300 + n, **({"nbubbles": 2} if ic == "shock_bubble" else {}))
+            i = b.add(cfg, U0, 0.0, 1e30, 8)
+            runs.append((i, cfg, U0))
+        b.advance(4)
+        b.set_tiling(64, 32)       # the conservative and viscous kinds keep 128-column tiles
+        b.advance(6)
+        b.sync()
+        for i, cfg, U0 in runs:
+            check_same(hp, b, i, cfg, U0, 0.0, 1e30, 8)
+    for cfg, _ in specs[:6]:
+        assert hp.Batch.instance_bytes(cfg) > 0

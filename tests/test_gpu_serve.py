@@ -118,3 +118,28 @@ def test_callback_initial_state(hp):
         s.set_state(U0)
         s.solve(0.0, 1e30, 7)
         assert s.get_state().tobytes() == out[0].tobytes()
+
+
+def test_conservative_and_viscous_requests(hp):
+    """Requests for the conservative path and the VISCOUS build are served beside
+    primitive-path ones; each result equals a lone solver's bit for bit."""
+    T, R = hp.BC_TRANSMISSIVE, hp.BC_REFLECTIVE
+    CONS, VISC = hp.FLAG_CONSERVATIVE, hp.FLAG_VISCOUS
+    cfgs = [hp.Config(system=hp.KAPILA_5EQN, order=2, nx=70, ny=60, cfl=0.4, bc_bottom=R, bc_top=R, flags=VISC, mu1=0.3),
+            hp.Config(system=hp.KAPILA_5EQN, order=2, nx=64, ny=64, cfl=0.4, flags=CONS),
+            hp.Config(system=hp.KAPILA_5EQN, order=1, nx=80, ny=40, cfl=0.4, flags=VISC | CONS, mu1=0.1, mu2=0.02),
+            hp.Config(system=hp.KAPILA_5EQN, order=2, nx=90, ny=50, cfl=0.4),
+            hp.Config(system=hp.EULER, order=2, nx=60, ny=60, cfl=0.4, gamma1=1.4, gamma2=1.4, pi1=0.0, pi2=0.0, flags=CONS)]
+    reqs = []
+    for i, c in enumerate(cfgs):
+        ic = hp.IC_EULER_QUADRANTS if c.system == hp.EULER else hp.IC_SHOCK_BUBBLE
+        reqs.append(hp.Request(0.002 * i, c, max_steps=10 + i, ic=ic, ic_seed=700 + i, ic_param=2))
+    res, stats, out = collect(hp, reqs, max_instances=4)
+    assert stats["completed"] == len(reqs) and stats["failed"] == 0
+    for i, r in enumerate(reqs):
+        U, rr = out[i]
+        with hp.Solver(r.cfg) as s:
+            s.set_state(initial(hp, r))
+            k, t, _, st = s.solve(r.t0, r.t_final, r.max_steps)
+            assert st == hp.OK and (k, t) == (rr["steps"], rr["t_end"]), i
+            assert s.get_state().tobytes() == U.tobytes(), i
