@@ -199,7 +199,9 @@ __device__ __forceinline__ float minmod_f(float a, float b)
     return (fabsf(a) < fabsf(b)) ? a : b;
 }
 
-template <int CELLS_>
+// SLAB: a y-slab of a decomposed grid (row offset, edge rows stored into the
+// neighbours' halo rows); the single-grid and batched kernels compile without it.
+template <int CELLS_, bool SLAB = false>
 __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps *maps, int strip, int run,
                                            unsigned char *smem, double *red_s)
 {
@@ -263,8 +265,9 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::F_ROW_BYTES + K::D_ROW_BYTES);
-                tma_load_3d(rowf(row), &maps->f, xs, src + p.row_off, 0, bar);   // the maps start row_off rows below row 0
-                tma_load_3d(rowd(row), &maps->d, xs, src + p.row_off, 0, bar);
+                const int ty = SLAB ? src + p.row_off : src;   // a slab's maps start row_off rows below row 0
+                tma_load_3d(rowf(row), &maps->f, xs, ty, 0, bar);
+                tma_load_3d(rowd(row), &maps->d, xs, ty, 0, bar);
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {
@@ -468,16 +471,17 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                         }
                         if (c < 4) p.out_f[(size_t)c * p.plane + gidx] = (float)o;
                         else p.out_d[(size_t)(c - 4) * p.plane + gidx] = o;
-                        // a y-slab's edge rows are the neighbours' halo rows: store them there too
-                        if (p.push_lo_f && jo < 3) {
-                            const long long at = (long long)(jo + p.push_shift_lo) * p.pitch + i;
-                            if (c < 4) p.push_lo_f[c * p.push_plane_lo + at] = (float)o;
-                            else p.push_lo_d[(c - 4) * p.push_plane_lo + at] = o;
-                        }
-                        if (p.push_hi_f && jo >= p.ny - 3) {
-                            const long long at = (long long)(jo + p.push_shift_hi) * p.pitch + i;
-                            if (c < 4) p.push_hi_f[c * p.push_plane_hi + at] = (float)o;
-                            else p.push_hi_d[(c - 4) * p.push_plane_hi + at] = o;
+                        if constexpr (SLAB) {   // a y-slab's edge rows are the neighbours' halo rows: store them there too
+                            if (p.push_lo_f && jo < 3) {
+                                const long long at = (long long)(jo + p.push_shift_lo) * p.pitch + i;
+                                if (c < 4) p.push_lo_f[c * p.push_plane_lo + at] = (float)o;
+                                else p.push_lo_d[(c - 4) * p.push_plane_lo + at] = o;
+                            }
+                            if (p.push_hi_f && jo >= p.ny - 3) {
+                                const long long at = (long long)(jo + p.push_shift_hi) * p.pitch + i;
+                                if (c < 4) p.push_hi_f[c * p.push_plane_hi + at] = (float)o;
+                                else p.push_hi_d[(c - 4) * p.push_plane_hi + at] = o;
+                            }
                         }
                     }
                 }
@@ -591,13 +595,13 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
     for (int k = t; k < SLOTS; k += K::NT) mbar_inval(&bars[k]);
 }
 
-template <int CELLS>
+template <int CELLS, bool SLAB>
 __global__ void __launch_bounds__(2 * CELLS, (MixedKernel<CELLS>::MIN_BLOCKS))
 mixed_kernel(const __grid_constant__ MixedMaps maps, const MixedParams p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    mixed_tile<CELLS>(p, &maps, blockIdx.x, blockIdx.y, smem_raw, red_s);
+    mixed_tile<CELLS, SLAB>(p, &maps, blockIdx.x, blockIdx.y, smem_raw, red_s);
 }
 
 template <int CELLS>
@@ -628,15 +632,15 @@ mixed_batch_kernel(const MixedParams *__restrict__ inst, const MixedMaps *__rest
 }
 
 struct MixedEntry {
-    const void *single, *batch;
+    const void *single, *batch, *slab;
     size_t smem;
     int threads;
 };
 template <int CELLS>
 static MixedEntry mixed_entry_of()
 {
-    return MixedEntry{reinterpret_cast<const void *>(mixed_kernel<CELLS>), reinterpret_cast<const void *>(mixed_batch_kernel<CELLS>),
-                      MixedKernel<CELLS>::smem_bytes(), 2 * CELLS};
+    return MixedEntry{reinterpret_cast<const void *>(mixed_kernel<CELLS, false>), reinterpret_cast<const void *>(mixed_batch_kernel<CELLS>),
+                      reinterpret_cast<const void *>(mixed_kernel<CELLS, true>), MixedKernel<CELLS>::smem_bytes(), 2 * CELLS};
 }
 static MixedEntry mixed_entry(int cells) { return cells == 64 ? mixed_entry_of<64>() : mixed_entry_of<128>(); }
 
@@ -647,6 +651,7 @@ static cudaError_t mixed_configure(int cells)
 {
     const MixedEntry e = mixed_entry(cells);
     cudaError_t r = cudaFuncSetAttribute(e.single, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(e.slab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
     if (r != cudaSuccess) return r;
     return cudaFuncSetAttribute(e.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
 }
@@ -675,7 +680,7 @@ cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p,
     MixedMaps mm = maps;
     MixedParams pp = p;
     void *args[] = {&mm, &pp};
-    return cudaLaunchKernel(e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
+    return cudaLaunchKernel(p.row_off ? e.slab : e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
 cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
