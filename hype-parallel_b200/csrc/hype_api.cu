@@ -571,7 +571,7 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     CUDA_TRY(s, cudaSetDevice(cfg->device));
     cudaDeviceProp prop;
     CUDA_TRY(s, cudaGetDeviceProperties(&prop, cfg->device));
-    if (prop.major != 10) return fail(s, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", cfg->device, prop.major, prop.minor);
+    if (prop.major != 10) return fail(s, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; the library is built for sm_100a", cfg->device, prop.major, prop.minor);
     s->mixed = cfg->precision == HYPE_PREC_MIXED;
 
     s->nv = hype_nvar(cfg->system);

@@ -588,7 +588,7 @@ int hype_batch_create(const hype_batch_config *c, hype_batch **out)
     BCUDA(b, cudaSetDevice(c->device));
     cudaDeviceProp prop;
     BCUDA(b, cudaGetDeviceProperties(&prop, c->device));
-    if (prop.major != 10) return bfail(b, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; this build targets sm_100a", c->device, prop.major, prop.minor);
+    if (prop.major != 10) return bfail(b, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; the library is built for sm_100a", c->device, prop.major, prop.minor);
     b->sms = prop.multiProcessorCount;
     BCUDA(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     for (int k = 0; k < NKIND; ++k) {
