@@ -54,7 +54,9 @@ struct StageKernel {
     static constexpr int MIN_BLOCKS = (NV <= 6 ? 2 : 1) * (128 / CELLS);
     static constexpr size_t smem_bytes()
     {
-        return 128 /* barriers */ + (size_t)SLOTS * SLOT_STRIDE * 8 + (size_t)(COEF_ELEMS + YT_ELEMS + CARRY_ELEMS) * 8 + 64;
+        // the ring, the per-cell arrays and one more row slot: the conserved input of the row
+        // being finished (row r-1), for the RK combination
+        return 128 /* barriers */ + (size_t)(SLOTS + 1) * SLOT_STRIDE * 8 + (size_t)(COEF_ELEMS + YT_ELEMS + CARRY_ELEMS) * 8 + 64;
     }
 };
 
@@ -186,7 +188,9 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     // conserved a1r1, a2r2, ru, rv) at the top face, kept for the row above:
     // [q][g][d][cell], right behind the carries
     constexpr int NG = CONS ? 4 : 2, G0 = CONS ? 0 : 2;
-    double *ygt_s = carry_s + K::CARRY_ELEMS;
+    // conserved input of row r-1 (the row the RK combination finishes), [c][BW], its own mbarrier
+    double *orow_s = carry_s + K::CARRY_ELEMS;
+    double *ygt_s = orow_s + K::SLOT_STRIDE;
 
     const int t = threadIdx.x;
     const int m = t >> 1;            // cell of this thread's pair
@@ -216,7 +220,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
 
     __syncthreads();   // the previous tile of this block is done with every buffer
     if (t == 0) {
-        for (int s = 0; s < SLOTS; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s <= SLOTS; ++s) mbar_init(&bars[s], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -233,6 +237,8 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     unsigned bad_cell = 0xffffffffu;
 
     for (int r = y0 - 1; r <= y0 + H; ++r) {
+        // this iteration finishes an owned row (r-1) with an RK combination that reads its input
+        const bool finish_row = r > y0 && p.mode != OUT_RHS;
         // ---------------- A. bring rows up to r+2 into the ring --------------
         if (t == 0) {
             fence_proxy_async();   // earlier generic accesses to the slots precede the TMA writes
@@ -242,6 +248,10 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::ROW_BYTES);
                 tma_load_3d(row_ptr(row), tmap, xs, src + p.row_off, 0, bar);   // the map starts row_off rows below row 0
+            }
+            if (finish_row) {   // row r-1's conserved input for the RK combination in section C
+                mbar_expect_tx(&bars[SLOTS], K::ROW_BYTES);
+                tma_load_3d(orow_s, tmap, xs, (r - 1) + p.row_off, 0, &bars[SLOTS]);
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {
@@ -311,6 +321,17 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 }
 #pragma unroll
                 for (int c = 0; c < NV; ++c) rp[c * BW + cc] = V[c];
+            }
+        }
+        if (finish_row) {   // the copy of row r-1 issued at the start of this iteration
+            const unsigned parity = (unsigned)((r - y0 - 1) & 1);
+            bool ok = false;
+            for (long it = 0; it < (1L << 24); ++it) {
+                if (mbar_try_wait(&bars[SLOTS], parity)) { ok = true; break; }
+            }
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                return;   // block-uniform exit
             }
         }
         __syncthreads();   // S1: prim rows r-2 .. r+2 ready
@@ -499,7 +520,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                             else p.out[(size_t)c * p.plane + gidx] = rhs;
                             continue;
                         }
-                        const double Sv = p.in[(size_t)c * p.plane + gidx];
+                        const double Sv = orow_s[c * BW + ccm];   // = p.in[c * plane + gidx], staged by TMA
                         const double bF = b * rhs;
                         double o;
                         if (p.mode == OUT_AXPY) {
@@ -744,7 +765,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
             }
         }
     }
-    for (int k = t; k < SLOTS; k += K::NT) mbar_inval(&bars[k]);
+    for (int k = t; k <= SLOTS; k += K::NT) mbar_inval(&bars[k]);
 }
 
 }  // namespace hype
