@@ -40,7 +40,8 @@ struct MixedKernel {
     static constexpr int MIN_BLOCKS = 2 * (128 / CELLS);
     static constexpr size_t smem_bytes()
     {
-        return 128 + (size_t)SLOTS * SLOT_BYTES + (size_t)COEF_FLOATS * 4 + (size_t)YTF_FLOATS * 4 +
+        // the ring plus one more slot: the stage input of the row being finished (row r-1)
+        return 128 + (size_t)(SLOTS + 1) * SLOT_BYTES + (size_t)COEF_FLOATS * 4 + (size_t)YTF_FLOATS * 4 +
                (size_t)YTD_DOUBLES * 8 + (size_t)CARRY_DOUBLES * 8 + 64;
     }
 };
@@ -213,7 +214,11 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
 
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     unsigned char *rows = smem + 128;
-    float *coef_f = reinterpret_cast<float *>(rows + (size_t)SLOTS * K::SLOT_BYTES);
+    // stage input of row r-1 (the row the RK combination finishes): FP32 then FP64 planes
+    unsigned char *orow = rows + (size_t)SLOTS * K::SLOT_BYTES;
+    const float *orowf = reinterpret_cast<const float *>(orow);
+    const double *orowd = reinterpret_cast<const double *>(orow + K::F_REGION);
+    float *coef_f = reinterpret_cast<float *>(rows + (size_t)(SLOTS + 1) * K::SLOT_BYTES);
     double *exch = reinterpret_cast<double *>(coef_f);                  // x-face fluxes after S3: [7][cell]
     float *ytf = coef_f + K::COEF_FLOATS;                                 // [q][4][cell]
     double *ytd = reinterpret_cast<double *>(ytf + K::YTF_FLOATS);        // [q][2][cell]
@@ -240,7 +245,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
 
     __syncthreads();
     if (t == 0) {
-        for (int k = 0; k < SLOTS; ++k) mbar_init(&bars[k], 1);
+        for (int k = 0; k <= SLOTS; ++k) mbar_init(&bars[k], 1);
         fence_mbar_init();
     }
     __syncthreads();
@@ -257,6 +262,8 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
     unsigned bad_cell = 0xffffffffu;
 
     for (int r = y0 - 1; r <= y0 + H; ++r) {
+        // this iteration finishes an owned row (r-1) with an RK combination that reads its input
+        const bool finish_row = r > y0 && p.mode != OUT_RHS;
         // ---------------- A. rows up to r+2: two TMA loads (FP32, FP64 planes) per row
         if (t == 0) {
             fence_proxy_async();
@@ -268,6 +275,12 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 const int ty = SLAB ? src + p.row_off : src;   // a slab's maps start row_off rows below row 0
                 tma_load_3d(rowf(row), &maps->f, xs, ty, 0, bar);
                 tma_load_3d(rowd(row), &maps->d, xs, ty, 0, bar);
+            }
+            if (finish_row) {   // row r-1's stage input for the RK combination
+                const int ty = SLAB ? (r - 1) + p.row_off : r - 1;
+                mbar_expect_tx(&bars[SLOTS], K::F_ROW_BYTES + K::D_ROW_BYTES);
+                tma_load_3d(orow, &maps->f, xs, ty, 0, &bars[SLOTS]);
+                tma_load_3d(orow + K::F_REGION, &maps->d, xs, ty, 0, &bars[SLOTS]);
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {
@@ -327,6 +340,16 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 rf[3 * BW + cc] = (float)v;
                 rd[cc] = pr;
                 rd[BW + cc] = a1;
+            }
+        }
+        if (finish_row) {   // the copy of row r-1 issued at the start of this iteration
+            const unsigned parity = (unsigned)((r - y0 - 1) & 1);
+            bool ok = false;
+            for (long it = 0; it < (1L << 22); ++it)
+                if (mbar_try_wait(&bars[SLOTS], parity)) { ok = true; break; }
+            if (__syncthreads_or(!ok)) {
+                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                return;
             }
         }
         __syncthreads();   // S1
@@ -461,7 +484,8 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                             p.out_rhs[((size_t)jo * p.nx + i) * NV + c] = rhs;
                             continue;
                         }
-                        const double Sv = c < 4 ? (double)p.in_f[(size_t)c * p.plane + gidx] : p.in_d[(size_t)(c - 4) * p.plane + gidx];
+                        // = the stage input at (row r-1, i), staged by TMA
+                        const double Sv = c < 4 ? (double)orowf[c * BW + ccm] : orowd[(c - 4) * BW + ccm];
                         double o;
                         if (p.mode == OUT_AXPY) {
                             o = Sv + b * rhs;
@@ -592,7 +616,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
             if (b > 0.0) atomicMax(&p.sc->smax, (unsigned long long)__double_as_longlong(b));
         }
     }
-    for (int k = t; k < SLOTS; k += K::NT) mbar_inval(&bars[k]);
+    for (int k = t; k <= SLOTS; k += K::NT) mbar_inval(&bars[k]);
 }
 
 template <int CELLS, bool SLAB>
