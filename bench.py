@@ -13,9 +13,11 @@ independent replicas (the path does not shard across GPUs here), so scaling
 is weak and no collective touches the data path; timing is the max over ranks.
 
 `--impl reference` times the reference's own HyPE-2D code on the host cores
-(oracle/_ref, the unmodified sources compiled against a one-rank PETSc
-stand-in): one process per core, each stepping an independent 256 x 256
-instance of the same workload.
+(oracle/_ref, the unmodified sources compiled against the PETSc stand-in) on
+the same 2048 x 2048 workload, as one live MPI rank per host core on the DMDA
+split PETSc would choose (the stand-in's shared-memory MPI); its input comes
+from the oracle's own generator, so that arm never loads this repository's
+library.
 """
 from __future__ import annotations
 
@@ -24,7 +26,6 @@ import ctypes
 import importlib.util
 import json
 import math
-import multiprocessing as mp
 import os
 import subprocess
 import sys
@@ -128,108 +129,90 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the reference's own code (oracle/_ref) or the oracle port
+# CPU baseline and reference arm: the reference's own code (oracle/_ref) run as
+# live MPI ranks on the host cores, on this workload
 # ---------------------------------------------------------------------------
-def _cpu_worker(args):
-    steps, nx, ny, use_ref = args
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def reference_run(nranks: int, warmup: int, steps: int, budget_s: float, nx: int = NX, ny: int = NY):
+    """The reference's RHSFunctionPrim and hype.c time loop (oracle/_ref: the
+    HyPE-2D sources on the PETSc stand-in) on this workload -- the 2048^2
+    4-bubble shock-bubble state of seed 0, built by the oracle's own generator --
+    as `nranks` live MPI ranks on the DMDA split PETSC_DECIDE gives (what
+    `mpiexec -n nranks` runs), halos and the dt reduction through shared memory.
+    Times up to `steps` SSP-RK steps after `warmup`, one at a time, stopping once
+    `budget_s` seconds of timed steps have passed (at least one step).
+    Falls back to the oracle port on one core when oracle/_ref is absent."""
     sys.path.insert(0, ROOT)
-    hp = load_pkg()
     import oracle as O
-    pc = hp.Config(nx=nx, ny=ny)
-    U = hp.initial_state(pc, "shock_bubble", seed=SEED, nbubbles=NBUB)
     cfg = O.Config(system=O.KAPILA, order=2, nx=nx, ny=ny, cfl=0.4)
-    if use_ref:
-        ref = O.Reference(O.KAPILA)
-        ref.setup(cfg)
-        t0 = time.perf_counter()
-        _, n, *_ = ref.solve(U, 0.0, 1e30, steps)
-    else:
+    U = O.initial_state(cfg, "shock_bubble", seed=SEED, nbubbles=NBUB)
+    if not O.reference_available():
         orc = O.Oracle()
         t0 = time.perf_counter()
-        _, n, *_ = orc.solve(cfg, U, 0.0, 1e30, steps)
-    dt = time.perf_counter() - t0
-    return nx * ny * steps, dt
+        _, n, *_ = orc.solve(cfg, U, 0.0, 1e30, 1)
+        sec = time.perf_counter() - t0
+        return {"value": nx * ny * n / sec, "cores": 1, "kind": "port", "timed_steps": n, "seconds": sec,
+                "process_grid": "1x1", "status": 0}
+    with O.LiveReference(cfg, nranks) as L:
+        st = L.begin(U, 0.0, 1e30)
+        if st == 0 and warmup > 0:
+            st = L.advance(warmup)[3]
+        done, sec = 0, 0.0
+        while st == 0 and done < max(1, steps):
+            n, _, _, st, s1 = L.advance(1)
+            done += 1
+            sec += s1
+            if sec >= budget_s:
+                break
+        xs = sorted({b[0] for b in L.blocks})
+        ys = sorted({b[1] for b in L.blocks})
+    return {"value": nx * ny * done / sec if sec > 0 else None, "cores": nranks, "kind": "reference", "timed_steps": done,
+            "seconds": sec, "process_grid": f"{len(xs)}x{len(ys)}", "status": st}
 
 
-def cpu_baseline(nproc: int, steps: int, nx: int = 256, ny: int = 256):
-    sys.path.insert(0, ROOT)
-    import oracle as O
-    use_ref = O.reference_available()
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(nproc) as pool:
-        res = pool.map(_cpu_worker, [(steps, nx, ny, use_ref)] * nproc)
-    cells = sum(r[0] for r in res)
-    tmax = max(r[1] for r in res)
-    return {"value": cells / tmax, "unit": UNIT, "cores": nproc, "kind": "reference" if use_ref else "port",
-            "sample": f"{nproc} x independent Kapila shock-bubble {nx}x{ny} (4 bubbles), {steps} SSPRK(4,3) steps each, "
-                      f"{'oracle/_ref: HyPE-2D sources on a one-rank PETSc stand-in' if use_ref else 'oracle port'}"}
-
-
-_REF = {}
-
-
-def _ref_init(nx, ny, use_ref):
-    """Pool worker set-up: one independent shock-bubble instance per process."""
-    sys.path.insert(0, ROOT)
-    hp = load_pkg()
-    import oracle as O
-    U = hp.initial_state(hp.Config(nx=nx, ny=ny), "shock_bubble", seed=SEED, nbubbles=NBUB)
-    cfg = O.Config(system=O.KAPILA, order=2, nx=nx, ny=ny, cfl=0.4)
-    _REF.update(cfg=cfg, U=U, t=0.0, cells=nx * ny)
-    if use_ref:
-        _REF["ref"] = O.Reference(O.KAPILA)
-        _REF["ref"].setup(cfg)
-    else:
-        _REF["orc"] = O.Oracle()
-
-
-def _ref_sample(steps):
-    """Advances this process's instance by `steps` SSPRK(4,3) steps (one TS solve, as hype.c runs it)."""
-    t0 = time.perf_counter()
-    if "ref" in _REF:
-        U, n, t, *_ = _REF["ref"].solve(_REF["U"], _REF["t"], 1e30, steps)
-    else:
-        U, n, t, *_ = _REF["orc"].solve(_REF["cfg"], _REF["U"], _REF["t"], 1e30, steps)
-    _REF["U"], _REF["t"] = U, t
-    return _REF["cells"] * n, time.perf_counter() - t0
+def cpu_baseline(budget_s: float = 20.0):
+    """The reference beside the GPU number: the same workload on all host cores,
+    a bounded sample (1 warm-up step, then steps until ~budget_s seconds)."""
+    cores = host_cores()
+    r = reference_run(cores, 1, 1 << 20, budget_s)
+    return {"value": r["value"], "unit": UNIT, "cores": r["cores"], "kind": r["kind"],
+            "sample": f"the 2048x2048 Kapila shock-bubble workload (seed 0, 4 bubbles), {r['timed_steps']} SSPRK(4,3) "
+                      f"step(s) after 1 warm-up step, {r['seconds']:.1f} s; oracle/_ref (HyPE-2D's sources on the PETSc "
+                      f"stand-in) as {r['cores']} live MPI ranks, process grid {r['process_grid']} (PETSC_DECIDE)"}
 
 
 def run_reference(args, rank, world):
-    """The reference's own CPU implementation of the path (oracle/_ref: the
-    HyPE-2D sources on a one-rank PETSc stand-in, or the oracle port if it was
-    not built) on all host cores: one process per core, each stepping an
-    independent 128 x 128 instance of the workload, 4 steps per sample.  Under
-    torchrun only rank 0 runs."""
+    """The reference's own CPU implementation of the path on all host cores, on
+    this arm's workload: oracle/_ref as one live MPI rank per core over the
+    2048^2 grid (reference_run).  A run of --steps K --warmup W times up to K
+    steps after min(W, 1) warm-up steps, within a time budget so the arm ends in
+    minutes on any host.  Under torchrun only rank 0 runs; it never loads this
+    repository's library."""
     if rank != 0:
         return 0
-    sys.path.insert(0, ROOT)
-    import oracle as O
-    use_ref = O.reference_available()
-    nproc = os.cpu_count() or 1
-    nx = ny = 128
-    per = 4
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(nproc, initializer=_ref_init, initargs=(nx, ny, use_ref)) as pool:
-        for _ in range(max(0, args.warmup)):
-            pool.map(_ref_sample, [per] * nproc, chunksize=1)
-        vals = []
-        for _ in range(args.steps):
-            t0 = time.perf_counter()
-            res = pool.map(_ref_sample, [per] * nproc, chunksize=1)
-            wall = time.perf_counter() - t0
-            vals.append(sum(r[0] for r in res) / wall)
-    value = float(np.median(vals))
-    kind = "reference" if use_ref else "port"
-    base = {"value": value, "unit": UNIT, "cores": nproc, "kind": kind,
-            "sample": f"{nproc} processes x independent Kapila shock-bubble {nx}x{ny} (4 bubbles), {per} SSPRK(4,3) "
-                      f"steps per sample, median of {args.steps} samples; "
-                      f"{'oracle/_ref: HyPE-2D sources on a one-rank PETSc stand-in' if use_ref else 'oracle port'}"}
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded shock-bubble generator)",
-            "config": {"workload": "kapila5-shock-bubble-2048x2048-fp64-weno3-ssprk43", "grid": f"{nx}x{ny} per core (sample)",
-                       "system": "kapila5", "order": 2, "bubbles": NBUB, "cfl": 0.4, "cores": nproc},
-            "cpu_baseline": base,
+    cores = host_cores()
+    r = reference_run(cores, min(args.warmup, 1), args.steps, args.ref_budget_s)
+    value = r["value"]
+    sample = (f"the 2048x2048 Kapila shock-bubble workload (seed 0, 4 bubbles), {r['timed_steps']} of {args.steps} "
+              f"requested SSPRK(4,3) steps timed ({r['seconds']:.1f} s, budget {args.ref_budget_s:.0f} s) after "
+              f"{min(args.warmup, 1)} warm-up step; "
+              + (f"oracle/_ref (HyPE-2D's sources on the PETSc stand-in) as {cores} live MPI ranks, process grid "
+                 f"{r['process_grid']} (PETSC_DECIDE)" if r["kind"] == "reference" else "oracle port, one core"))
+    base = {"value": value, "unit": UNIT, "cores": r["cores"], "kind": r["kind"], "sample": sample}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": r["timed_steps"],
+            "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * r["seconds"] / max(1, r["timed_steps"]),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded shock-bubble generator)",
+            "config": {"workload": "kapila5-shock-bubble-2048x2048-fp64-weno3-ssprk43", "grid": f"{NX}x{NY}",
+                       "system": "kapila5", "order": 2, "bubbles": NBUB, "cfl": 0.4, "ranks": r["cores"],
+                       "process_grid": r["process_grid"], "steps_requested": args.steps, "same_config": True},
+            "status": r["status"], "cpu_baseline": base,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -601,7 +584,7 @@ def run_gpu(args, rank, world, local_rank):
 
     if rank != 0:
         return 0
-    cpu = None if args.no_cpu_baseline else cpu_baseline(1, 2)
+    cpu = None if args.no_cpu_baseline else cpu_baseline()
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64", "data": "synthetic (seeded shock-bubble generator, random-init)",
@@ -631,6 +614,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-budget-s", type=float, default=120.0,
+                    help="reference arm: seconds of timed reference steps after which it stops early")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default stage tile shape")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")

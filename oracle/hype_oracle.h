@@ -11,6 +11,8 @@
 #ifndef HYPE_ORACLE_H
 #define HYPE_ORACLE_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -52,6 +54,12 @@ int hyo_solve(const hyo_config *cfg, double *U, double t0, double t_final, int m
 /* Counters from the last hyo_rhs call in this thread: cells whose PAD check
  * failed (fallback to minmod), for tests. */
 long hyo_last_pad_fallbacks(void);
+
+/* Seeded initial states of the benchmark workloads (hype_oracle_ic.c), the same
+ * bits as the product's include/hype_ic.h generators; U holds nx*ny*nvar doubles. */
+int hyo_ic_shock_bubble(const hyo_config *cfg, uint64_t seed, int nbubbles, double *U);
+int hyo_ic_bn_discs(const hyo_config *cfg, uint64_t seed, double *U);
+int hyo_ic_euler_quadrants(const hyo_config *cfg, uint64_t seed, double *U);
 
 #ifdef __cplusplus
 }

@@ -7,6 +7,8 @@
 #include <stdarg.h>
 #include <time.h>
 #include <stddef.h>
+#include <stdatomic.h>
+#include <sched.h>
 
 /* ------------------------------------------------------------------------- */
 /* MPI on one rank                                                            */
@@ -34,18 +36,104 @@ void petsc_mini_emulate_rank(int rank, int size, PetscInt ys, PetscInt ym, const
     if (size <= 1) { g_emu_rank = 0; g_emu_size = 1; g_emu_ys = 0; g_emu_ym = -1; g_emu_full = NULL; }
 }
 
-int MPI_Allreduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, MPI_Comm c)
+/* ------------------------------------------------------------------------- */
+/* Live ranks: `size` processes that share one memory segment (what mpiexec   */
+/* and MPI give the reference).  The segment holds a barrier, an abort flag,  */
+/* one reduction slot per rank and an exchange copy of the grid through which */
+/* DMGlobalToLocal passes each rank's edge strips to its neighbours.          */
+/* ------------------------------------------------------------------------- */
+#define LIVE_MAX_RANKS 1024
+#define LIVE_RED_SLOTS 8
+typedef struct {
+    _Atomic int arrived;
+    _Atomic int sense;
+    _Atomic int aborted;
+    int pad_;
+    long long pad2_;
+    double red[LIVE_MAX_RANKS][LIVE_RED_SLOTS];       /* MPI_Allreduce contributions */
+} live_hdr;
+static live_hdr *g_live = NULL;
+static double *g_live_exch = NULL;
+static int g_live_rank = 0, g_live_size = 1, g_live_px = 0, g_live_py = 0, g_live_sense = 0;
+static long long g_live_exch_doubles = 0;   /* capacity of the exchange copy */
+static double g_live_wait_s = 600.0;
+
+static size_t live_hdr_bytes(void) { return (sizeof(live_hdr) + 255) & ~(size_t)255; }
+size_t petsc_mini_live_bytes(long long grid_doubles) { return live_hdr_bytes() + (size_t)grid_doubles * sizeof(double); }
+
+int petsc_mini_live_join(int rank, int size, int px, int py, void *shm, long long grid_doubles)
 {
-    (void)t; (void)op; (void)c;
-    memmove(r, s, (size_t)count * sizeof(double));
+    if (size <= 1 || !shm) { g_live = NULL; g_live_exch = NULL; g_live_rank = 0; g_live_size = 1; return 0; }
+    if (size > LIVE_MAX_RANKS || rank < 0 || rank >= size) return 1;
+    if ((px > 0 || py > 0) && px * py != size) return 1;
+    g_live = (live_hdr *)shm;
+    g_live_exch = (double *)((char *)shm + live_hdr_bytes());
+    g_live_rank = rank; g_live_size = size; g_live_px = px; g_live_py = py;
+    g_live_sense = 0;
+    g_live_exch_doubles = grid_doubles;
     return 0;
 }
-int MPI_Comm_size(MPI_Comm c, int *size) { (void)c; *size = g_emu_size; return 0; }
-int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = g_emu_rank; return 0; }
+void petsc_mini_live_set_wait(double seconds) { g_live_wait_s = seconds; }
+
+static double live_now(void)
+{
+    struct timespec t; clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+/* Sense-reversing barrier over the live ranks.  A rank that aborted (MPI_Abort)
+ * raises the shared flag; the others leave the barrier through MPI_Abort too, as
+ * mpiexec ends every rank of a job one of whose ranks called MPI_Abort.  A wait
+ * longer than g_live_wait_s (a rank that died) counts as an abort as well. */
+static void live_barrier(void)
+{
+    const int my = g_live_sense = !g_live_sense;
+    if (atomic_fetch_add(&g_live->arrived, 1) == g_live_size - 1) {
+        atomic_store(&g_live->arrived, 0);
+        atomic_store(&g_live->sense, my);
+        return;
+    }
+    const double t0 = live_now();
+    for (long spin = 0;; ++spin) {
+        if (atomic_load(&g_live->sense) == my) return;
+        if (atomic_load(&g_live->aborted)) MPI_Abort(PETSC_COMM_WORLD, 1);
+        if ((spin & 1023) == 1023) {
+            sched_yield();
+            if (live_now() - t0 > g_live_wait_s) { atomic_store(&g_live->aborted, 1); MPI_Abort(PETSC_COMM_WORLD, 1); }
+        }
+    }
+}
+
+int MPI_Allreduce(const void *s, void *r, int count, MPI_Datatype t, MPI_Op op, MPI_Comm c)
+{
+    (void)t; (void)c;
+    if (!g_live) { memmove(r, s, (size_t)count * sizeof(double)); return 0; }
+    if (count > LIVE_RED_SLOTS) { fprintf(stderr, "petsc_mini: MPI_Allreduce of %d values\n", count); MPI_Abort(c, 1); }
+    const double *sv = (const double *)s;
+    for (int k = 0; k < count; ++k) g_live->red[g_live_rank][k] = sv[k];
+    live_barrier();
+    double out[LIVE_RED_SLOTS];
+    for (int k = 0; k < count; ++k) {
+        double v = g_live->red[0][k];
+        for (int q = 1; q < g_live_size; ++q) {
+            const double x = g_live->red[q][k];
+            if (op == MPIU_MIN) v = (x < v) ? x : v;
+            else if (op == MPIU_MAX) v = (x > v) ? x : v;
+            else v = v + x;
+        }
+        out[k] = v;
+    }
+    live_barrier();   /* every rank has read the slots before they are written again */
+    memcpy(r, out, (size_t)count * sizeof(double));
+    return 0;
+}
+int MPI_Comm_size(MPI_Comm c, int *size) { (void)c; *size = g_live ? g_live_size : g_emu_size; return 0; }
+int MPI_Comm_rank(MPI_Comm c, int *rank) { (void)c; *rank = g_live ? g_live_rank : g_emu_rank; return 0; }
 int MPI_Abort(MPI_Comm c, int code)
 {
     (void)c;
     g_abort_count++;
+    if (g_live) atomic_store(&g_live->aborted, 1);   /* ends the other ranks' collective calls */
     if (g_abort_env) longjmp(*g_abort_env, code ? code : 1);
     fprintf(stderr, "petsc_mini: MPI_Abort(%d)\n", code);
     exit(code ? code : 1);
@@ -128,18 +216,44 @@ PetscErrorCode VecRestoreArrayRead(Vec x, const PetscScalar **a) { (void)x; *a =
 PetscErrorCode VecGetLocalSize(Vec x, PetscInt *n) { *n = x->n; return 0; }
 
 /* ------------------------------------------------------------------------- */
-/* DMDA (one rank)                                                            */
+/* DMDA                                                                       */
 /* ------------------------------------------------------------------------- */
 
 struct _p_DM {
     PetscInt M, N, dof, s;
     DMBoundaryType bx, by;
     PetscInt xs_g, ys_g, xm_g, ym_g;   /* ghost corners */
-    PetscInt ys, ym;                    /* owned rows (all of them on one rank) */
+    PetscInt xs, xm, ys, ym;            /* owned block (the whole grid on one rank) */
     DM cda;                             /* coordinate DM (dof 2) */
     Vec coords;
-    /* one row-pointer table per array handed out (released on restore) */
 };
+
+/* Ownership ranges of a DMDA over an m x n process grid, as PETSc's DMSetUp_DA_2D
+ * (src/dm/impls/da/da2.c) sets them up with PETSC_DECIDE: m = the integer nearest
+ * sqrt(M size / N), lowered until it divides size, n = size / m, the two swapped
+ * when M > N and m < n; then M / m points per rank along x, the first M % m ranks
+ * one more (the same along y), ranks numbered x fastest. */
+static void live_grid(PetscInt M, PetscInt N, int size, int *m_out, int *n_out)
+{
+    int m = g_live_px, n = g_live_py;
+    if (m <= 0 || n <= 0) {
+        m = (int)(0.5 + sqrt(((PetscReal)M) * ((PetscReal)size) / ((PetscReal)N)));
+        if (!m) m = 1;
+        while (m > 0) {
+            n = size / m;
+            if (m * n == size) break;
+            m--;
+        }
+        if (M > N && m < n) { int t = m; m = n; n = t; }
+    }
+    *m_out = m; *n_out = n;
+}
+static void own_range(PetscInt M, int m, int r, PetscInt *start, PetscInt *len)
+{
+    PetscInt st = 0;
+    for (int q = 0; q < r; ++q) st += M / m + ((M % m) > q);
+    *start = st; *len = M / m + ((M % m) > r);
+}
 
 PetscErrorCode DMDACreate2d(MPI_Comm c, DMBoundaryType bx, DMBoundaryType by, DMDAStencilType st,
                             PetscInt M, PetscInt N, PetscInt m, PetscInt n, PetscInt dof, PetscInt s,
@@ -148,12 +262,24 @@ PetscErrorCode DMDACreate2d(MPI_Comm c, DMBoundaryType bx, DMBoundaryType by, DM
     (void)c; (void)st; (void)m; (void)n; (void)lx; (void)ly;
     DM d = (DM)calloc(1, sizeof(*d));
     d->M = M; d->N = N; d->dof = dof; d->s = s; d->bx = bx; d->by = by;
-    /* GHOSTED and PERIODIC both carry s ghost layers on a single rank */
+    /* GHOSTED and PERIODIC both carry s ghost layers on every side of a rank's block */
     int gx = (bx == DM_BOUNDARY_NONE) ? 0 : s;
     int gy = (by == DM_BOUNDARY_NONE) ? 0 : s;
-    d->xs_g = -gx; d->xm_g = M + 2 * gx;
+    d->xs = 0; d->xm = M;
     d->ys = 0; d->ym = N;
-    if (g_emu_ym >= 0) { d->ys = g_emu_ys; d->ym = g_emu_ym; }
+    if (g_live) {
+        int pm, pn;
+        live_grid(M, N, g_live_size, &pm, &pn);
+        own_range(M, pm, g_live_rank % pm, &d->xs, &d->xm);
+        own_range(N, pn, g_live_rank / pm, &d->ys, &d->ym);
+        if ((long long)M * N * dof > g_live_exch_doubles) {
+            fprintf(stderr, "petsc_mini: live exchange copy too small for a %dx%dx%d DMDA\n", M, N, dof);
+            MPI_Abort(c, 1);
+        }
+    } else if (g_emu_ym >= 0) {
+        d->ys = g_emu_ys; d->ym = g_emu_ym;
+    }
+    d->xs_g = d->xs - gx; d->xm_g = d->xm + 2 * gx;
     d->ys_g = d->ys - gy; d->ym_g = d->ym + 2 * gy;
     *da = d;
     return 0;
@@ -169,7 +295,7 @@ PetscErrorCode DMDestroy(DM *da)
     return 0;
 }
 PetscErrorCode DMView(DM da, PetscViewer v) { (void)da; (void)v; return 0; }
-PetscErrorCode DMCreateGlobalVector(DM da, Vec *v) { *v = vec_new(da->M * da->ym * da->dof, da, 0); return 0; }
+PetscErrorCode DMCreateGlobalVector(DM da, Vec *v) { *v = vec_new(da->xm * da->ym * da->dof, da, 0); return 0; }
 PetscErrorCode DMCreateLocalVector(DM da, Vec *v) { *v = vec_new(da->xm_g * da->ym_g * da->dof, da, 1); return 0; }
 
 static inline PetscInt wrap(PetscInt i, PetscInt n) { PetscInt r = i % n; return r < 0 ? r + n : r; }
@@ -178,6 +304,22 @@ PetscErrorCode DMGlobalToLocalBegin(DM da, Vec g, InsertMode m, Vec l)
 {
     (void)m;
     const PetscInt dof = da->dof;
+    if (g_live) {
+        /* each rank publishes the strips of width s along its block's edges into the
+         * exchange copy (what its neighbours read), then reads its ghosts from there */
+        const PetscInt s = da->s;
+        for (PetscInt j = da->ys; j < da->ys + da->ym; ++j) {
+            PetscScalar *dst = g_live_exch + ((size_t)j * da->M + da->xs) * dof;
+            const PetscScalar *src = g->a + (size_t)(j - da->ys) * da->xm * dof;
+            if (j < da->ys + s || j >= da->ys + da->ym - s || da->xm <= 2 * s) {
+                memcpy(dst, src, (size_t)da->xm * dof * sizeof(PetscScalar));
+            } else {
+                memcpy(dst, src, (size_t)s * dof * sizeof(PetscScalar));
+                memcpy(dst + (size_t)(da->xm - s) * dof, src + (size_t)(da->xm - s) * dof, (size_t)s * dof * sizeof(PetscScalar));
+            }
+        }
+        live_barrier();
+    }
     for (PetscInt j = da->ys_g; j < da->ys_g + da->ym_g; ++j) {
         int jin = (j >= 0 && j < da->N);
         if (!jin && da->by != DM_BOUNDARY_PERIODIC) continue;       /* no source: keep */
@@ -186,25 +328,28 @@ PetscErrorCode DMGlobalToLocalBegin(DM da, Vec g, InsertMode m, Vec l)
             int iin = (i >= 0 && i < da->M);
             if (!iin && da->bx != DM_BOUNDARY_PERIODIC) continue;   /* no source: keep */
             PetscInt is = iin ? i : wrap(i, da->M);
-            /* this rank's rows from its global vector, the other ranks' from the emulation's array */
-            const int own = js >= da->ys && js < da->ys + da->ym;
-            if (!own && !g_emu_full) continue;
-            const PetscScalar *src = own ? g->a + ((size_t)(js - da->ys) * da->M + is) * dof
-                                         : g_emu_full + ((size_t)js * da->M + is) * dof;
+            /* this rank's block from its global vector, the other ranks' points from the
+             * live exchange copy or the emulation's array */
+            const int own = js >= da->ys && js < da->ys + da->ym && is >= da->xs && is < da->xs + da->xm;
+            const PetscScalar *other = g_live ? g_live_exch : g_emu_full;
+            if (!own && !other) continue;
+            const PetscScalar *src = own ? g->a + ((size_t)(js - da->ys) * da->xm + (is - da->xs)) * dof
+                                         : other + ((size_t)js * da->M + is) * dof;
             PetscScalar *dst = l->a + ((size_t)(j - da->ys_g) * da->xm_g + (i - da->xs_g)) * dof;
             memcpy(dst, src, (size_t)dof * sizeof(PetscScalar));
         }
     }
+    if (g_live) live_barrier();   /* every rank has read the copy before it is written again */
     return 0;
 }
 PetscErrorCode DMGlobalToLocalEnd(DM da, Vec g, InsertMode m, Vec l) { (void)da; (void)g; (void)m; (void)l; return 0; }
 
 PetscErrorCode DMDAGetCorners(DM da, PetscInt *xs, PetscInt *ys, PetscInt *zs, PetscInt *xm, PetscInt *ym, PetscInt *zm)
 {
-    if (xs) *xs = 0;
+    if (xs) *xs = da->xs;
     if (ys) *ys = da->ys;
     if (zs) *zs = 0;
-    if (xm) *xm = da->M;
+    if (xm) *xm = da->xm;
     if (ym) *ym = da->ym;
     if (zm) *zm = 1;
     return 0;
@@ -226,7 +371,7 @@ PetscErrorCode DMDAVecGetArray(DM da, Vec v, void *array)
 {
     PetscInt xs, ys, xm, ym;
     if (v->local) { xs = da->xs_g; ys = da->ys_g; xm = da->xm_g; ym = da->ym_g; }
-    else { xs = 0; ys = v->dm->ys; xm = v->dm->M; ym = v->dm->ym; }
+    else { xs = v->dm->xs; ys = v->dm->ys; xm = v->dm->xm; ym = v->dm->ym; }
     const PetscInt dof = v->dm->dof;
     char **rows = (char **)malloc((size_t)ym * sizeof(char *));
     for (PetscInt r = 0; r < ym; ++r)

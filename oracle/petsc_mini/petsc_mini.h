@@ -7,7 +7,8 @@
  * PETSc itself (DMDA halo scatter, TS SSP schemes) is not available in this
  * image; what is restated here follows PETSc's published behaviour:
  *   - DMDA 2D, dof per point, stencil width s, DM_BOUNDARY_GHOSTED/PERIODIC,
- *     one rank: owned range = whole grid, local vectors carry s ghost layers.
+ *     local vectors carry s ghost layers; one rank owns the whole grid, live
+ *     ranks (petsc_mini_live_join) own the blocks of PETSc's process grid.
  *     DMGlobalToLocal copies owned values and fills ghost points whose source
  *     exists (periodic wrap); other ghost points keep their previous contents.
  *   - DMDAVecGetArray returns row pointers offset so that a[j][i] is valid for
@@ -71,6 +72,17 @@ int MPI_Abort(MPI_Comm c, int code);
 /* test hook: emulate rank `rank` of `size` owning rows ys..ys+ym-1 of a y-split DMDA,
  * the other ranks' rows read from `full`; size <= 1 switches it off */
 void petsc_mini_emulate_rank(int rank, int size, PetscInt ys, PetscInt ym, const PetscScalar *full);
+/* Live ranks: `size` processes (this one is `rank`) share the zero-filled segment
+ * `shm` of petsc_mini_live_bytes(grid_doubles) bytes, grid_doubles being at least
+ * M*N*dof of the DMDAs they create.  DMDAs created after the join are split over a
+ * px x py process grid (0, 0: PETSc's PETSC_DECIDE rule), DMGlobalToLocal passes
+ * each rank's edge strips to its neighbours through the segment, MPI_Allreduce
+ * reduces over the ranks (MIN, MAX or sum, in rank order) and MPI_Abort in one rank
+ * ends the collective calls of all of them.  Returns 0, or 1 for a bad argument.
+ * size <= 1 leaves the live mode.  After an abort the segment is spent. */
+size_t petsc_mini_live_bytes(long long grid_doubles);
+int petsc_mini_live_join(int rank, int size, int px, int py, void *shm, long long grid_doubles);
+void petsc_mini_live_set_wait(double seconds);   /* longest barrier wait before an abort (600 s) */
 
 /* ---- objects ------------------------------------------------------------ */
 typedef struct _p_Vec         *Vec;

@@ -13,7 +13,13 @@
  *                                          basis()/basis_grad(), reconstruction.c:11-100)
  * ref_rhs() calls the reference's RHSFunctionPrim / RHSFunction once.
  * ref_solve() mirrors hype.c:337-384: a direct RHS call seeds Ctx.dt, then
- * TSSolve with the reference's MonitorFunction resetting dt every step.
+ * TSSolve with the reference's MonitorFunction resetting dt every step;
+ * ref_begin() / ref_advance() are the same loop split into chunks of steps.
+ *
+ * With live ranks (ref_live_join before ref_setup) the process is one MPI rank
+ * of a DMDA split over several processes, as under mpiexec: state arrays
+ * crossing this file's entry points are then the rank's block (ref_corners),
+ * compact, in the Vec layout.
  */
 #include <setjmp.h>
 
@@ -52,19 +58,41 @@ static AppCtx Ctx;
 static DM da = NULL;
 static Vec U = NULL, RHS = NULL;
 static TS ts_rhs = NULL;
+static TS ts_run = NULL;      /* the time loop of ref_begin / ref_advance */
 static int g_ready = 0;
 
 int ref_nvar(void) { return nVar; }
 
+/* one MPI rank of `size` live processes sharing `shm` (petsc_mini_live_join); call before ref_setup */
+size_t ref_live_bytes(long long grid_doubles) { return petsc_mini_live_bytes(grid_doubles); }
+int ref_live_join(int rank, int size, int px, int py, void *shm, long long grid_doubles)
+{
+    return petsc_mini_live_join(rank, size, px, py, shm, grid_doubles);
+}
+void ref_live_set_wait(double seconds) { petsc_mini_live_set_wait(seconds); }
+
+/* this rank's block of the grid (the whole grid on one rank) */
+int ref_corners(int *xs, int *ys, int *xm, int *ym)
+{
+    if (!g_ready) return -1;
+    PetscInt a, b, c, d;
+    DMDAGetCorners(da, &a, &b, NULL, &c, &d, NULL);
+    *xs = a; *ys = b; *xm = c; *ym = d;
+    return 0;
+}
+static size_t local_doubles(void) { PetscInt n; VecGetLocalSize(U, &n); return (size_t)n; }
+
 void ref_teardown(void)
 {
     if (!g_ready) return;
+    if (ts_run) TSDestroy(&ts_run);
     VecDestroy(&U); VecDestroy(&RHS); VecDestroy(&Ctx.W); VecDestroy(&Ctx.localU);
     TSDestroy(&ts_rhs);
     free5d(Ctx.u_bnd); free3d(Ctx.F);
 #ifdef VISCOUS
     free6d(Ctx.u_bnd_grad);
-#endif free3d(Ctx.G); free3d(Ctx.D); free3d(Ctx.E);
+#endif
+    free3d(Ctx.G); free3d(Ctx.D); free3d(Ctx.E);
     free3d(Ctx.phiFace); free2d(Ctx.phiNode); free2d(Ctx.phiVol);
     free2d(Ctx.gradphiVol_x); free2d(Ctx.gradphiVol_y);
     free3d(Ctx.gradphiFace_x); free3d(Ctx.gradphiFace_y);
@@ -176,30 +204,23 @@ int ref_rhs(double t, const double *Uin, double *RHSout, double *dt_out, int pri
 {
     if (!g_ready) return -1;
     PetscScalar *a;
-    VecGetArray(U, &a); memcpy(a, Uin, sizeof(double) * (size_t)Ctx.N_x * Ctx.N_y * nVar); VecRestoreArray(U, &a);
+    VecGetArray(U, &a); memcpy(a, Uin, sizeof(double) * local_doubles()); VecRestoreArray(U, &a);
     jmp_buf env;
     petsc_mini_set_abort_target(&env);
     if (setjmp(env)) { petsc_mini_set_abort_target(NULL); return 1; }
     PetscErrorCode ierr = prim ? RHSFunctionPrim(ts_rhs, t, U, RHS, &Ctx) : RHSFunction(ts_rhs, t, U, RHS, &Ctx);
     petsc_mini_set_abort_target(NULL);
     if (ierr) return -2;
-    VecGetArray(RHS, &a); memcpy(RHSout, a, sizeof(double) * (size_t)Ctx.N_x * Ctx.N_y * nVar); VecRestoreArray(RHS, &a);
+    VecGetArray(RHS, &a); memcpy(RHSout, a, sizeof(double) * local_doubles()); VecRestoreArray(RHS, &a);
     if (dt_out) *dt_out = Ctx.dt;
     return 0;
 }
 
-/* Time loop as hype.c:337-384, with -ts_max_steps given as max_steps. */
-int ref_solve(double *Uio, double t0, double t_final, int max_steps, int prim,
-              int *steps_out, double *t_out, double *dt_out)
+/* TS set-up of hype.c:337-382 around the state in U: the direct RHS call that seeds
+ * Ctx.dt (hype.c:343), then the scheme of order N, MATCHSTEP and the monitor. */
+static TS make_ts(int prim, double t_final, int max_steps)
 {
-    if (!g_ready) return -1;
-    PetscScalar *a;
-    VecGetArray(U, &a); memcpy(a, Uio, sizeof(double) * (size_t)Ctx.N_x * Ctx.N_y * nVar); VecRestoreArray(U, &a);
-    Ctx.InitialTime = t0; Ctx.InitialStep = 0; Ctx.FinalTime = t_final;
     TS ts;
-    jmp_buf env;
-    petsc_mini_set_abort_target(&env);
-    if (setjmp(env)) { petsc_mini_set_abort_target(NULL); return 1; }
     TSCreate(PETSC_COMM_SELF, &ts);
     TSSetProblemType(ts, TS_NONLINEAR);
     TSSetDM(ts, da);
@@ -209,7 +230,7 @@ int ref_solve(double *Uio, double t0, double t_final, int max_steps, int prim,
     TSSetTime(ts, Ctx.InitialTime);
     TSSetTimeStep(ts, Ctx.dt);
     TSMonitorSet(ts, MonitorFunction, &Ctx, NULL);
-    TSSetMaxTime(ts, Ctx.FinalTime);
+    TSSetMaxTime(ts, t_final);
     TSSetExactFinalTime(ts, TS_EXACTFINALTIME_MATCHSTEP);
     TSSetMaxSteps(ts, max_steps);
     TSSetFromOptions(ts);
@@ -220,15 +241,76 @@ int ref_solve(double *Uio, double t0, double t_final, int max_steps, int prim,
         else if (Ctx.N == 2) { TSSSPSetType(ts, TSSSPRKS3); TSSSPSetNumStages(ts, 4); }
         else TSSSPSetType(ts, TSSSPRK104);
     }
+    return ts;
+}
+
+/* Time loop as hype.c:337-384, with -ts_max_steps given as max_steps. */
+int ref_solve(double *Uio, double t0, double t_final, int max_steps, int prim,
+              int *steps_out, double *t_out, double *dt_out)
+{
+    if (!g_ready) return -1;
+    PetscScalar *a;
+    VecGetArray(U, &a); memcpy(a, Uio, sizeof(double) * local_doubles()); VecRestoreArray(U, &a);
+    Ctx.InitialTime = t0; Ctx.InitialStep = 0; Ctx.FinalTime = t_final;
+    TS ts = NULL;
+    jmp_buf env;
+    petsc_mini_set_abort_target(&env);
+    if (setjmp(env)) { petsc_mini_set_abort_target(NULL); if (ts) TSDestroy(&ts); return 1; }
+    ts = make_ts(prim, Ctx.FinalTime, max_steps);
     PetscErrorCode ierr = TSSolve(ts, U);
     petsc_mini_set_abort_target(NULL);
     PetscInt n; PetscReal tt;
     TSGetStepNumber(ts, &n); TSGetTime(ts, &tt);
     TSDestroy(&ts);
     if (ierr) return -2;
-    VecGetArray(U, &a); memcpy(Uio, a, sizeof(double) * (size_t)Ctx.N_x * Ctx.N_y * nVar); VecRestoreArray(U, &a);
+    VecGetArray(U, &a); memcpy(Uio, a, sizeof(double) * local_doubles()); VecRestoreArray(U, &a);
     if (steps_out) *steps_out = n;
     if (t_out) *t_out = tt;
     if (dt_out) *dt_out = Ctx.dt;
+    return 0;
+}
+
+/* The same loop in chunks: ref_begin loads the state and seeds dt (hype.c:343);
+ * each ref_advance runs up to nsteps more steps of the one TS (TSSolve resumes
+ * where the last chunk stopped: its monitor call at the start only sets dt again
+ * to Ctx.dt).  Returns 0, 1 where the reference aborted, -1 without a begin. */
+int ref_begin(const double *Uin, double t0, double t_final, int prim)
+{
+    if (!g_ready) return -1;
+    if (ts_run) TSDestroy(&ts_run);
+    PetscScalar *a;
+    VecGetArray(U, &a); memcpy(a, Uin, sizeof(double) * local_doubles()); VecRestoreArray(U, &a);
+    Ctx.InitialTime = t0; Ctx.InitialStep = 0; Ctx.FinalTime = t_final;
+    jmp_buf env;
+    petsc_mini_set_abort_target(&env);
+    if (setjmp(env)) { petsc_mini_set_abort_target(NULL); return 1; }
+    ts_run = make_ts(prim, t_final, 0);
+    petsc_mini_set_abort_target(NULL);
+    return 0;
+}
+int ref_advance(int nsteps, int *steps_out, double *t_out, double *dt_out)
+{
+    if (!g_ready || !ts_run) return -1;
+    PetscInt n0;
+    TSGetStepNumber(ts_run, &n0);
+    TSSetMaxSteps(ts_run, n0 + nsteps);
+    jmp_buf env;
+    petsc_mini_set_abort_target(&env);
+    if (setjmp(env)) { petsc_mini_set_abort_target(NULL); TSDestroy(&ts_run); return 1; }
+    PetscErrorCode ierr = TSSolve(ts_run, U);
+    petsc_mini_set_abort_target(NULL);
+    if (ierr) return -2;
+    PetscInt n; PetscReal tt;
+    TSGetStepNumber(ts_run, &n); TSGetTime(ts_run, &tt);
+    if (steps_out) *steps_out = n;
+    if (t_out) *t_out = tt;
+    if (dt_out) *dt_out = Ctx.dt;
+    return 0;
+}
+int ref_get_state(double *Uout)
+{
+    if (!g_ready) return -1;
+    PetscScalar *a;
+    VecGetArray(U, &a); memcpy(Uout, a, sizeof(double) * local_doubles()); VecRestoreArray(U, &a);
     return 0;
 }
