@@ -160,6 +160,7 @@ def lib() -> ctypes.CDLL:
         L.hype_totals.argtypes = [vp, ctypes.c_int, _DP, _DP, _DP]
         L.hype_launch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3 + [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
         L.hype_last_elapsed_ms.argtypes = [vp, _DP]
+        L.hype_test_skip_row_loads.argtypes = [vp, ctypes.c_int]
         L.hype_time_stage.argtypes = [vp, ctypes.c_int, _DP]
         L.hype_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.hype_config_default.argtypes = [ctypes.POINTER(_Cfg)]
@@ -286,6 +287,9 @@ class Solver:
     def n(self) -> int:
         return self.cfg.nx * self.cfg.ny * self.cfg.nvar
 
+    def last_error(self) -> str:
+        return lib().hype_last_error(self._h).decode()
+
     def rhs_function_prim(self, t: float, U: np.ndarray, RHS: np.ndarray | None = None, check: bool = True):
         """RHSFunctionPrim: returns (RHS, dt, status)."""
         U = np.ascontiguousarray(U, dtype=np.float64)
@@ -411,6 +415,11 @@ class Solver:
         ms = ctypes.c_double(0.0)
         self._check(lib().hype_last_elapsed_ms(self._h, ctypes.byref(ms)))
         return ms.value
+
+    def test_skip_row_loads(self, row: int) -> None:
+        """Test hook (hype_test_skip_row_loads): issue no row load for rows >= row,
+        so the kernels' bounded wait runs out; row < 0 turns it off."""
+        self._check(lib().hype_test_skip_row_loads(self._h, row))
 
 
 def fp64_rate(device: int = 0, reps: int = 5) -> float:

@@ -154,6 +154,7 @@ static StageParams base_params(const hype_solver *s)
     p.inlet = s->dInlet;
     p.kb = 1.0;
     p.row_off = s->row_off;
+    if (s->test_skip_row >= 0) { p.skip_loads = 1; p.skip_loads_from = s->test_skip_row; }
     return p;
 }
 
@@ -267,6 +268,7 @@ static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double
     p.sc = s->dSc; p.reduce_smax = reduce;
     p.strips = s->strips; p.runs = s->runs;
     p.row_off = s->row_off;
+    if (s->test_skip_row >= 0) { p.skip_loads = 1; p.skip_loads_from = s->test_skip_row; }
     if (push && k_out >= 0 && mode != OUT_RHS) {   // a slab's state output: edge rows to the neighbours' halos
         p.push_lo_f = s->nbf_lo[k_out]; p.push_lo_d = s->nbd_lo[k_out];
         p.push_hi_f = s->nbf_hi[k_out]; p.push_hi_d = s->nbd_hi[k_out];
@@ -1167,6 +1169,15 @@ int hype_last_elapsed_ms(const hype_solver *s, double *ms)
 {
     if (!s || !ms) return HYPE_ERR_INVALID;
     *ms = s->last_ms;
+    return HYPE_OK;
+}
+
+int hype_test_skip_row_loads(hype_solver *s, int row)
+{
+    if (!s) return HYPE_ERR_INVALID;
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));   // no captured step of the old setting is in flight
+    s->test_skip_row = row < 0 ? -1 : row;
+    if (s->step_exec) { cudaGraphExecDestroy(s->step_exec); s->step_exec = nullptr; }
     return HYPE_OK;
 }
 

@@ -68,6 +68,9 @@ struct StageParams {
     int push_shift_lo, push_shift_hi;
     long long push_plane_lo, push_plane_hi;
     double *push_lo, *push_hi;
+    // test hook (hype_test_skip_row_loads): with skip_loads set, no row load is issued for
+    // rows >= skip_loads_from, so the bounded wait on it runs out; 0 in normal operation
+    int skip_loads, skip_loads_from;
 };
 
 // Tile geometry of the stage kernel: a tile is CELLS reconstruction columns
@@ -172,6 +175,7 @@ struct MixedParams {
     long long push_plane_lo, push_plane_hi;
     float *push_lo_f, *push_hi_f;
     double *push_lo_d, *push_hi_d;
+    int skip_loads, skip_loads_from;   // test hook, as in StageParams
 };
 struct MixedMaps {
     CUtensorMap f;              // FP32 planes: (nx, ny, 4), box (cells + 8, 1, 4)

@@ -11,10 +11,18 @@
 // in one file-scope __device__ array of HYPE_NOALLOC_MAX_BYTES, which every GPU
 // that loads this library holds until the process exits.
 //
-// Set-up: the first call on a device (with that device current) looks up the
-// array's device address with cudaGetSymbolAddress -- the name is only a host
-// stand-in in host code, never a device pointer -- and caches it per device.
-// Make that first call before any stream capture.
+// Set-up: every call (with the target device current) looks up the array's
+// device address with cudaGetSymbolAddress -- the name is only a host stand-in
+// in host code, never a device pointer.  The lookup allocates nothing; doing it
+// per call rather than once means a module that was reloaded (after
+// cudaDeviceReset, or a primary context released and re-created) is never
+// addressed through a stale pointer.  The first call on a device loads the
+// module there, so make it before any stream capture.
+//
+// Stream: the work runs on the legacy default stream, which waits for and is
+// waited for by work on ordinary (blocking) streams.  A caller that produced dU
+// on a stream created with cudaStreamNonBlocking must synchronise that stream
+// (or the device) before the call.
 //
 // Sharing: every call uses the same array and it keeps the last call's
 // contents.  Each call clears the scalars that must start at zero and
@@ -24,7 +32,6 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstring>
-#include <mutex>
 #include "../../include/hype_gpu.h"
 #include "hype_internal.h"
 
@@ -37,9 +44,6 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[HYPE_NOALLOC_MAX_BYTES
 constexpr int kMaxDevices = 64;
 constexpr size_t kPlanesOffset = 256;   // DevScalars first, planes after (256-byte aligned)
 static_assert(sizeof(DevScalars) <= kPlanesOffset, "DevScalars must fit ahead of the planes");
-
-std::mutex g_setup_mutex;
-unsigned char *g_scratch_dev[kMaxDevices] = {nullptr};
 
 __global__ void noalloc_reset_kernel(DevScalars *sc)
 {
@@ -56,17 +60,13 @@ typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32
                                      const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                      CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// the scratch array's device address on `dev` (set-up on first use)
+// the scratch array's device address on the current device `dev`
 int scratch_on(int dev, unsigned char **out)
 {
     if (dev < 0 || dev >= kMaxDevices) return HYPE_ERR_INVALID;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_dev[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return HYPE_ERR_CUDA;
-        g_scratch_dev[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_scratch_dev[dev];
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return HYPE_ERR_CUDA;
+    *out = static_cast<unsigned char *>(p);
     return HYPE_OK;
 }
 

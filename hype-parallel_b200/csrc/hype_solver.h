@@ -50,6 +50,7 @@ struct hype_solver {
     long long nb_plane_lo = 0, nb_plane_hi = 0;
     int nb_shift_lo = 0, nb_shift_hi = 0;
     bool began = false;
+    int test_skip_row = -1;           // hype_test_skip_row_loads: first row whose loads are not issued (-1: off)
     double last_ms = 0.0;
     char err[512] = {0};
 };

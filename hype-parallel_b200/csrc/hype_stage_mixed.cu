@@ -260,6 +260,19 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
     float smax_loc = 0.0f;
     bool bad = false;
     unsigned bad_cell = 0xffffffffu;
+    // a bounded wait ran out: thread 0 waits for the loads in flight, then the block returns
+    // (the same as the FP64 tile, hype_stage_tile.cuh)
+    auto give_up = [&](bool orow_pending, unsigned orow_parity) {
+        if (t != 0) return;
+        raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+        const unsigned long long deadline = global_ns() + TMA_WAIT_NS;
+        bool drained = true;
+        for (int row = next_conv; row < next_issue; ++row)
+            drained = drained && mbar_wait_until(&bars[slot_of(row)], (unsigned)(((row - row_lo) / SLOTS) & 1), deadline);
+        if (orow_pending) drained = drained && mbar_wait_until(&bars[SLOTS], orow_parity, deadline);
+        if (drained)
+            for (int k = 0; k <= SLOTS; ++k) mbar_inval(&bars[k]);
+    };
 
     for (int r = y0 - 1; r <= y0 + H; ++r) {
         // this iteration finishes an owned row (r-1) with an RK combination that reads its input
@@ -267,7 +280,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         // ---------------- A. rows up to r+2: two TMA loads (FP32, FP64 planes) per row
         if (t == 0) {
             fence_proxy_async();
-            for (; next_issue <= min(r + 3, row_hi); ++next_issue) {
+            for (; next_issue <= min(r + 3, row_hi) && (!p.skip_loads || next_issue < p.skip_loads_from); ++next_issue) {
                 const int row = next_issue;
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
@@ -276,7 +289,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 tma_load_3d(rowf(row), &maps->f, xs, ty, 0, bar);
                 tma_load_3d(rowd(row), &maps->d, xs, ty, 0, bar);
             }
-            if (finish_row) {   // row r-1's stage input for the RK combination
+            if (finish_row && (!p.skip_loads || r - 1 < p.skip_loads_from)) {   // row r-1's stage input for the RK combination
                 const int ty = SLAB ? (r - 1) + p.row_off : r - 1;
                 mbar_expect_tx(&bars[SLOTS], K::F_ROW_BYTES + K::D_ROW_BYTES);
                 tma_load_3d(orow, &maps->f, xs, ty, 0, &bars[SLOTS]);
@@ -286,11 +299,9 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         for (; next_conv <= r + 2; ++next_conv) {
             const int row = next_conv;
             const unsigned parity = (unsigned)(((row - row_lo) / SLOTS) & 1);
-            bool ok = false;
-            for (long it = 0; it < (1L << 22); ++it)
-                if (mbar_try_wait(&bars[slot_of(row)], parity)) { ok = true; break; }
+            const bool ok = mbar_wait_bounded(&bars[slot_of(row)], parity);
             if (__syncthreads_or(!ok)) {
-                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                give_up(finish_row && (!p.skip_loads || r - 1 < p.skip_loads_from), (unsigned)((r - y0 - 1) & 1));
                 return;
             }
             float *rf = rowf(row);
@@ -344,11 +355,9 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         }
         if (finish_row) {   // the copy of row r-1 issued at the start of this iteration
             const unsigned parity = (unsigned)((r - y0 - 1) & 1);
-            bool ok = false;
-            for (long it = 0; it < (1L << 22); ++it)
-                if (mbar_try_wait(&bars[SLOTS], parity)) { ok = true; break; }
+            const bool ok = mbar_wait_bounded(&bars[SLOTS], parity);
             if (__syncthreads_or(!ok)) {
-                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                give_up(false, 0u);
                 return;
             }
         }

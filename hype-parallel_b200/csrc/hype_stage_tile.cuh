@@ -235,6 +235,20 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     double smax_loc = 0.0, smaxv_loc = 0.0;
     bool bad = false;
     unsigned bad_cell = 0xffffffffu;
+    // A bounded wait ran out (ERR_TMA_TIMEOUT): thread 0 waits for the loads still in
+    // flight -- ring rows issued but not yet converted, and the finish-row slot while
+    // its load is outstanding -- then invalidates the barriers; the block returns.
+    auto give_up = [&](bool orow_pending, unsigned orow_parity) {
+        if (t != 0) return;
+        raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+        const unsigned long long deadline = global_ns() + TMA_WAIT_NS;
+        bool drained = true;
+        for (int row = next_conv; row < next_issue; ++row)
+            drained = drained && mbar_wait_until(&bars[slot_of(row)], (unsigned)(((row - row_lo) / SLOTS) & 1), deadline);
+        if (orow_pending) drained = drained && mbar_wait_until(&bars[SLOTS], orow_parity, deadline);
+        if (drained)
+            for (int k = 0; k <= SLOTS; ++k) mbar_inval(&bars[k]);
+    };
 
     for (int r = y0 - 1; r <= y0 + H; ++r) {
         // this iteration finishes an owned row (r-1) with an RK combination that reads its input
@@ -242,14 +256,14 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
         // ---------------- A. bring rows up to r+2 into the ring --------------
         if (t == 0) {
             fence_proxy_async();   // earlier generic accesses to the slots precede the TMA writes
-            for (; next_issue <= min(r + 3, row_hi); ++next_issue) {
+            for (; next_issue <= min(r + 3, row_hi) && (!p.skip_loads || next_issue < p.skip_loads_from); ++next_issue) {
                 const int row = next_issue;
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::ROW_BYTES);
                 tma_load_3d(row_ptr(row), tmap, xs, src + p.row_off, 0, bar);   // the map starts row_off rows below row 0
             }
-            if (finish_row) {   // row r-1's conserved input for the RK combination in section C
+            if (finish_row && (!p.skip_loads || r - 1 < p.skip_loads_from)) {   // row r-1's conserved input for the RK combination in section C
                 mbar_expect_tx(&bars[SLOTS], K::ROW_BYTES);
                 tma_load_3d(orow_s, tmap, xs, (r - 1) + p.row_off, 0, &bars[SLOTS]);
             }
@@ -257,12 +271,9 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
         for (; next_conv <= r + 2; ++next_conv) {
             const int row = next_conv;
             const unsigned parity = (unsigned)(((row - row_lo) / SLOTS) & 1);
-            bool ok = false;
-            for (long it = 0; it < (1L << 24); ++it) {
-                if (mbar_try_wait(&bars[slot_of(row)], parity)) { ok = true; break; }
-            }
+            const bool ok = mbar_wait_bounded(&bars[slot_of(row)], parity);
             if (__syncthreads_or(!ok)) {
-                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                give_up(finish_row && (!p.skip_loads || r - 1 < p.skip_loads_from), (unsigned)((r - y0 - 1) & 1));
                 return;   // block-uniform exit; the caller's next barrier is block-uniform too
             }
             double *rp = row_ptr(row);
@@ -325,12 +336,9 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
         }
         if (finish_row) {   // the copy of row r-1 issued at the start of this iteration
             const unsigned parity = (unsigned)((r - y0 - 1) & 1);
-            bool ok = false;
-            for (long it = 0; it < (1L << 24); ++it) {
-                if (mbar_try_wait(&bars[SLOTS], parity)) { ok = true; break; }
-            }
+            const bool ok = mbar_wait_bounded(&bars[SLOTS], parity);
             if (__syncthreads_or(!ok)) {
-                if (t == 0) raise_error(p.sc, ERR_TMA_TIMEOUT, 0u);
+                give_up(false, 0u);   // the finish-row load is the one that did not come
                 return;   // block-uniform exit
             }
         }

@@ -43,6 +43,34 @@ __device__ __forceinline__ void mbar_inval(uint64_t *bar)
     asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
 
+// Bounded waits on TMA row loads.  Every mbarrier wait of the stage tiles (FP64
+// and mixed) gives up once TMA_WAIT_NS nanoseconds of the GPU's global timer have
+// passed without the load completing: the block then raises ERR_TMA_TIMEOUT (the
+// host call returns HYPE_ERR_TIMEOUT) instead of waiting for ever.  Before it
+// returns, the block waits, against one more deadline of the same length, for the
+// loads it has already issued (mbar_drain), so no copy is left writing into the
+// shared memory of a block that has exited; only if that drain also runs out does
+// it leave them.
+constexpr unsigned long long TMA_WAIT_NS = 2000000000ull;   // 2 s
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ bool mbar_wait_until(uint64_t *bar, unsigned parity, unsigned long long deadline)
+{
+    for (unsigned it = 0;; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((it & 31u) == 31u && global_ns() > deadline) return false;
+    }
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity)
+{
+    if (mbar_try_wait(bar, parity)) return true;
+    return mbar_wait_until(bar, parity, global_ns() + TMA_WAIT_NS);
+}
+
 // Ghost source index along one axis (rhs_function_prim.c:75-315 and the DMDA
 // periodic wrap): transmissive copies the edge cell, reflective mirrors; a
 // slab edge (BC_HALO) reads its halo rows as they are.

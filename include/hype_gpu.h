@@ -165,10 +165,12 @@ HYPE_API int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long 
  * about 590 x 590 cells), else HYPE_ERR_NOMEM is returned before any device
  * work.  FP64 only; periodic, reflective and transmissive boundaries only
  * (HYPE_ERR_INVALID otherwise).  Runs on the legacy default stream and returns
- * when the result is in dRHS.  The first call on a device sets up (looks up
- * the array's device address) and should come before any stream capture.
- * Calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.
+ * when the result is in dRHS; a dU written on a stream created with
+ * cudaStreamNonBlocking is not ordered before that stream, so synchronise such
+ * a stream first.  Each call looks up the array's device address (no
+ * allocation); the first call on a device loads the module there and should
+ * come before any stream capture.  Calls share the array: calls that overlap
+ * on the GPU race and must be serialised by the caller.
  */
 #define HYPE_NOALLOC_MAX_BYTES (16u * 1024u * 1024u)
 HYPE_API int hype_rhs_prim_noalloc(const hype_config *cfg, double t, const double *dU, double *dRHS, double *dt);
@@ -276,6 +278,17 @@ HYPE_API int hype_last_elapsed_ms(const hype_solver *s, double *ms);
  * every SM, best of `reps` launches timed with CUDA events.  *ops_per_s counts
  * one per multiply and one per add. */
 HYPE_API int hype_fp64_rate(int device, int reps, double *ops_per_s);
+
+/*
+ * Test hook for the error path of the bounded device waits; no counterpart in
+ * the reference.  With row >= 0 the stage kernels of this solver issue no TMA
+ * row load for rows >= row, so the wait for that row runs out (after about 2 s
+ * of GPU time per wave of blocks): the block waits for the loads it did issue,
+ * raises the timeout bit and returns, and the call reports HYPE_ERR_TIMEOUT
+ * with the context still usable.  row < 0 restores normal operation.  Waits
+ * for the solver's stream first and drops its captured step graph.
+ */
+HYPE_API int hype_test_skip_row_loads(hype_solver *s, int row);
 
 #ifdef __cplusplus
 }

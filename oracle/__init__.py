@@ -250,6 +250,26 @@ class Reference:
                                 ctypes.byref(steps), ctypes.byref(tt), ctypes.byref(dt))
         return U, steps.value, tt.value, dt.value, st
 
+    def begin(self, U: np.ndarray, t0: float, t_final: float) -> int:
+        """The time loop of solve() in chunks: loads U and seeds dt (hype.c:343)."""
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self.lib.ref_begin.argtypes = [_DP, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+        return self.lib.ref_begin(_ptr(U), t0, t_final, 0 if self._cfg.conservative else 1)
+
+    def advance(self, nsteps: int):
+        """Up to nsteps more steps of the loop begin() set up: (steps, t, dt_next, status)."""
+        self.lib.ref_advance.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_int), _DP, _DP]
+        n, tt, dt = ctypes.c_int(0), ctypes.c_double(0.0), ctypes.c_double(0.0)
+        st = self.lib.ref_advance(nsteps, ctypes.byref(n), ctypes.byref(tt), ctypes.byref(dt))
+        return n.value, tt.value, dt.value, st
+
+    def state(self) -> np.ndarray:
+        """The state of the loop begin() set up (Vec layout)."""
+        self.lib.ref_get_state.argtypes = [_DP]
+        U = np.empty(self._cfg.nx * self._cfg.ny * self._cfg.nvar, dtype=np.float64)
+        self.lib.ref_get_state(_ptr(U))
+        return U
+
 
 # ---------------------------------------------------------------------------
 # the reference as live MPI ranks
