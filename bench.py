@@ -327,6 +327,47 @@ def bn_leg(hp, args, local_rank):
     return out
 
 
+def fast_leg(hp, args, local_rank, world, U0, U_ref, n_done, value_exact, ms_stage_exact):
+    """The FP64 performance form (HYPE_PREC_FP64_FAST: fused multiply-adds, shared
+    reciprocals; within 1e-12 of the reference per RHS call, tests/test_gpu_fast.py)
+    on the same workload and step counts as the bit-exact headline: throughput, its
+    stage kernel alone against the measured FMA rate, and its state after the same
+    steps against the bit-exact state (per field, relative to the field's largest value)."""
+    cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=NX, ny=NY, cfl=0.4, device=local_rank, precision=hp.PREC_FP64_FAST)
+    with hp.Solver(cfg) as s:
+        s.set_state(U0)
+        tile = s.autotune(3) if not args.no_autotune else None
+        s.begin(0.0, 1e30, 1 << 30)
+        s.advance(max(3, args.warmup))
+        s.wait()
+        s.advance(args.steps)
+        n, t, dt, st = s.wait()
+        ms = max_over_ranks(s.last_elapsed_ms(), world)
+        U = s.get_state()
+        ms_stage = s.time_stage(20)
+        info = s.launch_info()
+    F, B = U.reshape(-1, 6), U_ref.reshape(-1, 6)
+    err = {}
+    for nm, cols in (("a1rho1", [0]), ("a2rho2", [1]), ("momentum_vector", [2, 3]), ("E", [4]), ("alpha1", [5])):
+        d = np.sqrt(((F[:, cols] - B[:, cols]) ** 2).sum(axis=1)).max()
+        err[nm] = float(d / np.sqrt((B[:, cols] ** 2).sum(axis=1)).max())
+    fma_peak = hp.fp64_fma_rate(local_rank, 5)
+    v = replica_throughput(world, NX * NY, args.steps, ms)
+    return {"value": v, "unit": UNIT, "ms_per_step": ms / args.steps, "status": st, "steps_done": n,
+            "speedup_vs_bitexact": v / value_exact, "stage_ms_per_launch": ms_stage,
+            "stage_speedup_vs_bitexact": ms_stage_exact / ms_stage, "autotuned_tile": tile, "launch": info,
+            "fp64": {"achieved_tflops_stage": RHS_FLOPS_2048 / (ms_stage * 1e-3) / 1e12,
+                     "peak_tflops_fma": fma_peak / 1e12,
+                     "frac_stage": RHS_FLOPS_2048 / (ms_stage * 1e-3) / fma_peak,
+                     "peak_source": "hype_fp64_fma_rate: independent FP64 fused multiply-add chains on every SM, 2 FLOPs each, "
+                                    "best of 5 launches",
+                     "flops": "the reference's operation count (4784.5 per cell-RHS), not the fused instruction count"},
+            "state_vs_bitexact_after_run": {"steps": n_done, "fields_rel_Linf": err,
+                                            "norm": "max over cells of the difference / max over cells of the bit-exact "
+                                                    "field (momentum: Euclidean norm per cell)"},
+            "correctness": "within 1e-12 relative L-infinity of the reference per RHS call (tests/test_gpu_fast.py)"}
+
+
 def group_leg(hp, args, local_rank, U0, U_ref):
     """The FP64 workload as y-slabs on this GPU (hype_group): the cost of the
     decomposition (halo rows stored by the stage kernels into the neighbours,
@@ -567,6 +608,7 @@ def run_gpu(args, rank, world, local_rank):
                  "rel_error_vs_fp64_after_run": {"fields_L1_Linf": errs, "steps": err_steps},
                  "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt"}
 
+    fast = None if args.no_fast else fast_leg(hp, args, local_rank, world, U0, U_fp64, n_done, value, ms_stage)
     group = None if args.group_slabs <= 1 else group_leg(hp, args, local_rank, U0, U_fp64)
     bn = None if args.no_bn else bn_leg(hp, args, local_rank)
     batched = None if args.no_batch else batch_leg(hp, args, local_rank)
@@ -602,7 +644,8 @@ def run_gpu(args, rank, world, local_rank):
             "gpu_launches": args.steps * 6,
             "clocks": clk.summary(),
             "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2},
-            "forms": {"mixed": mixed, "bn1024": bn, "batched": batched, "serving": serving, "y_slabs": group}}
+            "forms": {"fp64_fast": fast, "mixed": mixed, "bn1024": bn, "batched": batched, "serving": serving,
+                      "y_slabs": group}}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -619,6 +662,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default stage tile shape")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision leg")
+    ap.add_argument("--no-fast", action="store_true", help="skip the FP64 performance-form leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-grids leg")
     ap.add_argument("--no-bn", action="store_true", help="skip the Baer-Nunziato 1024^2 leg")
     ap.add_argument("--error-steps", type=int, default=500,

@@ -28,7 +28,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libhype_b200.so")
 OK, ERR_INVALID, ERR_CUDA, ERR_INADMISSIBLE, ERR_TIMEOUT, ERR_NOMEM, ERR_NO_DEVICE, ERR_BUSY = range(8)
 EULER, KAPILA_5EQN, BAER_NUNZIATO = 0, 1, 2
 BC_WALL, BC_INLET, BC_PERIODIC, BC_REFLECTIVE, BC_TRANSMISSIVE = 0, 1, 2, 3, 4
-PREC_FP64, PREC_MIXED = 0, 1
+PREC_FP64, PREC_MIXED, PREC_FP64_FAST = 0, 1, 2
 FLAG_BN_FIX_P2 = 1
 FLAG_CONSERVATIVE = 2
 FLAG_VISCOUS = 4
@@ -161,11 +161,13 @@ def lib() -> ctypes.CDLL:
         L.hype_launch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3 + [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
         L.hype_last_elapsed_ms.argtypes = [vp, _DP]
         L.hype_test_skip_row_loads.argtypes = [vp, ctypes.c_int]
+        L.hype_test_fast_rcp.argtypes = [ctypes.c_int, _DP, ctypes.c_int, _DP, _DP]
         L.hype_time_stage.argtypes = [vp, ctypes.c_int, _DP]
         L.hype_autotune.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
         L.hype_config_default.argtypes = [ctypes.POINTER(_Cfg)]
         L.hype_get_primitive.argtypes = [vp, _DP]
         L.hype_fp64_rate.argtypes = [ctypes.c_int, ctypes.c_int, _DP]
+        L.hype_fp64_fma_rate.argtypes = [ctypes.c_int, ctypes.c_int, _DP]
         L.hype_group_create.argtypes = [ctypes.POINTER(_Cfg), ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(vp)]
         L.hype_group_destroy.argtypes = [vp]
         L.hype_group_last_error.argtypes = [vp]
@@ -422,6 +424,17 @@ class Solver:
         self._check(lib().hype_test_skip_row_loads(self._h, row))
 
 
+def test_fast_rcp(x: np.ndarray, device: int = 0):
+    """The FP64 performance form's reciprocal and IEEE 1/x of the same values on
+    the GPU (hype_test_fast_rcp): returns (fast, ieee)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    fast, ieee = np.empty_like(x), np.empty_like(x)
+    st = lib().hype_test_fast_rcp(device, _ptr(x), x.size, _ptr(fast), _ptr(ieee))
+    if st != OK:
+        raise HypeError(st, "hype_test_fast_rcp failed")
+    return fast, ieee
+
+
 def fp64_rate(device: int = 0, reps: int = 5) -> float:
     """Measured rate of separately rounded FP64 multiplies and adds on `device`
     (hype_fp64_rate): the FP64 roofline of the bit-exact kernels, in ops/s."""
@@ -429,6 +442,16 @@ def fp64_rate(device: int = 0, reps: int = 5) -> float:
     st = lib().hype_fp64_rate(device, reps, ctypes.byref(r))
     if st != OK:
         raise HypeError(st, lib().hype_status_string(st).decode())
+    return r.value
+
+
+def fp64_fma_rate(device: int = 0, reps: int = 5) -> float:
+    """Measured FP64 rate with fused multiply-adds (hype_fp64_fma_rate), FLOP/s
+    counting two per FMA: the FP64 roofline of the performance form."""
+    r = ctypes.c_double(0.0)
+    st = lib().hype_fp64_fma_rate(device, reps, ctypes.byref(r))
+    if st != OK:
+        raise HypeError(st, "hype_fp64_fma_rate failed")
     return r.value
 
 

@@ -146,6 +146,7 @@ static StageParams base_params(const hype_solver *s)
     p.bc[0] = s->cfg.bc_left; p.bc[1] = s->cfg.bc_right; p.bc[2] = s->cfg.bc_bottom; p.bc[3] = s->cfg.bc_top;
     p.eos.g1 = s->cfg.gamma1; p.eos.g2 = s->cfg.gamma2; p.eos.pi1 = s->cfg.pi1; p.eos.pi2 = s->cfg.pi2;
     p.eos.fix_p2 = (s->cfg.flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
+    p.eos.derive();
     p.r1_h = s->r1_h;
     p.cfl_h = s->cfl_h;
     p.mu1 = s->cfg.mu1;
@@ -206,6 +207,9 @@ static int set_tiling(hype_solver *s, int cells, int waves = 1)
         s->cells = cells;
         CUDA_TRY(s, stage_cons_configure(cfg->system, cfg->order));
         s->bps = stage_cons_blocks_per_sm(cfg->system, cfg->order);
+    } else if (s->fast) {
+        CUDA_TRY(s, stage_fast_configure(cfg->system, cfg->order, cells));
+        s->bps = stage_fast_blocks_per_sm(cfg->system, cfg->order, cells);
     } else {
         CUDA_TRY(s, stage_configure(cfg->system, cfg->order, cells));
         s->bps = stage_blocks_per_sm(cfg->system, cfg->order, cells);
@@ -246,6 +250,7 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
     if (s->cfg.flags & HYPE_FLAG_VISCOUS)
         return launch_stage_visc(s->cfg.order, (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) != 0, tmap_for(s, in), p, s->stream);
     if (s->cfg.flags & HYPE_FLAG_CONSERVATIVE) return launch_stage_cons(s->cfg.system, s->cfg.order, tmap_for(s, in), p, s->stream);
+    if (s->fast) return launch_stage_fast(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
     return launch_stage(s->cfg.system, s->cfg.order, s->cells, tmap_for(s, in), p, s->stream);
 }
 
@@ -357,8 +362,10 @@ static int check_config(const hype_config *c, hype_solver *s)
     if ((c->bc_left == HYPE_BC_PERIODIC) != (c->bc_right == HYPE_BC_PERIODIC) ||
         (c->bc_bottom == HYPE_BC_PERIODIC) != (c->bc_top == HYPE_BC_PERIODIC))
         return fail(s, HYPE_ERR_INVALID, "periodic boundaries must be set on both sides of an axis");
-    if (c->precision != HYPE_PREC_FP64 && c->precision != HYPE_PREC_MIXED)
+    if (c->precision != HYPE_PREC_FP64 && c->precision != HYPE_PREC_MIXED && c->precision != HYPE_PREC_FP64_FAST)
         return fail(s, HYPE_ERR_INVALID, "unknown precision %d", c->precision);
+    if (c->precision == HYPE_PREC_FP64_FAST && (c->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS)))
+        return fail(s, HYPE_ERR_INVALID, "the FP64 performance form covers the primitive-variable inviscid path");
     if (c->precision == HYPE_PREC_MIXED && c->system != HYPE_KAPILA_5EQN)
         return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for the Kapila system");
     if (c->precision == HYPE_PREC_MIXED && (c->order != 2 || c->bc_left == HYPE_BC_INLET))
@@ -575,6 +582,7 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     CUDA_TRY(s, cudaGetDeviceProperties(&prop, cfg->device));
     if (prop.major != 10) return fail(s, HYPE_ERR_NO_DEVICE, "device %d is sm_%d%d; the library is built for sm_100a", cfg->device, prop.major, prop.minor);
     s->mixed = cfg->precision == HYPE_PREC_MIXED;
+    s->fast = cfg->precision == HYPE_PREC_FP64_FAST;
 
     s->nv = hype_nvar(cfg->system);
     s->pitch = s->mixed ? ((cfg->nx + 31) & ~31) : ((cfg->nx + 15) & ~15);   // 128-byte rows

@@ -306,11 +306,13 @@ cudaError_t launch_totals(const double *planes, double *red, int nx, int ny, int
 
 // ---------------------------------------------------------------------------
 // FP64 rate: 8 independent chains x = x*m + c per thread, which --fmad=false
-// keeps as one multiply and one add each.  The data-dependent store keeps the
-// chains alive; it never fires for these constants.
+// keeps as one multiply and one add each (FUSED: one explicit fused multiply-add,
+// two FLOPs).  The data-dependent store keeps the chains alive; it never fires
+// for these constants.
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int RATE_CHAINS = 8;
+template <bool FUSED>
 __global__ void __launch_bounds__(256) fp64_rate_kernel(double *sink, int iters, double seed)
 {
     double x[RATE_CHAINS];
@@ -319,16 +321,16 @@ __global__ void __launch_bounds__(256) fp64_rate_kernel(double *sink, int iters,
     const double m = 0.999999999, c = 1e-9;
     for (int it = 0; it < iters; ++it) {
 #pragma unroll
-        for (int k = 0; k < RATE_CHAINS; ++k) x[k] = x[k] * m + c;
+        for (int k = 0; k < RATE_CHAINS; ++k) x[k] = FUSED ? fma(x[k], m, c) : x[k] * m + c;
     }
     double s = 0.0;
 #pragma unroll
     for (int k = 0; k < RATE_CHAINS; ++k) s += x[k];
     if (s == -1.0) sink[0] = s;
 }
-}  // namespace
 
-extern "C" int hype_fp64_rate(int device, int reps, double *ops_per_s)
+// best of `reps` timed launches (one warm-up launch first); 2 operations per chain link
+int fp64_rate_of(bool fused, int device, int reps, double *ops_per_s)
 {
     if (!ops_per_s || reps < 1) return HYPE_ERR_INVALID;
     int ndev = 0;
@@ -344,11 +346,12 @@ extern "C" int hype_fp64_rate(int device, int reps, double *ops_per_s)
     if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
         cudaEventCreate(&e1) != cudaSuccess)
         rc = HYPE_ERR_CUDA;
-    const int blocks = sms * 8, threads = 256, iters = 4096;
+    const int blocks = sms * 8, threads = 256, iters = fused ? 8192 : 4096;
     double best = 0.0;
     for (int r = 0; r <= reps && rc == HYPE_OK; ++r) {   // launch 0 warms up
         cudaEventRecord(e0, st);
-        fp64_rate_kernel<<<blocks, threads, 0, st>>>(sink, iters, 1.0 + r);
+        if (fused) fp64_rate_kernel<true><<<blocks, threads, 0, st>>>(sink, iters, 1.0 + r);
+        else fp64_rate_kernel<false><<<blocks, threads, 0, st>>>(sink, iters, 1.0 + r);
         cudaEventRecord(e1, st);
         if (cudaEventSynchronize(e1) != cudaSuccess || cudaGetLastError() != cudaSuccess) { rc = HYPE_ERR_CUDA; break; }
         float ms = 0.f;
@@ -363,3 +366,7 @@ extern "C" int hype_fp64_rate(int device, int reps, double *ops_per_s)
     *ops_per_s = best;
     return rc;
 }
+}  // namespace
+
+extern "C" int hype_fp64_rate(int device, int reps, double *ops_per_s) { return fp64_rate_of(false, device, reps, ops_per_s); }
+extern "C" int hype_fp64_fma_rate(int device, int reps, double *flops_per_s) { return fp64_rate_of(true, device, reps, flops_per_s); }

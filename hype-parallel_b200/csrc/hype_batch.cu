@@ -633,6 +633,8 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     char msg[256];
     int rc = validate_config(cfg, msg, sizeof(msg));
     if (rc) return bfail(b, rc, "%s", msg);
+    if (cfg->precision == HYPE_PREC_FP64_FAST)
+        return bfail(b, HYPE_ERR_INVALID, "the FP64 performance form runs in single solvers and slab groups, not in batches");
     if ((long long)cfg->nx * cfg->ny > b->cfg.max_cells)
         return bfail(b, HYPE_ERR_INVALID, "grid %dx%d exceeds the batch's max_cells (%lld)", cfg->nx, cfg->ny, (long long)b->cfg.max_cells);
     int s = -1;

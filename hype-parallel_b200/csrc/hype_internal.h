@@ -88,6 +88,10 @@ int stage_batch_blocks_per_sm(int sys, int order, int cells);   // resident bloc
 cudaError_t launch_stage(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 cudaError_t launch_stage_batch(int sys, int order, int cells, const StageParams *inst, const CUtensorMap *tmaps,
                                const int2 *work, int *sched, int blocks, cudaStream_t s);
+// the FP64 performance form (primitive path, HYPE_PREC_FP64_FAST): grid form, 64- or 128-column tiles
+cudaError_t stage_fast_configure(int sys, int order, int cells);
+int stage_fast_blocks_per_sm(int sys, int order, int cells);
+cudaError_t launch_stage_fast(int sys, int order, int cells, const CUtensorMap &tmap, const StageParams &p, cudaStream_t s);
 // the VISCOUS build (Kapila, N = 1..3, primitive or conservative): 128-column tiles, grid form
 cudaError_t stage_visc_configure(int order, bool cons);
 int stage_visc_blocks_per_sm(int order, bool cons);

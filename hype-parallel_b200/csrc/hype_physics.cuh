@@ -27,6 +27,21 @@ enum : unsigned { ERR_INADMISSIBLE_FACE = 1u, ERR_NONFINITE = 2u, ERR_TMA_TIMEOU
 struct Eos {
     double g1, g2, pi1, pi2;
     int fix_p2;   // Baer-Nunziato: 0 = flux pressure of phase 2 read from V[8] as baer_nunziato.c:271 does
+    // constants the FP64 performance form (hype_physics_fast.cuh) reads instead of
+    // dividing by them; filled by derive() at the start of each of its tiles
+    double g1m1, g2m1, inv_g1m1, inv_g2m1, inv_g12, g1pi1, g2pi2, c1, c2;
+    __host__ __device__ void derive()
+    {
+        g1m1 = g1 - 1.0;
+        g2m1 = g2 - 1.0;
+        inv_g1m1 = 1.0 / g1m1;
+        inv_g2m1 = 1.0 / g2m1;
+        inv_g12 = 1.0 / (g1m1 * g2m1);
+        g1pi1 = g1 * pi1;
+        g2pi2 = g2 * pi2;
+        c1 = g1pi1 * g2m1;   // alpha_1 gamma_1 pi_1 (gamma_2 - 1) per unit alpha_1 (kapila_5eqn.c:27)
+        c2 = g2pi2 * g1m1;
+    }
 };
 
 // HyPE-2D/hype.h:50-62

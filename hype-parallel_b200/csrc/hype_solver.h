@@ -36,6 +36,7 @@ struct hype_solver {
     int bps = 0;                      // stage blocks per SM
     // mixed precision (Kapila N=2): state k = 0 (U), 1 (S0), 2 (S1) as FP32 + FP64 planes
     bool mixed = false;
+    bool fast = false;                // FP64 performance form (HYPE_PREC_FP64_FAST)
     float *mf[3] = {nullptr, nullptr, nullptr};
     double *md[3] = {nullptr, nullptr, nullptr};
     hype::MixedMaps mm[3];

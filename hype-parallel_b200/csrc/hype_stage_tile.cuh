@@ -29,6 +29,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include "hype_internal.h"
+#include "hype_physics_fast.cuh"
 #include "hype_tma.cuh"
 
 namespace hype {
@@ -114,11 +115,11 @@ __device__ __forceinline__ double face_grad(const double *uc, int q)
 
 // one face Gauss point with n = e_x (DIR 0) or e_y (DIR 1): riemann.c:112-140
 // (RiemannSolverPrim, VL/VR primitive) or, for the conservative path,
-// riemann.c:52-105 (RiemannSolver, VL/VR conserved)
-template <int SYS, int DIR, bool CONS>
+// riemann.c:52-105 (RiemannSolver, VL/VR conserved); S is the system's physics
+// (System<SYS>, or FastSystem<SYS> for the FP64 performance form)
+template <class S, int DIR, bool CONS>
 __device__ __forceinline__ double riemann_gp(const Eos &eos, const double *VL, const double *VR, double *F, double *D, bool &bad)
 {
-    using S = System<SYS>;
     constexpr int NV = S::NV;
     constexpr double nx = DIR == 0 ? 1.0 : 0.0, ny = DIR == 0 ? 0.0 : 1.0;
     if constexpr (CONS) {
@@ -165,12 +166,16 @@ __device__ __forceinline__ double riemann_gp(const Eos &eos, const double *VL, c
 // viscous fluxes (riemann.c:146-186) with gradients taken from the unlimited
 // coefficients (rhs_function_prim.c:356-374), and the viscous eigenvalue
 // maximum goes to DevScalars.smax_v for the dt (rhs_function_prim.c:617).
-template <int SYS, int N, int CELLS_, bool CONS, bool VISC = false>
+// FAST: the FP64 performance form (primitive path only): FastSystem / ReconFast
+// of hype_physics_fast.cuh, in a translation unit built with FMA contraction;
+// reads the derived constants of p.eos (Eos::derive, filled by the host).
+template <int SYS, int N, int CELLS_, bool CONS, bool VISC = false, bool FAST = false>
 __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorMap *tmap, int strip, int run,
                                            unsigned char *smem_raw, double *red_s)
 {
+    static_assert(!(FAST && (CONS || VISC)), "the FP64 performance form covers the primitive inviscid path");
     using K = StageKernel<SYS, N, CELLS_>;
-    using S = typename K::S;
+    using S = std::conditional_t<FAST, FastSystem<SYS>, typename K::S>;
     using QD = typename K::QD;
     constexpr int NV = K::NV, CELLS = K::CELLS, BW = K::BW, SLOTS = K::SLOTS, NDOF = K::NDOF;
     constexpr int NFGP = QD::NFGP, NVGP = QD::NVGP, NNODE = QD::NNODE;
@@ -215,6 +220,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
     const int bcL = p.bc[0], bcR = p.bc[1], bcB = p.bc[2], bcT = p.bc[3];
     const bool py = (bcB == BC_PERIODIC || bcT == BC_PERIODIC);
     const double dt = (p.mode == OUT_RHS) ? 0.0 : p.sc->dt;
+    const double b = dt / p.kb;   // the RK combination's dt/kb, the same for every row
     const Eos eos = p.eos;
     const double r1_h = p.r1_h;
 
@@ -359,7 +365,8 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 st.ym2 = w_m2[c * BW + ccm]; st.ym1 = w_m1[c * BW + ccm]; st.yp1 = w_p1[c * BW + ccm]; st.yp2 = w_p2[c * BW + ccm];
                 st.pp = w_p1[c * BW + ccm + 1]; st.pm = w_m1[c * BW + ccm + 1]; st.mp = w_p1[c * BW + ccm - 1]; st.mm = w_m1[c * BW + ccm - 1];
                 double cf[NDOF];
-                Recon<N>::run(st, cf);
+                if constexpr (FAST) ReconFast<N>::run(st, cf);
+                else Recon<N>::run(st, cf);
 #pragma unroll
                 for (int k = 1; k < NDOF; ++k) coef_s[cidx(k - 1, c, m)] = cf[k];
             }
@@ -455,7 +462,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     VR[c] = face_val<N, 2>(cf, q);
                     VL[c] = yt_s[(q * NV + c) * CELLS + m];
                 }
-                const double s = riemann_gp<SYS, 1, CONS>(eos, VL, VR, Fq, Dq, bad);
+                const double s = riemann_gp<S, 1, CONS>(eos, VL, VR, Fq, Dq, bad);
                 smax_loc = fmax(smax_loc, s);
 #pragma unroll
                 for (int c = 0; c < NV; ++c) { Fq[c] = QD::wf(0) * Fq[c]; Dq[c] = QD::wf(0) * Dq[c]; }
@@ -516,7 +523,6 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     // row r-1: rhs = ncp + ((-1/h) X - (1/h) Y)  (rhs_function_prim.c:589-602), then the RK combination
                     const int jo = r - 1;
                     const size_t gidx = (size_t)jo * p.pitch + i;
-                    const double b = dt / p.kb;
 #pragma unroll
                     for (int c = 0; c < NV; ++c) {
                         if ((c & 1) != h) continue;
@@ -666,7 +672,7 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     VL[c] = face_val<N, 1>(cl, q);
                     VR[c] = face_val<N, 0>(cr, q);
                 }
-                const double s = riemann_gp<SYS, 0, CONS>(eos, VL, VR, Fq, Dq, bad);
+                const double s = riemann_gp<S, 0, CONS>(eos, VL, VR, Fq, Dq, bad);
                 smax_loc = fmax(smax_loc, s);
 #pragma unroll
                 for (int c = 0; c < NV; ++c) { Fq[c] = QD::wf(0) * Fq[c]; Dq[c] = QD::wf(0) * Dq[c]; }

@@ -58,6 +58,11 @@ extern "C" {
 /* ---- arithmetic ---------------------------------------------------------- */
 #define HYPE_PREC_FP64   0    /* bit-compatible with the reference's C          */
 #define HYPE_PREC_MIXED  1    /* FP32 state/reconstruction/flux, FP64 EOS and totals */
+#define HYPE_PREC_FP64_FAST 2 /* FP64 with fused multiply-adds and shared reciprocals:
+                                 within 1e-12 relative L-infinity (per field, of the
+                                 field's largest value) of the reference per RHS call;
+                                 primitive inviscid path (no HYPE_FLAG_CONSERVATIVE or
+                                 HYPE_FLAG_VISCOUS), single solvers and slab groups    */
 
 /* ---- flags --------------------------------------------------------------- */
 #define HYPE_FLAG_BN_FIX_P2   1u  /* Baer-Nunziato: take the phase-2 flux pressure from V[7]
@@ -278,6 +283,11 @@ HYPE_API int hype_last_elapsed_ms(const hype_solver *s, double *ms);
  * every SM, best of `reps` launches timed with CUDA events.  *ops_per_s counts
  * one per multiply and one per add. */
 HYPE_API int hype_fp64_rate(int device, int reps, double *ops_per_s);
+
+/* The FP64 roofline of the performance form (HYPE_PREC_FP64_FAST), which fuses
+ * multiplies and adds: the same measurement with one fused multiply-add per
+ * chain link, counted as two FLOPs. */
+HYPE_API int hype_fp64_fma_rate(int device, int reps, double *flops_per_s);
 
 /*
  * Test hook for the error path of the bounded device waits; no counterpart in
