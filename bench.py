@@ -541,6 +541,7 @@ def run_gpu(args, rank, world, local_rank):
     # measured rate of separately rounded FP64 multiplies and adds
     flops_cu = 4 * RHS_FLOPS_2048 / (NX * NY) + RK_FLOPS_PER_CELL
     fp64_peak = hp.fp64_rate(local_rank, 5)
+    stage_flops = RHS_FLOPS_2048 + 12 * cells   # one stage: an RHS plus the AXPY combination (1 mul + 1 add per field)
     fp64 = {"flops_per_cell_update": flops_cu, "achieved_tflops": value / world * flops_cu / 1e12,
             "peak_tflops": fp64_peak / 1e12, "frac": (value / world * flops_cu) / fp64_peak,
             "stage_kernel_frac": (NX * NY * RHS_FLOPS_2048 / (NX * NY) / (ms_stage * 1e-3)) / fp64_peak,
@@ -633,11 +634,19 @@ def run_gpu(args, rank, world, local_rank):
             "config": {"workload": "kapila5-shock-bubble-2048x2048-fp64-weno3-ssprk43", "grid": f"{NX}x{NY}",
                        "system": "kapila5", "order": 2, "bubbles": NBUB, "cfl": 0.4, "precision": "fp64-bitexact",
                        "parallelism": f"replicas{world}", "l2": "state 201 MB per buffer > 126 MB L2 (no flush needed)"},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "roofline": {"bound": "fp64", "achieved": stage_flops / (ms_stage * 1e-3) / 1e12, "peak": fp64_peak / 1e12,
+                         "unit": "TFLOP/s", "frac": stage_flops / (ms_stage * 1e-3) / fp64_peak,
                          "traffic": STAGE_TRAFFIC_BYTES, "traffic_source": "one ncu capture of the stage kernel (profiles/)",
-                         "algorithmic_bytes": alg_bytes_launch, "peak_source": peak_src, "fp64": fp64,
-                         "note": "stage kernel alone: 96 B/cell algorithmic (one FP64 state read + one write) per launch; "
-                                 "the kernel is FP64-pipe bound, see profiles/"},
+                         "algorithmic_flops": stage_flops,
+                         "peak_source": "measured in this run: hype_fp64_rate, independent FP64 multiply and add chains on "
+                                        "every SM without FMA (the bit-exact kernel's instruction mix), best of 5 launches",
+                         "hbm": {"achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                                 "algorithmic_bytes": alg_bytes_launch, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({peak_src})"},
+                         "step": fp64,
+                         "note": "stage kernel alone, one SSPRK(4,3) stage of 2048^2 cells per launch: the reference's "
+                                 "operation count (4784.5 per cell-RHS, oracle/flops.cpp, plus 12 for the stage combination) "
+                                 "over the CUDA-event time; 96 B/cell algorithmic HBM bytes per launch (one FP64 state read + "
+                                 "one write).  The kernel is FP64-pipe bound (profiles/stage_kernel_kapila2048_fp64.md)"},
             "stage_kernel": {"ms_per_launch": ms_stage, "launch": info, "autotuned_tile": tile},
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -263,6 +263,25 @@ class Reference:
         st = self.lib.ref_advance(nsteps, ctypes.byref(n), ctypes.byref(tt), ctypes.byref(dt))
         return n.value, tt.value, dt.value, st
 
+    def set_output(self, write_interval: int, restart_interval: int) -> None:
+        """The output schedule of the reference's MonitorFunction (post_process.c:12-64),
+        written in the current directory during solve(); 0 turns a kind off."""
+        self.lib.ref_set_output.argtypes = [ctypes.c_int, ctypes.c_int]
+        self.lib.ref_set_output(write_interval, restart_interval)
+
+    def write_final(self, steps: int) -> int:
+        """hype.c:389-400: sol-<steps>.vts of the state the last solve() left, in the
+        current directory."""
+        self.lib.ref_write_final.argtypes = [ctypes.c_int]
+        return self.lib.ref_write_final(steps)
+
+    def load_restart(self):
+        """hype.c:316-325: (state, status) read by VecLoad from restart1.bin in the
+        current directory."""
+        self.lib.ref_load_restart.argtypes = [_DP]
+        U = np.empty(self._cfg.nx * self._cfg.ny * self._cfg.nvar, dtype=np.float64)
+        return U, self.lib.ref_load_restart(_ptr(U))
+
     def state(self) -> np.ndarray:
         """The state of the loop begin() set up (Vec layout)."""
         self.lib.ref_get_state.argtypes = [_DP]

@@ -208,7 +208,7 @@ PetscErrorCode VecNorm(Vec x, NormType t, PetscReal *out)
     *out = r;
     return 0;
 }
-PetscErrorCode VecView(Vec x, PetscViewer v) { (void)x; (void)v; return 0; }
+PetscErrorCode VecView(Vec x, PetscViewer v);   /* binary viewers: below, with the viewers */
 PetscErrorCode VecGetArray(Vec x, PetscScalar **a) { *a = x->a; return 0; }
 PetscErrorCode VecRestoreArray(Vec x, PetscScalar **a) { (void)x; *a = NULL; return 0; }
 PetscErrorCode VecGetArrayRead(Vec x, const PetscScalar **a) { *a = x->a; return 0; }
@@ -606,8 +606,126 @@ PetscErrorCode PetscTime(PetscLogDouble *t)
     *t = (PetscLogDouble)ts.tv_sec + 1e-9 * (PetscLogDouble)ts.tv_nsec;
     return 0;
 }
-struct _p_PetscViewer { int dummy; };
-static struct _p_PetscViewer g_null_viewer;
-PetscErrorCode PetscViewerVTKOpen(MPI_Comm c, const char *name, PetscFileMode m, PetscViewer *v) { (void)c; (void)name; (void)m; *v = &g_null_viewer; return 0; }
-PetscErrorCode PetscViewerBinaryOpen(MPI_Comm c, const char *name, PetscFileMode m, PetscViewer *v) { (void)c; (void)name; (void)m; *v = &g_null_viewer; return 0; }
-PetscErrorCode PetscViewerDestroy(PetscViewer *v) { if (v) *v = NULL; return 0; }
+/* Viewers.  A binary viewer follows PETSc's published binary format: VecView
+ * writes the Vec class id 1211214 and the global length as big-endian 32-bit
+ * integers, then the values as big-endian IEEE doubles in the DMDA's natural
+ * (row-major, component-interleaved) order, and records "-vecload_block_size
+ * <dof>" in the companion file <name>.info for a block size above 1; VecLoad
+ * reads that layout back.  With live ranks every rank passes its block through
+ * the exchange copy and rank 0 writes the file; on load every rank reads its own
+ * block.
+ * A VTK viewer does not restate PETSc's XML framing: VecView on it writes the
+ * viewed Vec's values as raw little-endian doubles in natural order to the
+ * viewer's file name, which is what a test compares with the data arrays of a
+ * .vts file (DMView on it is a no-op). */
+enum { VIEWER_NULL = 0, VIEWER_BINARY = 1, VIEWER_VTK = 2 };
+struct _p_PetscViewer { int kind; FILE *f; FILE *info; int writing; char name[4096]; };
+#define VEC_FILE_CLASSID 1211214
+
+PetscErrorCode PetscViewerVTKOpen(MPI_Comm c, const char *name, PetscFileMode m, PetscViewer *v)
+{
+    (void)c; (void)m;
+    PetscViewer b = (PetscViewer)calloc(1, sizeof(*b));
+    b->kind = VIEWER_VTK;
+    b->writing = 1;
+    snprintf(b->name, sizeof(b->name), "%s", name);
+    *v = b;
+    return 0;
+}
+PetscErrorCode PetscViewerBinaryOpen(MPI_Comm c, const char *name, PetscFileMode m, PetscViewer *v)
+{
+    (void)c;
+    PetscViewer b = (PetscViewer)calloc(1, sizeof(*b));
+    b->kind = VIEWER_BINARY;
+    b->writing = (m != FILE_MODE_READ);
+    if (!g_live || g_live_rank == 0 || !b->writing) {
+        b->f = fopen(name, b->writing ? "wb" : "rb");
+        if (!b->f) { free(b); *v = NULL; return 1; }
+        if (b->writing) {
+            char info[4096];
+            snprintf(info, sizeof(info), "%s.info", name);
+            b->info = fopen(info, "w");
+        }
+    }
+    *v = b;
+    return 0;
+}
+PetscErrorCode PetscViewerDestroy(PetscViewer *v)
+{
+    if (v && *v && (*v)->kind != VIEWER_NULL) {
+        if ((*v)->f) fclose((*v)->f);
+        if ((*v)->info) fclose((*v)->info);
+        free(*v);
+    }
+    if (v) *v = NULL;
+    return 0;
+}
+
+static void be32_put(unsigned char *p, unsigned u) { p[0] = u >> 24; p[1] = u >> 16; p[2] = u >> 8; p[3] = u; }
+static unsigned be32_get(const unsigned char *p) { return ((unsigned)p[0] << 24) | ((unsigned)p[1] << 16) | ((unsigned)p[2] << 8) | p[3]; }
+static void be64_put(unsigned char *p, double d)
+{
+    unsigned long long u; memcpy(&u, &d, 8);
+    for (int k = 0; k < 8; ++k) p[k] = (unsigned char)(u >> (56 - 8 * k));
+}
+static double be64_get(const unsigned char *p)
+{
+    unsigned long long u = 0;
+    for (int k = 0; k < 8; ++k) u = (u << 8) | p[k];
+    double d; memcpy(&d, &u, 8);
+    return d;
+}
+
+PetscErrorCode VecView(Vec x, PetscViewer v)
+{
+    if (!v || v->kind == VIEWER_NULL || !v->writing) return 0;
+    DM da = x->dm;
+    const PetscInt dof = da->dof;
+    const size_t n = (size_t)da->M * da->N * dof;
+    const PetscScalar *full = x->a;
+    if (g_live) {   /* gather the blocks in natural order through the exchange copy */
+        for (PetscInt j = da->ys; j < da->ys + da->ym; ++j)
+            memcpy(g_live_exch + ((size_t)j * da->M + da->xs) * dof, x->a + (size_t)(j - da->ys) * da->xm * dof,
+                   (size_t)da->xm * dof * sizeof(PetscScalar));
+        live_barrier();
+        full = g_live_exch;
+    }
+    int rc = 0;
+    if (v->kind == VIEWER_VTK) {
+        if (!g_live || g_live_rank == 0) {
+            FILE *f = fopen(v->name, "wb");
+            if (!f || fwrite(full, sizeof(PetscScalar), n, f) != n) rc = 1;
+            if (f) fclose(f);
+        }
+    } else if (v->f) {
+        unsigned char head[8];
+        be32_put(head, VEC_FILE_CLASSID);
+        be32_put(head + 4, (unsigned)n);
+        unsigned char *body = (unsigned char *)malloc(n * 8);
+        for (size_t k = 0; k < n; ++k) be64_put(body + 8 * k, full[k]);
+        if (fwrite(head, 1, 8, v->f) != 8 || fwrite(body, 1, n * 8, v->f) != n * 8) rc = 1;
+        free(body);
+        if (v->info && dof > 1) fprintf(v->info, "-vecload_block_size %d\n", dof);
+    }
+    if (g_live) live_barrier();   /* rank 0 has written before the copy is reused */
+    return rc;
+}
+
+PetscErrorCode VecLoad(Vec x, PetscViewer v)
+{
+    if (!v || v->kind != VIEWER_BINARY || v->writing || !v->f) return 1;
+    DM da = x->dm;
+    const PetscInt dof = da->dof;
+    const size_t n = (size_t)da->M * da->N * dof;
+    unsigned char head[8];
+    if (fread(head, 1, 8, v->f) != 8 || be32_get(head) != VEC_FILE_CLASSID || be32_get(head + 4) != (unsigned)n) return 1;
+    unsigned char *body = (unsigned char *)malloc(n * 8);
+    const int ok = fread(body, 1, n * 8, v->f) == n * 8;
+    if (ok)
+        for (PetscInt j = da->ys; j < da->ys + da->ym; ++j)
+            for (PetscInt i = da->xs; i < da->xs + da->xm; ++i)
+                for (PetscInt c = 0; c < dof; ++c)
+                    x->a[((size_t)(j - da->ys) * da->xm + (i - da->xs)) * dof + c] = be64_get(body + 8 * (((size_t)j * da->M + i) * dof + c));
+    free(body);
+    return ok ? 0 : 1;
+}

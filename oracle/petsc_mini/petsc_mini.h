@@ -110,6 +110,7 @@ PetscErrorCode VecAXPBY(Vec y, PetscScalar a, PetscScalar b, Vec x);
 PetscErrorCode VecAXPBYPCZ(Vec z, PetscScalar a, PetscScalar b, PetscScalar c, Vec x, Vec y);
 PetscErrorCode VecNorm(Vec x, NormType t, PetscReal *out);
 PetscErrorCode VecView(Vec x, PetscViewer v);
+PetscErrorCode VecLoad(Vec x, PetscViewer v);
 PetscErrorCode VecGetArray(Vec x, PetscScalar **a);
 PetscErrorCode VecRestoreArray(Vec x, PetscScalar **a);
 PetscErrorCode VecGetArrayRead(Vec x, const PetscScalar **a);

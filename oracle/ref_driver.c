@@ -307,6 +307,49 @@ int ref_advance(int nsteps, int *steps_out, double *t_out, double *dt_out)
     if (dt_out) *dt_out = Ctx.dt;
     return 0;
 }
+int ref_get_state(double *Uout);
+
+/* The output schedule of the reference's MonitorFunction (post_process.c:12-64):
+ * a solution file every write_interval steps (sol-%08d.vts, primitive variables
+ * from ComputePrimitiveVariables), restart1.bin every restart_interval steps and
+ * restart2.bin where (step + 7) % restart_interval == 0, written in the current
+ * directory.  0 turns a kind of output off (the default after ref_setup). */
+void ref_set_output(int write_interval, int restart_interval)
+{
+    Ctx.WriteInterval = write_interval;
+    Ctx.RestartInterval = restart_interval;
+}
+
+/* hype.c:389-400 after TSSolve: the primitive variables of U written to
+ * sol-<steps>.vts in the current directory. */
+int ref_write_final(int steps)
+{
+    if (!g_ready) return -1;
+    ComputePrimitiveVariables(U, Ctx.W, da);
+    char filename[20];
+    PetscViewer viewer;
+    sprintf(filename, "sol-%08d.vts", steps);
+    if (PetscViewerVTKOpen(PETSC_COMM_WORLD, filename, FILE_MODE_WRITE, &viewer)) return 1;
+    DMView(da, viewer);
+    const int rc = VecView(Ctx.W, viewer) != 0;
+    PetscViewerDestroy(&viewer);
+    return rc;
+}
+
+/* hype.c:316-325: the state read from restart1.bin in the current directory with
+ * VecLoad, returned in Uout.  Returns 0, or 1 where the file is missing or does
+ * not hold a Vec of this grid. */
+int ref_load_restart(double *Uout)
+{
+    if (!g_ready) return -1;
+    PetscViewer viewer_binary;
+    if (PetscViewerBinaryOpen(PETSC_COMM_WORLD, "restart1.bin", FILE_MODE_READ, &viewer_binary)) return 1;
+    const int rc = VecLoad(U, viewer_binary) != 0;
+    PetscViewerDestroy(&viewer_binary);
+    if (rc) return 1;
+    return ref_get_state(Uout);
+}
+
 int ref_get_state(double *Uout)
 {
     if (!g_ready) return -1;

@@ -130,3 +130,65 @@ def test_solve_monitored_writes_the_monitor_schedule(hp, outdir):
         s.set_state(U0)
         s.solve(0.0, 1e30, 9)
         assert read_petsc_vec(os.path.join(outdir, "restart2.bin")).tobytes() == s.get_state().tobytes()
+
+
+def test_monitor_files_equal_the_reference_files(hp, outdir):
+    """The GPU's monitored solve against the reference's own MonitorFunction
+    (post_process.c:12-64) and final write (hype.c:389-400) run through the PETSc
+    stand-in on the same state: the same file names, restart files equal byte for
+    byte (header, big-endian data, .info), and each .vts data array equal to the
+    primitive variables the reference hands its VTK viewer.  Then each side reads
+    the other's restart1.bin (hype.c:316-325 VecLoad; hype_read_restart) and both
+    resume 6 steps from it to the same bits."""
+    import cases
+    import oracle as O
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    ocfg = O.Config(system=O.KAPILA, order=2, nx=36, ny=26, cfl=0.4, gamma1=4.4, gamma2=1.4, pi1=6.0e8, pi2=0.0)
+    U0 = O.initial_state(ocfg, "shock_bubble", seed=11, nbubbles=2)
+    gdir, rdir = os.path.join(outdir, "gpu"), os.path.join(outdir, "ref")
+    os.makedirs(gdir)
+    os.makedirs(rdir)
+    cfg = cases.to_pkg(ocfg)
+    with hp.Solver(cfg) as s:
+        s.set_state(U0)
+        steps, t, _ = s.solve_monitored(0.0, 1e30, 14, 4, 3, gdir)
+        Ug = s.get_state()
+    ref = O.Reference(O.KAPILA)
+    ref.setup(ocfg)
+    ref.set_output(4, 3)
+    here = os.getcwd()
+    os.chdir(rdir)
+    try:
+        Ur, n, tr, _, st = ref.solve(U0, 0.0, 1e30, 14)
+        assert st == 0 and ref.write_final(n) == 0
+    finally:
+        os.chdir(here)
+    assert (steps, float(t).hex()) == (n, float(tr).hex())
+    assert Ug.tobytes() == Ur.tobytes()
+    gfiles, rfiles = sorted(os.listdir(gdir)), sorted(os.listdir(rdir))
+    assert gfiles == rfiles
+    for f in gfiles:
+        if f.startswith("restart"):
+            assert open(os.path.join(gdir, f), "rb").read() == open(os.path.join(rdir, f), "rb").read(), f
+        else:
+            _, names, arr = read_vts(os.path.join(gdir, f))
+            W = np.fromfile(os.path.join(rdir, f), dtype="<f8").reshape(-1, 6)
+            for c, nm in enumerate(names[1:]):
+                assert arr[nm][:, 0].tobytes() == W[:, c].tobytes(), (f, nm)
+    # cross reads, then 6 more steps from the restart state on each side
+    os.replace(os.path.join(gdir, "restart1.bin"), os.path.join(rdir, "restart1.bin"))
+    os.chdir(rdir)
+    try:
+        Ul, rc = ref.load_restart()
+    finally:
+        os.chdir(here)
+    assert rc == 0 and Ul.tobytes() == Ug.tobytes()
+    ref.set_output(0, 0)
+    Ur6, n6, t6, dt6, st6 = ref.solve(Ul, float(t), 1e30, 6)
+    with hp.Solver(cfg) as s:
+        assert s.read_restart(os.path.join(rdir, "restart1.bin")) == hp.OK
+        assert s.get_state().tobytes() == Ug.tobytes()
+        g6, tg6, dtg6, stg6 = s.solve(float(t), 1e30, 6)
+        assert stg6 == hp.OK and (g6, float(tg6).hex(), float(dtg6).hex()) == (n6, float(t6).hex(), float(dt6).hex())
+        assert s.get_state().tobytes() == Ur6.tobytes()
