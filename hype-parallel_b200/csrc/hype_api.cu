@@ -82,11 +82,12 @@ CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, 
 }  // namespace hype
 
 // 3-D map over the field planes: dims (x = nx, y = ny, z = nvar), box (cells + 6, 1, nvar);
-// a slab's map also covers its halo rows and starts row_off rows below row 0.
+// a slab's map also covers its halo rows and starts row_off rows below row 0, a
+// block's also its halo columns, starting col_off columns left of column 0.
 static int make_tmap(hype_solver *s, CUtensorMap *m, double *base)
 {
-    CUresult r = encode_planes_map(m, base - (long long)s->row_off * s->pitch, false, s->cfg.nx, s->cfg.ny + 2 * s->row_off, s->nv,
-                                   s->pitch, s->plane, stage_box_width(s->cells));
+    CUresult r = encode_planes_map(m, base - (long long)s->row_off * s->pitch - s->col_off, false, s->cfg.nx + 2 * s->col_off,
+                                   s->cfg.ny + 2 * s->row_off, s->nv, s->pitch, s->plane, stage_box_width(s->cells));
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return HYPE_OK;
 }
@@ -155,6 +156,7 @@ static StageParams base_params(const hype_solver *s)
     p.inlet = s->dInlet;
     p.kb = 1.0;
     p.row_off = s->row_off;
+    p.col_off = s->col_off;
     if (s->test_skip_row >= 0) { p.skip_loads = 1; p.skip_loads_from = s->test_skip_row; }
     return p;
 }
@@ -295,7 +297,10 @@ static double *buf_of(hype_solver *s, int b)
 }
 
 double *hype::solver_buf(hype_solver *s, int role) { return buf_of(s, role); }
-double *hype::solver_alloc_base(const hype_solver *s, double *buf) { return buf ? buf - (long long)s->row_off * s->pitch : nullptr; }
+double *hype::solver_alloc_base(const hype_solver *s, double *buf)
+{
+    return buf ? buf - (long long)s->row_off * s->pitch - s->col_off : nullptr;
+}
 
 cudaError_t hype::solver_stage(hype_solver *s, const PlanStage &q)
 {
@@ -568,12 +573,14 @@ int hype_destroy(hype_solver *s)
 
 // Device buffers, streams and descriptors of a checked configuration.  row_off > 0
 // makes a y-slab: every plane carries row_off halo rows below and above the slab's
-// rows; `inlet` replaces the inlet table computed from cfg (a slab's rows of the
-// whole grid's table).
-static int create_common(hype_solver *s, const hype_config *cfg, int row_off, const std::vector<double> *inlet)
+// rows; col_off > 0 (a block of a grid split in x, FP64 only) adds col_off halo
+// columns left and right of its columns; `inlet` replaces the inlet table computed
+// from cfg (a slab's rows of the whole grid's table).
+static int create_common(hype_solver *s, const hype_config *cfg, int row_off, const std::vector<double> *inlet, int col_off = 0)
 {
     s->cfg = *cfg;
     s->row_off = row_off;
+    s->col_off = col_off;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= cfg->device || cfg->device < 0)
         return fail(s, HYPE_ERR_NO_DEVICE, "CUDA device %d not available", cfg->device);
@@ -585,13 +592,14 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     s->fast = cfg->precision == HYPE_PREC_FP64_FAST;
 
     s->nv = hype_nvar(cfg->system);
-    s->pitch = s->mixed ? ((cfg->nx + 31) & ~31) : ((cfg->nx + 15) & ~15);   // 128-byte rows
+    if (s->mixed && col_off) return fail(s, HYPE_ERR_INVALID, "a block of a grid split in x takes an FP64 precision");
+    s->pitch = s->mixed ? ((cfg->nx + 31) & ~31) : ((cfg->nx + 2 * col_off + 15) & ~15);   // 128-byte rows
     s->plane = (long long)s->pitch * (cfg->ny + 2 * row_off);
     s->h = (cfg->x_max - cfg->x_min) / (double)cfg->nx;   // hype.c:57
     s->r1_h = 1. / s->h;                                  // rhs_function_prim.c:26
     s->cfl_h = cfg->cfl * s->h;                           // rhs_function_prim.c:620
     const size_t state_bytes = sizeof(double) * (size_t)s->plane * s->nv;
-    const size_t aos_bytes = sizeof(double) * (size_t)cfg->nx * (cfg->ny + 2 * row_off) * s->nv;
+    const size_t aos_bytes = sizeof(double) * (size_t)(cfg->nx + 2 * col_off) * (cfg->ny + 2 * row_off) * s->nv;
     CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(s, cudaEventCreate(&s->ev0));
     CUDA_TRY(s, cudaEventCreate(&s->ev1));
@@ -605,7 +613,7 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
     for (cudaEvent_t &e : s->ev_sb) CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     double **bufs[] = {&s->dU, &s->dS0, &s->dS1, &s->dS2};
-    const long long off = (long long)row_off * s->pitch;   // the buffers point at row 0
+    const long long off = (long long)row_off * s->pitch + col_off;   // the buffers point at cell (0, 0)
     for (double **b : bufs) {
         if (b == &s->dS2 && cfg->order != 3) continue;
         if (cudaMalloc(b, state_bytes) != cudaSuccess) return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", state_bytes);
@@ -642,7 +650,7 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     return set_tiling(s, s->mixed ? MIXED_CELLS : STAGE_CELLS);
 }
 
-int hype::create_slab(const hype_config *global, int row0, int rows, bool halo_lo, bool halo_hi, hype_solver **out)
+int hype::create_block(const hype_config *global, int col0, int cols, int row0, int rows, const bool halo[4], hype_solver **out)
 {
     if (!out) return HYPE_ERR_INVALID;
     *out = nullptr;
@@ -652,24 +660,52 @@ int hype::create_slab(const hype_config *global, int row0, int rows, bool halo_l
     int rc = check_config(global, s);
     if (rc) return rc;
     if (rows < 3 || row0 < 0 || row0 + rows > global->ny) return fail(s, HYPE_ERR_INVALID, "bad slab rows %d..%d", row0, row0 + rows - 1);
+    if (cols < 3 || col0 < 0 || col0 + cols > global->nx)
+        return fail(s, HYPE_ERR_INVALID, "bad block columns %d..%d", col0, col0 + cols - 1);
+    const bool xsplit = cols != global->nx;
     hype_config c = *global;
+    const double h = (global->x_max - global->x_min) / (double)global->nx;   // hype.c:57, the whole grid's spacing
+    c.nx = cols;
     c.ny = rows;
-    const double hy = (global->y_max - global->y_min) / (double)global->ny;   // the slab's extent (informative)
+    const double hy = (global->y_max - global->y_min) / (double)global->ny;   // the block's extent (informative)
     c.y_min = global->y_min + (double)row0 * hy;
     c.y_max = global->y_min + (double)(row0 + rows) * hy;
-    if (halo_lo) c.bc_bottom = BC_HALO;
-    if (halo_hi) c.bc_top = BC_HALO;
+    if (xsplit) {
+        c.x_min = global->x_min + (double)col0 * h;
+        c.x_max = global->x_min + (double)(col0 + cols) * h;
+    }
+    if (halo[0]) c.bc_left = BC_HALO;
+    if (halo[1]) c.bc_right = BC_HALO;
+    if (halo[2]) c.bc_bottom = BC_HALO;
+    if (halo[3]) c.bc_top = BC_HALO;
     s->row0 = row0;
-    if (global->bc_left != HYPE_BC_INLET) return create_common(s, &c, 3, nullptr);
-    // the slab's ghost-extended rows -3 .. rows+2 are rows row0-3 .. row0+rows+2 of the whole table
-    std::vector<double> whole, tab;
-    const double h = (global->x_max - global->x_min) / (double)global->nx;
-    const int nv = hype_nvar(global->system);
-    inlet_table(*global, h, whole);
-    tab.assign((size_t)3 * (rows + 6) * nv, 0.0);
-    for (int g = 0; g < 3; ++g)
-        std::memcpy(&tab[(size_t)g * (rows + 6) * nv], &whole[((size_t)g * (global->ny + 6) + row0) * nv], sizeof(double) * (rows + 6) * nv);
-    return create_common(s, &c, 3, &tab);
+    s->col0 = col0;
+    const int col_off = xsplit ? 4 : 0;   // 3 halo columns, 4 to keep TMA x origins 16-byte aligned
+    if (c.bc_left != HYPE_BC_INLET) {
+        rc = create_common(s, &c, 3, nullptr, col_off);
+    } else {
+        // the slab's ghost-extended rows -3 .. rows+2 are rows row0-3 .. row0+rows+2 of the whole table
+        std::vector<double> whole, tab;
+        const int nv = hype_nvar(global->system);
+        inlet_table(*global, h, whole);
+        tab.assign((size_t)3 * (rows + 6) * nv, 0.0);
+        for (int g = 0; g < 3; ++g)
+            std::memcpy(&tab[(size_t)g * (rows + 6) * nv], &whole[((size_t)g * (global->ny + 6) + row0) * nv],
+                        sizeof(double) * (rows + 6) * nv);
+        rc = create_common(s, &c, 3, &tab, col_off);
+    }
+    if (rc == HYPE_OK && xsplit) {   // the whole grid's h, not the block extent's rounding of it
+        s->h = h;
+        s->r1_h = 1. / s->h;                                  // rhs_function_prim.c:26
+        s->cfl_h = global->cfl * s->h;                        // rhs_function_prim.c:620
+    }
+    return rc;
+}
+
+int hype::create_slab(const hype_config *global, int row0, int rows, bool halo_lo, bool halo_hi, hype_solver **out)
+{
+    const bool halo[4] = {false, false, halo_lo, halo_hi};
+    return create_block(global, 0, global ? global->nx : 0, row0, rows, halo, out);
 }
 
 extern "C" {
@@ -708,7 +744,7 @@ static int read_scalars(hype_solver *s)
     if (s->hSc->err & ERR_INADMISSIBLE_FACE) {
         const unsigned cell = s->hSc->err_cell;
         return fail(s, HYPE_ERR_INADMISSIBLE, "inadmissible face state near cell (i=%u, j=%u)",
-                    cell % (unsigned)s->cfg.nx, cell / (unsigned)s->cfg.nx + (unsigned)s->row0);
+                    cell % (unsigned)s->cfg.nx + (unsigned)s->col0, cell / (unsigned)s->cfg.nx + (unsigned)s->row0);
     }
     return HYPE_OK;
 }
@@ -797,21 +833,47 @@ int hype_create_slab(const hype_config *cfg, int row0, int rows, hype_solver **o
     return create_slab(cfg, row0, rows, !whole && (row0 > 0 || periodic), !whole && (row0 + rows < cfg->ny || periodic), out);
 }
 
+int hype_create_block(const hype_config *cfg, int col0, int cols, int row0, int rows, hype_solver **out)
+{
+    if (!cfg) return HYPE_ERR_INVALID;
+    const bool px = cfg->bc_left == HYPE_BC_PERIODIC, py = cfg->bc_bottom == HYPE_BC_PERIODIC;
+    const bool wx = col0 == 0 && cols == cfg->nx, wy = row0 == 0 && rows == cfg->ny;
+    const bool halo[4] = {!wx && (col0 > 0 || px), !wx && (col0 + cols < cfg->nx || px),
+                          !wy && (row0 > 0 || py), !wy && (row0 + rows < cfg->ny || py)};
+    return create_block(cfg, col0, cols, row0, rows, halo, out);
+}
+
 int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_stride, double *RHS, double *dt)
 {
     (void)t;
     if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
-    if (!s->dSc || s->row_off == 0) return fail(s, HYPE_ERR_INVALID, "not a slab solver (hype_create_slab)");
+    if (!s->dSc || s->row_off == 0) return fail(s, HYPE_ERR_INVALID, "not a slab or block solver (hype_create_slab, hype_create_block)");
     const int nx = s->cfg.nx, rows = s->cfg.ny;
-    if (row_stride < (long long)nx * s->nv) return fail(s, HYPE_ERR_INVALID, "row_stride below nx * nvar");
-    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const int lo = s->cfg.bc_bottom == BC_HALO ? 3 : 0, hi = s->cfg.bc_top == BC_HALO ? 3 : 0;
+    const int cl = s->cfg.bc_left == BC_HALO ? 3 : 0, cr = s->cfg.bc_right == BC_HALO ? 3 : 0;
+    const int width = cl + nx + cr;   // cells per staged row
+    if (row_stride < (long long)width * s->nv) return fail(s, HYPE_ERR_INVALID, "row_stride below the staged row width * nvar");
+    CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t row_bytes = sizeof(double) * (size_t)nx * s->nv;
+    int rc;
+    if (s->col_off) {   // a block: rows -lo .. rows+hi-1, columns -cl .. nx+cr-1, compact, then planes
+        const size_t wide_bytes = sizeof(double) * (size_t)width * s->nv;
+        CUDA_TRY(s, cudaMemcpy2DAsync(s->dAosIn, wide_bytes, U - (long long)lo * row_stride - (long long)cl * s->nv,
+                                      sizeof(double) * (size_t)row_stride, wide_bytes, (size_t)(rows + lo + hi),
+                                      cudaMemcpyHostToDevice, s->stream));
+        CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, s->dS0 - (long long)lo * s->pitch - cl, width, 0, rows + lo + hi, s->nv,
+                                              s->pitch, s->plane, s->stream));
+        if ((rc = reset_scalars(s))) return rc;
+        CUDA_TRY(s, stage(s, s->dS0, s->dAosOut, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
+        CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, row_bytes * rows, cudaMemcpyDeviceToHost, s->stream));
+        if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
+        if (dt) *dt = host_dt(s);
+        return rc;
+    }
     // the slab's rows and its ghost rows into the staging array (local row -3 first), then planes
     CUDA_TRY(s, cudaMemcpy2DAsync(s->dAosIn + (size_t)(3 - lo) * nx * s->nv, row_bytes, U - (long long)lo * row_stride,
                                   sizeof(double) * (size_t)row_stride, row_bytes, (size_t)(rows + lo + hi), cudaMemcpyHostToDevice,
                                   s->stream));
-    int rc;
     if (s->mixed) {   // rows -lo .. rows+hi-1 into the mixed state S0 (FP32 and FP64 planes)
         const size_t row_elems = (size_t)nx * s->nv;
         CUDA_TRY(s, launch_aos_to_mixed(s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[1] - (long long)lo * s->pitch,

@@ -68,6 +68,9 @@ struct StageParams {
     int push_shift_lo, push_shift_hi;
     long long push_plane_lo, push_plane_hi;
     double *push_lo, *push_hi;
+    // block of a grid split in x as well (a DMDA rank's block): the planes carry col_off
+    // halo columns left of column 0 (and right of nx-1); the tensor map starts there
+    int col_off;
     // test hook (hype_test_skip_row_loads): with skip_loads set, no row load is issued for
     // rows >= skip_loads_from, so the bounded wait on it runs out; 0 in normal operation
     int skip_loads, skip_loads_from;

@@ -45,6 +45,10 @@ struct hype_solver {
     // role, with their plane sizes and the row shift from this slab's rows to theirs
     int row_off = 0;
     int row0 = 0;                     // first global row of the slab
+    // block of a grid split in x as well (hype_create_block): col_off halo columns left
+    // and right of the block's columns in every plane, col0 its first global column
+    int col_off = 0;
+    int col0 = 0;
     double *nb_lo[4] = {}, *nb_hi[4] = {};
     float *nbf_lo[3] = {}, *nbf_hi[3] = {};      // the same for a mixed state: FP32 and FP64 planes
     double *nbd_lo[3] = {}, *nbd_hi[3] = {};
@@ -62,6 +66,9 @@ int solver_fail(hype_solver *s, int code, const char *fmt, ...);
 // a slab solver: rows row0 .. row0+rows-1 of the grid of `global`, with halo rows on
 // the sides flagged halo_lo / halo_hi (a neighbouring slab there)
 int create_slab(const hype_config *global, int row0, int rows, bool halo_lo, bool halo_hi, hype_solver **out);
+// a block solver: columns col0 .. col0+cols-1 and rows row0 .. row0+rows-1 of the grid
+// of `global`; halo[4] flags the sides (left, right, bottom, top) with a neighbour
+int create_block(const hype_config *global, int col0, int cols, int row0, int rows, const bool halo[4], hype_solver **out);
 double *solver_buf(hype_solver *s, int role);                  // B_U .. B_S2
 double *solver_alloc_base(const hype_solver *s, double *buf);  // start of a padded buffer
 // one stage of the plan; a state output also goes to the neighbours' halo rows

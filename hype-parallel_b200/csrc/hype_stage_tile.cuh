@@ -267,11 +267,11 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 const int src = map_axis(row, p.ny, bcB, bcT);
                 uint64_t *bar = &bars[slot_of(row)];
                 mbar_expect_tx(bar, K::ROW_BYTES);
-                tma_load_3d(row_ptr(row), tmap, xs, src + p.row_off, 0, bar);   // the map starts row_off rows below row 0
+                tma_load_3d(row_ptr(row), tmap, xs + p.col_off, src + p.row_off, 0, bar);   // the map starts col_off columns left of column 0, row_off rows below row 0
             }
             if (finish_row && (!p.skip_loads || r - 1 < p.skip_loads_from)) {   // row r-1's conserved input for the RK combination in section C
                 mbar_expect_tx(&bars[SLOTS], K::ROW_BYTES);
-                tma_load_3d(orow_s, tmap, xs, (r - 1) + p.row_off, 0, &bars[SLOTS]);
+                tma_load_3d(orow_s, tmap, xs + p.col_off, (r - 1) + p.row_off, 0, &bars[SLOTS]);
             }
         }
         for (; next_conv <= r + 2; ++next_conv) {

@@ -72,8 +72,9 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity
 }
 
 // Ghost source index along one axis (rhs_function_prim.c:75-315 and the DMDA
-// periodic wrap): transmissive copies the edge cell, reflective mirrors; a
-// slab edge (BC_HALO) reads its halo rows as they are.
+// periodic wrap): transmissive copies the edge cell, reflective mirrors; the
+// edge of a slab or block of a decomposed grid (BC_HALO) reads its halo rows or
+// columns as they are.
 __device__ __forceinline__ int map_axis(int g, int n, int bc_lo, int bc_hi)
 {
     if (g < 0) {

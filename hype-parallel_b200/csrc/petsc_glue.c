@@ -19,17 +19,17 @@
  *   - the scratch of AppCtx (W, u_bnd, F, G, D, E) is not touched: the kernels
  *     need none of it; with several ranks, localU takes the ghosted state, as in
  *     rhs_function_prim.c:44-45.
- * Several MPI ranks (a DMDA split in y only, e.g. -da_processors_x 1): each rank's
- * GPU solver owns its rows (hype_create_slab); DMGlobalToLocal brings the 3 ghost
- * rows from the neighbouring ranks, hype_rhs_prim_slab computes the rank's RHS and
- * dt, and Ctx->dt is the MPI_Allreduce(MIN) of the ranks' dt, as in
- * rhs_function_prim.c:620-623.
+ Several MPI ranks (the DMDA of hype.c:108-122 split PETSC_DECIDE x PETSC_DECIDE,
+ * in x, in y or both): each rank's GPU solver owns its block of cells
+ * (hype_create_block); DMGlobalToLocal brings the 3 ghost rows and columns from
+ * the neighbouring ranks (corners included, BOX stencil), hype_rhs_prim_slab
+ * computes the rank's RHS and dt, and Ctx->dt is the MPI_Allreduce(MIN) of the
+ * ranks' dt, as in rhs_function_prim.c:620-623.
  * Differences:
  *   - an inadmissible face state (the reference prints and calls MPI_Abort,
  *     e.g. kapila_5eqn.c:353-357) prints the same kind of message and returns
  *     a non-zero PetscErrorCode, so TS stops through CHKERRQ instead of the
  *     process ending;
- *   - a DMDA split across x as well returns an error (the slabs are whole rows);
  *   - a failed RHS on any rank makes every rank return the error (a reduction of
  *     the status), where the reference's failing rank would MPI_Abort.
  * The GPU solver is created on first use and re-created when the AppCtx
@@ -43,10 +43,11 @@
 #include "hype_gpu.h"
 
 /* one GPU solver per path: [0] primitive, [1] conservative reconstruction; with
- * several ranks, for this rank's rows row0 .. row0+rows-1 */
+ * several ranks, for this rank's block: columns col0 .. col0+cols-1, rows row0 ..
+ * row0+rows-1 */
 static hype_solver *glue_solver[2] = {NULL, NULL};
 static hype_config glue_cfg[2];
-static int glue_row0[2], glue_rows[2];
+static int glue_col0[2], glue_cols[2], glue_row0[2], glue_rows[2];
 
 static int glue_system(void)
 {
@@ -102,33 +103,34 @@ static PetscErrorCode glue_rhs(int conservative, TS ts, PetscReal t, Vec U, Vec 
     MPI_Comm_size(PETSC_COMM_WORLD, &size);
     hype_config c;
     glue_config(Ctx, conservative, &c);
-    int row0 = 0, rows = c.ny, st = HYPE_OK;
+    int col0 = 0, cols = c.nx, row0 = 0, rows = c.ny, st = HYPE_OK;
     DM da = NULL;
     PetscInt gxs = 0, gys = 0, gxm = 0, gym = 0;
-    if (size > 1) {   /* this rank's rows of the DMDA (rhs_function_prim.c:36-53) */
+    if (size > 1) {   /* this rank's block of the DMDA (rhs_function_prim.c:36-53) */
         PetscInt xs, ys, xm, ym;
         TSGetDM(ts, &da);
         DMDAGetCorners(da, &xs, &ys, NULL, &xm, &ym, NULL);
         DMDAGetGhostCorners(da, &gxs, &gys, NULL, &gxm, &gym, NULL);
+        col0 = (int)xs;
+        cols = (int)xm;
         row0 = (int)ys;
         rows = (int)ym;
-        if (xs != 0 || xm != c.nx) {
-            fprintf(stderr, "RHSFunction (GPU): the DMDA must be split in y only (-da_processors_x 1)\n");
-            st = HYPE_ERR_INVALID;
-        }
     }
     if (st == HYPE_OK && (!glue_solver[conservative] || memcmp(&c, &glue_cfg[conservative], sizeof(c)) != 0 ||
+                          glue_col0[conservative] != col0 || glue_cols[conservative] != cols ||
                           glue_row0[conservative] != row0 || glue_rows[conservative] != rows)) {
         hype_destroy(glue_solver[conservative]);
         glue_solver[conservative] = NULL;
         hype_solver *s = NULL;
-        st = size > 1 ? hype_create_slab(&c, row0, rows, &s) : hype_create(&c, &s);
+        st = size > 1 ? hype_create_block(&c, col0, cols, row0, rows, &s) : hype_create(&c, &s);
         if (st != HYPE_OK) {
             fprintf(stderr, "RHSFunction (GPU): %s\n", s ? hype_last_error(s) : hype_status_string(st));
             hype_destroy(s);
         } else {
             glue_solver[conservative] = s;
             glue_cfg[conservative] = c;
+            glue_col0[conservative] = col0;
+            glue_cols[conservative] = cols;
             glue_row0[conservative] = row0;
             glue_rows[conservative] = rows;
         }
@@ -149,8 +151,8 @@ static PetscErrorCode glue_rhs(int conservative, TS ts, PetscReal t, Vec U, Vec 
         hype_solver *s = glue_solver[conservative];
         if (size > 1) {
             const int nv = hype_nvar(c.system);
-            /* cell (0, row0) of the ghosted local array; its rows are gxm records apart */
-            const double *u0 = (const double *)u + ((size_t)(row0 - gys) * gxm + (size_t)(0 - gxs)) * nv;
+            /* cell (col0, row0) of the ghosted local array; its rows are gxm records apart */
+            const double *u0 = (const double *)u + ((size_t)(row0 - gys) * gxm + (size_t)(col0 - gxs)) * nv;
             st = hype_rhs_prim_slab(s, (double)t, u0, (long long)gxm * nv, (double *)r, &dt);
         } else {
             st = hype_rhs_prim(s, (double)t, (const double *)u, (double *)r, &dt);

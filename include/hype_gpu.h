@@ -145,14 +145,25 @@ HYPE_API int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, do
  * the caller instead of a boundary condition.  FP64 or mixed precision. */
 HYPE_API int hype_create_slab(const hype_config *cfg, int row0, int rows, hype_solver **out);
 
-/* RHSFunctionPrim (or RHSFunction) on a slab: rhs_function_prim.c:12-626 for one
- * rank.  U points at the slab's cell (0, 0) in a host array whose rows are
- * row_stride doubles apart: nx*nvar for a compact array, or the ghosted width times
- * nvar for a DMDA local vector after DMGlobalToLocal.  Rows -3..-1 and rows..rows+2
- * are read on the sides with a neighbour; ghost columns are never read.  RHS
- * receives the slab's rows, compact.  *dt is this slab's CFL h / (2 s_max); the
- * caller takes the minimum over ranks, as rhs_function_prim.c:620-623 does with
- * MPI_Allreduce(MIN). */
+/* One MPI rank's block of a grid decomposed over ranks in x and y: HyPE-2D's DMDA
+ * as hype.c:108-122 creates it (PETSC_DECIDE x PETSC_DECIDE ranks, BOX stencil,
+ * ghost width 3).  The solver owns global columns col0 .. col0+cols-1 and rows
+ * row0 .. row0+rows-1 of the grid `cfg` describes (the whole grid's nx, ny, domain
+ * and boundaries); cols, rows >= 3.  A side with a neighbouring rank (an inner
+ * edge, or a periodic axis the block does not span) takes its 3 ghost rows or
+ * columns, corners included, from the caller instead of a boundary condition.
+ * With cols == nx this is hype_create_slab.  A block split in x takes an FP64
+ * precision (HYPE_ERR_INVALID for mixed precision). */
+HYPE_API int hype_create_block(const hype_config *cfg, int col0, int cols, int row0, int rows, hype_solver **out);
+
+/* RHSFunctionPrim (or RHSFunction) on a slab or block: rhs_function_prim.c:12-626
+ * for one rank.  U points at the block's cell (0, 0) in a host array whose rows
+ * are row_stride doubles apart: cols*nvar for a compact array, or the ghosted width
+ * times nvar for a DMDA local vector after DMGlobalToLocal.  Rows -3..-1 and
+ * rows..rows+2, and columns -3..-1 and cols..cols+2, are read on the sides with a
+ * neighbour; other ghost cells are never read.  RHS receives the block's cells,
+ * compact.  *dt is this block's CFL h / (2 s_max); the caller takes the minimum
+ * over ranks, as rhs_function_prim.c:620-623 does with MPI_Allreduce(MIN). */
 HYPE_API int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_stride, double *RHS, double *dt);
 
 /*

@@ -129,3 +129,61 @@ def test_glue_ranks_bitwise_vs_oracle(name, nranks, hp, orc, glue_libs):
         assert min(dts) >= dto
     else:
         assert min(dts) == dto
+
+
+# (case, ranks, px, py): px = py = 0 is PETSc's own PETSC_DECIDE split (hype.c:108-122)
+LIVE_CASES = [("kapila_37x23_rough_mixed_bc", 4, 0, 0), ("kapila_24x24_periodic", 6, 3, 2), ("kapila_18x14_inlet", 3, 3, 1),
+              ("kapila_15x13_N3", 4, 2, 2), ("bn_13x21_periodic_N1", 4, 2, 2), ("euler_21x19_reflective_N1", 6, 3, 2),
+              ("kapila_cons_37x23_rough", 4, 2, 2), ("kapila_visc_37x23_rough", 4, 0, 0)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nranks,px,py", LIVE_CASES)
+def test_glue_live_ranks_blocks_bitwise_vs_reference_ranks(name, nranks, px, py, hp):
+    """The glue as live MPI ranks (one process each, all on one GPU) on a DMDA split
+    in x and y -- each rank's GPU solver a block with 3 ghost rows and columns from
+    DMGlobalToLocal, dt reduced with MPI_Allreduce(MIN) -- against the reference's
+    RHSFunctionPrim / RHSFunction run as the same ranks (oracle.LiveReference):
+    one RHS call and a 3-step hype.c time loop (dt reset from the reduced Ctx->dt
+    every step, post_process.c:19) bit for bit."""
+    import glue_live
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    _, cfg, kind, seed = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    subprocess.run(["make", "-s", "-C", GLUE], check=True, capture_output=True)
+    with O.LiveReference(cfg, nranks, px, py, wait_s=120.0) as ref:
+        Rr, dtr, str_ = ref.rhs(U)
+        Ur, nr, tr, dtnr, sr = ref.solve(U, 0.0, 1.0, 3)
+        blocks = sorted(ref.blocks)
+    assert str_ == 0 and sr == 0
+    lib = LIBNAME[(cfg.system, int(cfg.viscous))]
+    with glue_live.LiveGlue(cfg, lib, nranks, px, py) as g:
+        assert sorted(g.blocks) == blocks
+        if px > 1:
+            assert all(b[2] < cfg.nx for b in blocks)   # the grid is split in x
+        R, dts, st = g.rhs(U)
+        assert st == 0
+        assert all(d == dtr for d in dts)
+        assert R.tobytes() == Rr.tobytes()
+        Ug, ng, tg, dtng, sg = g.solve(U, 0.0, 1.0, 3)
+    assert sg == 0 and (ng, tg, dtng) == (nr, tr, dtnr)
+    assert Ug.tobytes() == Ur.tobytes()
+
+
+def test_glue_live_ranks_without_gpu_all_return_the_error(hp, glue_libs):
+    """Without a GPU every rank's solver fails to be created; the glue's reduction
+    of the status (MPI_Allreduce(MAX)) makes every rank of a 2 x 2 DMDA return
+    the error, RHS and time loop alike, instead of one rank aborting the job."""
+    import torch
+    import glue_live
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    _, cfg, kind, seed = cases.case_by_name("kapila_24x24_periodic")
+    U = cases.state(cfg, kind, seed)
+    with glue_live.LiveGlue(cfg, "kapila", 4, 2, 2, wait_s=60.0) as g:
+        assert sorted(g.blocks) == [(0, 0, 12, 12), (0, 12, 12, 12), (12, 0, 12, 12), (12, 12, 12, 12)]
+        R, dts, st = g.rhs(U)
+        assert st == hp.ERR_NO_DEVICE
+        _, n, _, _, st = g.solve(U, 0.0, 1.0, 3)
+        assert st == hp.ERR_NO_DEVICE and n == 0
