@@ -176,19 +176,21 @@ def test_monitor_files_equal_the_reference_files(hp, outdir):
             W = np.fromfile(os.path.join(rdir, f), dtype="<f8").reshape(-1, 6)
             for c, nm in enumerate(names[1:]):
                 assert arr[nm][:, 0].tobytes() == W[:, c].tobytes(), (f, nm)
-    # cross reads, then 6 more steps from the restart state on each side
+    # cross reads of the GPU's restart1.bin (last written at step 12), then 6 more
+    # steps from the restart state on each side
+    U12 = read_petsc_vec(os.path.join(gdir, "restart1.bin"))
     os.replace(os.path.join(gdir, "restart1.bin"), os.path.join(rdir, "restart1.bin"))
     os.chdir(rdir)
     try:
         Ul, rc = ref.load_restart()
     finally:
         os.chdir(here)
-    assert rc == 0 and Ul.tobytes() == Ug.tobytes()
+    assert rc == 0 and Ul.tobytes() == U12.tobytes()
     ref.set_output(0, 0)
-    Ur6, n6, t6, dt6, st6 = ref.solve(Ul, float(t), 1e30, 6)
+    Ur6, n6, t6, dt6, st6 = ref.solve(Ul, 0.0, 1e30, 6)
     with hp.Solver(cfg) as s:
         assert s.read_restart(os.path.join(rdir, "restart1.bin")) == hp.OK
-        assert s.get_state().tobytes() == Ug.tobytes()
-        g6, tg6, dtg6, stg6 = s.solve(float(t), 1e30, 6)
+        assert s.get_state().tobytes() == U12.tobytes()
+        g6, tg6, dtg6, stg6 = s.solve(0.0, 1e30, 6)
         assert stg6 == hp.OK and (g6, float(tg6).hex(), float(dtg6).hex()) == (n6, float(t6).hex(), float(dt6).hex())
         assert s.get_state().tobytes() == Ur6.tobytes()

@@ -135,38 +135,59 @@ def test_glue_ranks_bitwise_vs_oracle(name, nranks, hp, orc, glue_libs):
 LIVE_CASES = [("kapila_37x23_rough_mixed_bc", 4, 0, 0), ("kapila_24x24_periodic", 6, 3, 2), ("kapila_18x14_inlet", 3, 3, 1),
               ("kapila_15x13_N3", 4, 2, 2), ("bn_13x21_periodic_N1", 4, 2, 2), ("euler_21x19_reflective_N1", 6, 3, 2),
               ("kapila_cons_37x23_rough", 4, 2, 2), ("kapila_visc_37x23_rough", 4, 0, 0)]
+LIVE_SOLVES = [("kapila_32x32_bubble_solve", 4, 0, 0), ("kapila_24x20_bubble_solve_N1", 6, 3, 2),
+               ("kapila_16x16_solve_N3", 4, 2, 2), ("euler_32x24_solve", 6, 0, 0), ("bn_20x20_solve", 4, 4, 1),
+               ("kapila_cons_32x32_solve", 4, 2, 2), ("kapila_visc_32x32_solve", 4, 0, 0)]
+
+
+def _live_glue_setup():
+    if not O.reference_available():
+        pytest.skip("oracle/_ref not built")
+    subprocess.run(["make", "-s", "-C", GLUE], check=True, capture_output=True)
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name,nranks,px,py", LIVE_CASES)
-def test_glue_live_ranks_blocks_bitwise_vs_reference_ranks(name, nranks, px, py, hp):
+def test_glue_live_ranks_rhs_bitwise_vs_reference_ranks(name, nranks, px, py, hp):
     """The glue as live MPI ranks (one process each, all on one GPU) on a DMDA split
-    in x and y -- each rank's GPU solver a block with 3 ghost rows and columns from
-    DMGlobalToLocal, dt reduced with MPI_Allreduce(MIN) -- against the reference's
-    RHSFunctionPrim / RHSFunction run as the same ranks (oracle.LiveReference):
-    one RHS call and a 3-step hype.c time loop (dt reset from the reduced Ctx->dt
-    every step, post_process.c:19) bit for bit."""
+    in x and y -- each rank's GPU solver a block with 3 ghost rows and columns,
+    corners included, from DMGlobalToLocal, dt reduced with MPI_Allreduce(MIN) --
+    against the reference's RHSFunctionPrim / RHSFunction run as the same ranks
+    (oracle.LiveReference): RHS and dt bit for bit."""
     import glue_live
-    if not O.reference_available():
-        pytest.skip("oracle/_ref not built")
+    _live_glue_setup()
     _, cfg, kind, seed = cases.case_by_name(name)
     U = cases.state(cfg, kind, seed)
-    subprocess.run(["make", "-s", "-C", GLUE], check=True, capture_output=True)
     with O.LiveReference(cfg, nranks, px, py, wait_s=120.0) as ref:
-        Rr, dtr, str_ = ref.rhs(U)
-        Ur, nr, tr, dtnr, sr = ref.solve(U, 0.0, 1.0, 3)
+        Rr, dtr, sr = ref.rhs(U)
         blocks = sorted(ref.blocks)
-    assert str_ == 0 and sr == 0
-    lib = LIBNAME[(cfg.system, int(cfg.viscous))]
-    with glue_live.LiveGlue(cfg, lib, nranks, px, py) as g:
+    assert sr == 0
+    with glue_live.LiveGlue(cfg, LIBNAME[(cfg.system, int(cfg.viscous))], nranks, px, py) as g:
         assert sorted(g.blocks) == blocks
         if px > 1:
             assert all(b[2] < cfg.nx for b in blocks)   # the grid is split in x
         R, dts, st = g.rhs(U)
-        assert st == 0
-        assert all(d == dtr for d in dts)
-        assert R.tobytes() == Rr.tobytes()
-        Ug, ng, tg, dtng, sg = g.solve(U, 0.0, 1.0, 3)
+    assert st == 0
+    assert all(d == dtr for d in dts)
+    assert R.tobytes() == Rr.tobytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,nranks,px,py", LIVE_SOLVES)
+def test_glue_live_ranks_time_loop_bitwise_vs_reference_ranks(name, nranks, px, py, hp):
+    """hype.c's time loop (hype.c:337-384: a direct RHS call seeds Ctx->dt, TSSolve
+    with dt reset from Ctx->dt every step, post_process.c:19) with the glue's RHS on
+    live ranks over a DMDA split in x and y, against the reference's loop on the
+    same ranks: steps, final time, next dt and state bit for bit."""
+    import glue_live
+    _live_glue_setup()
+    (_, cfg, kind, seed), t0, tf, nmax = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    with O.LiveReference(cfg, nranks, px, py, wait_s=120.0) as ref:
+        Ur, nr, tr, dtnr, sr = ref.solve(U, t0, tf, nmax)
+    assert sr == 0 and nr > 0
+    with glue_live.LiveGlue(cfg, LIBNAME[(cfg.system, int(cfg.viscous))], nranks, px, py) as g:
+        Ug, ng, tg, dtng, sg = g.solve(U, t0, tf, nmax)
     assert sg == 0 and (ng, tg, dtng) == (nr, tr, dtnr)
     assert Ug.tobytes() == Ur.tobytes()
 
