@@ -348,7 +348,7 @@ static int upload_inst(hype_batch *b, int s)
 static int rebuild_work(hype_batch *b, int id)
 {
     Kind &k = b->kinds[id];
-    struct Item { long long cost; int2 it; };
+    struct Item { long long cost; int2 it; int H, run, st, strips; };
     int K = 1;
     k.cost = 0;
     for (int s : k.members) {
@@ -375,12 +375,33 @@ static int rebuild_work(hype_batch *b, int id)
                 const int H = (int)(((long long)(run + 1) * in.cfg.ny) / in.runs) - (int)(((long long)run * in.cfg.ny) / in.runs);
                 for (int st = 0; st < in.strips; ++st) {
                     const int w = in.cfg.nx / in.strips + 1;
-                    items.push_back(Item{(long long)(w + halo) * (H + 6), make_int2(s, run * in.strips + st)});
+                    items.push_back(Item{(long long)(w + halo) * (H + 6), make_int2(s, run * in.strips + st), H, run, st, in.strips});
                 }
             }
         }
         mem[0] = (int)mem.size() - 1;
-        std::stable_sort(items.begin(), items.end(), [](const Item &x, const Item &y) { return x.cost > y.cost; });
+        auto longest_first = [](const Item &x, const Item &y) { return x.cost > y.cost; };
+        std::stable_sort(items.begin(), items.end(), longest_first);
+        // The last wave of the list (half the resident blocks' worth of items) decides
+        // when the launch ends: its tiles of 32 rows or more are split into two runs of
+        // the instance's decomposition refined twice (item_refine), so the blocks finish
+        // closer together.  The list is sorted again.
+        const int tail = std::min((int)items.size(), std::max(1, b->sms * k.bps / 2));
+        const int split_from = (int)items.size() - tail;
+        for (int i = (int)items.size() - 1; i >= split_from; --i) {
+            Item &x = items[i];
+            if (x.H < 32) continue;
+            const int w = (int)(x.cost / (x.H + 6));
+            const int s = x.it.x, st = x.st, S = x.strips, r = x.run;
+            const Inst &in = b->inst[s];
+            const long long R2 = 2LL * in.runs;
+            int h2[2];
+            for (int q = 0; q < 2; ++q)
+                h2[q] = (int)(((long long)(2 * r + q + 1) * in.cfg.ny) / R2) - (int)(((long long)(2 * r + q) * in.cfg.ny) / R2);
+            x = Item{(long long)w * (h2[0] + 6), make_int2(s, (1 << 28) | ((2 * r) * S + st)), h2[0], 2 * r, st, S};
+            items.push_back(Item{(long long)w * (h2[1] + 6), make_int2(s, (1 << 28) | ((2 * r + 1) * S + st)), h2[1], 2 * r + 1, st, S});
+        }
+        std::stable_sort(items.begin(), items.end(), longest_first);
         const int n = (int)items.size();
         if (n > l.work_cap) {
             int cap = l.work_cap > 0 ? l.work_cap : 1024;

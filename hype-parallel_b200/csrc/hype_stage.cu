@@ -42,10 +42,12 @@ stage_batch_kernel(const StageParams *__restrict__ inst, const CUtensorMap *__re
         const int2 it = work[w];
         if (threadIdx.x == 0) {
             p_s = inst[it.x];
+            p_s.runs *= item_refine(it.y);
             fence_tensormap_acquire(&tmaps[it.x]);
         }
         __syncthreads();
-        stage_tile<SYS, N, CELLS, false>(p_s, &tmaps[it.x], it.y % p_s.strips, it.y / p_s.strips, smem_raw, red_s);
+        const int tile = item_tile(it.y);
+        stage_tile<SYS, N, CELLS, false>(p_s, &tmaps[it.x], tile % p_s.strips, tile / p_s.strips, smem_raw, red_s);
         last = p_s.sc;
     }
     work_finish(sched);

@@ -37,7 +37,7 @@ struct MixedKernel {
     static constexpr int YTF_FLOATS = 2 * 4 * CELLS;     // top-face rho1 rho2 u v, by Gauss point
     static constexpr int YTD_DOUBLES = 2 * 2 * CELLS;    // top-face p, a1
     static constexpr int CARRY_DOUBLES = 14 * CELLS;     // t1[6], G below[6], E5 below, ncp5
-    static constexpr int MIN_BLOCKS = 2 * (128 / CELLS);
+    static constexpr int MIN_BLOCKS = 3 * (128 / CELLS);
     static constexpr size_t smem_bytes()
     {
         // the ring plus one more slot: the stage input of the row being finished (row r-1)
@@ -654,11 +654,13 @@ mixed_batch_kernel(const MixedParams *__restrict__ inst, const MixedMaps *__rest
         const int2 it = work[w];
         if (threadIdx.x == 0) {
             p_s = inst[it.x];
+            p_s.runs *= item_refine(it.y);
             fence_tensormap_acquire(&maps[it.x].f);
             fence_tensormap_acquire(&maps[it.x].d);
         }
         __syncthreads();
-        mixed_tile<CELLS>(p_s, &maps[it.x], it.y % p_s.strips, it.y / p_s.strips, smem_raw, red_s);
+        const int tile = item_tile(it.y);
+        mixed_tile<CELLS>(p_s, &maps[it.x], tile % p_s.strips, tile / p_s.strips, smem_raw, red_s);
         last = p_s.sc;
     }
     work_finish(sched);

@@ -122,6 +122,14 @@ __device__ __forceinline__ int work_take(int *sched, int nwork, const DevScalars
     __syncthreads();
     return w;
 }
+// A work item's tile: it.y = (log2 f << 28) | (run' * strips + strip), where run' is a
+// run of the instance's row decomposition refined f times (run r split into runs
+// r f .. r f + f-1).  The refined boundaries floor(run' ny / (f runs)) equal the
+// instance's own floor(r ny / runs) at run' = r f, so plain and refined tiles of one
+// instance cover its rows exactly once.
+__device__ __forceinline__ int item_refine(int y) { return 1 << ((unsigned)y >> 28); }
+__device__ __forceinline__ int item_tile(int y) { return y & 0x0fffffff; }
+
 __device__ __forceinline__ void work_finish(int *sched)
 {
     if (threadIdx.x == 0) {
