@@ -165,16 +165,18 @@ static StageParams base_params(const hype_solver *s)
 // resident blocks each), at least 8 rows per run.  Rebuilds the TMA
 // descriptors, whose box width follows the tile width, and drops the captured
 // step graph (recaptured on the next hype_begin / hype_advance).
-// FP32 (4 planes) and FP64 (2 planes) maps of a mixed state, box (cells + 8, 1, planes);
-// a slab's maps also cover its halo rows and start row_off rows below row 0
+// FP32 (nf planes) and FP64 (nd planes) maps of a mixed state (MixedLayout), box
+// (cells + 8, 1, planes); a slab's maps also cover its halo rows and start row_off
+// rows below row 0
 static int make_mixed_maps(hype_solver *s, MixedMaps *mm, float *pf, double *pd)
 {
     const int bw = mixed_box_width(s->cells);
     const long long off = (long long)s->row_off * s->pitch;
     const int rows = s->cfg.ny + 2 * s->row_off;
-    CUresult r = encode_planes_map(&mm->f, pf - off, true, s->cfg.nx, rows, 4, s->pitch, s->plane, bw);
+    const MixedLayout L = mixed_layout(s->cfg.system);
+    CUresult r = encode_planes_map(&mm->f, pf - off, true, s->cfg.nx, rows, L.nf, s->pitch, s->plane, bw);
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP32 planes) failed (%d)", (int)r);
-    r = encode_planes_map(&mm->d, pd - off, false, s->cfg.nx, rows, 2, s->pitch, s->plane, bw);
+    r = encode_planes_map(&mm->d, pd - off, false, s->cfg.nx, rows, L.nd, s->pitch, s->plane, bw);
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled (FP64 planes) failed (%d)", (int)r);
     return HYPE_OK;
 }
@@ -185,7 +187,7 @@ static int set_tiling(hype_solver *s, int cells, int waves = 1)
     int rc;
     s->cells = cells;
     if (s->mixed) {
-        s->bps = mixed_blocks_per_sm(cells);
+        s->bps = mixed_blocks_per_sm(cfg->system, cells);
         if (s->bps < 1) return fail(s, HYPE_ERR_CUDA, "mixed stage kernel does not fit on an SM");
         s->strips = mixed_strips(cfg->nx, cells);
         s->waves = waves > 0 ? waves : 1;
@@ -266,6 +268,7 @@ static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double
     p.nx = s->cfg.nx; p.ny = s->cfg.ny; p.pitch = s->pitch; p.plane = s->plane;
     p.bc[0] = s->cfg.bc_left; p.bc[1] = s->cfg.bc_right; p.bc[2] = s->cfg.bc_bottom; p.bc[3] = s->cfg.bc_top;
     p.eos.g1 = s->cfg.gamma1; p.eos.g2 = s->cfg.gamma2; p.eos.pi1 = s->cfg.pi1; p.eos.pi2 = s->cfg.pi2;
+    p.eos.fix_p2 = (s->cfg.flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
     p.r1_h = s->r1_h; p.cfl_h = s->cfl_h;
     p.in_f = s->mf[k_in]; p.in_d = s->md[k_in];
     if (k_x >= 0) { p.xn_f = s->mf[k_x]; p.xn_d = s->md[k_x]; }
@@ -282,7 +285,7 @@ static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double
         p.push_plane_lo = s->nb_plane_lo; p.push_shift_lo = s->nb_shift_lo;
         p.push_plane_hi = s->nb_plane_hi; p.push_shift_hi = s->nb_shift_hi;
     }
-    return launch_mixed(s->cells, s->mm[k_in], p, s->stream);
+    return launch_mixed(s->cfg.system, s->cells, s->mm[k_in], p, s->stream);
 }
 
 static double *buf_of(hype_solver *s, int b)
@@ -371,8 +374,6 @@ static int check_config(const hype_config *c, hype_solver *s)
         return fail(s, HYPE_ERR_INVALID, "unknown precision %d", c->precision);
     if (c->precision == HYPE_PREC_FP64_FAST && (c->flags & (HYPE_FLAG_CONSERVATIVE | HYPE_FLAG_VISCOUS)))
         return fail(s, HYPE_ERR_INVALID, "the FP64 performance form covers the primitive-variable inviscid path");
-    if (c->precision == HYPE_PREC_MIXED && c->system != HYPE_KAPILA_5EQN)
-        return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for the Kapila system");
     if (c->precision == HYPE_PREC_MIXED && (c->order != 2 || c->bc_left == HYPE_BC_INLET))
         return fail(s, HYPE_ERR_INVALID, "mixed precision is implemented for N = 2 without inlet boundaries");
     if (c->precision == HYPE_PREC_MIXED && (c->flags & HYPE_FLAG_CONSERVATIVE))
@@ -621,12 +622,13 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
         *b += off;
     }
     if (s->mixed) {
+        const MixedLayout L = mixed_layout(cfg->system);
         for (int k = 0; k < 3; ++k) {
-            if (cudaMalloc(&s->mf[k], sizeof(float) * 4 * (size_t)s->plane) != cudaSuccess ||
-                cudaMalloc(&s->md[k], sizeof(double) * 2 * (size_t)s->plane) != cudaSuccess)
+            if (cudaMalloc(&s->mf[k], sizeof(float) * L.nf * (size_t)s->plane) != cudaSuccess ||
+                cudaMalloc(&s->md[k], sizeof(double) * L.nd * (size_t)s->plane) != cudaSuccess)
                 return fail(s, HYPE_ERR_NOMEM, "cudaMalloc of the mixed state failed");
-            CUDA_TRY(s, cudaMemset(s->mf[k], 0, sizeof(float) * 4 * (size_t)s->plane));
-            CUDA_TRY(s, cudaMemset(s->md[k], 0, sizeof(double) * 2 * (size_t)s->plane));
+            CUDA_TRY(s, cudaMemset(s->mf[k], 0, sizeof(float) * L.nf * (size_t)s->plane));
+            CUDA_TRY(s, cudaMemset(s->md[k], 0, sizeof(double) * L.nd * (size_t)s->plane));
             s->mf[k] += off;   // row 0 of the slab
             s->md[k] += off;
         }
@@ -761,12 +763,12 @@ static int reset_scalars(hype_solver *s)
 // interleaved FP64 state (device) -> state k (0 = U, 1 = S0) in the solver's layout
 static cudaError_t load_state(hype_solver *s, const double *aos, int k)
 {
-    if (s->mixed) return launch_aos_to_mixed(aos, s->mf[k], s->md[k], s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream);
+    if (s->mixed) return launch_aos_to_mixed(s->cfg.system, aos, s->mf[k], s->md[k], s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream);
     return launch_aos_to_planes(aos, k == 0 ? s->dU : s->dS0, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream);
 }
 static cudaError_t store_state(hype_solver *s, int k, double *aos)
 {
-    if (s->mixed) return launch_mixed_to_aos(s->mf[k], s->md[k], aos, s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream);
+    if (s->mixed) return launch_mixed_to_aos(s->cfg.system, s->mf[k], s->md[k], aos, s->cfg.nx, s->cfg.ny, s->pitch, s->plane, s->stream);
     return launch_planes_to_aos(k == 0 ? s->dU : s->dS0, aos, s->cfg.nx, s->cfg.ny, s->nv, s->pitch, s->plane, s->stream);
 }
 
@@ -876,7 +878,7 @@ int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_
                                   s->stream));
     if (s->mixed) {   // rows -lo .. rows+hi-1 into the mixed state S0 (FP32 and FP64 planes)
         const size_t row_elems = (size_t)nx * s->nv;
-        CUDA_TRY(s, launch_aos_to_mixed(s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[1] - (long long)lo * s->pitch,
+        CUDA_TRY(s, launch_aos_to_mixed(s->cfg.system, s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[1] - (long long)lo * s->pitch,
                                         s->md[1] - (long long)lo * s->pitch, nx, rows + lo + hi, s->pitch, s->plane, s->stream));
         if ((rc = reset_scalars(s))) return rc;
         CUDA_TRY(s, stage_m(s, 1, -1, OUT_RHS, 0, 1.0, 0, -1, 1, s->dAosOut));
@@ -1144,7 +1146,7 @@ int hype_launch_info(const hype_solver *s, int *gx, int *gy, int *threads, size_
     if (gx) *gx = s->strips;
     if (gy) *gy = s->runs;
     if (threads) *threads = stage_threads(s->cells);
-    if (smem) *smem = s->mixed ? mixed_smem_bytes(s->cells) : stage_smem_bytes(s->cfg.system, s->cfg.order, s->cells);
+    if (smem) *smem = s->mixed ? mixed_smem_bytes(s->cfg.system, s->cells) : stage_smem_bytes(s->cfg.system, s->cfg.order, s->cells);
     if (bps) *bps = s->bps;
     return HYPE_OK;
 }
@@ -1167,9 +1169,10 @@ int hype_time_stage(hype_solver *s, int reps, double *ms_per_launch)
     };
     if (s->mixed) {
         const long long moff = (long long)s->row_off * s->pitch;   // whole planes, halo rows included
-        CUDA_TRY(s, cudaMemcpyAsync(s->mf[1] - moff, s->mf[0] - moff, sizeof(float) * 4 * (size_t)s->plane, cudaMemcpyDeviceToDevice,
+        const MixedLayout L = mixed_layout(s->cfg.system);
+        CUDA_TRY(s, cudaMemcpyAsync(s->mf[1] - moff, s->mf[0] - moff, sizeof(float) * L.nf * (size_t)s->plane, cudaMemcpyDeviceToDevice,
                                     s->stream));
-        CUDA_TRY(s, cudaMemcpyAsync(s->md[1] - moff, s->md[0] - moff, sizeof(double) * 2 * (size_t)s->plane, cudaMemcpyDeviceToDevice,
+        CUDA_TRY(s, cudaMemcpyAsync(s->md[1] - moff, s->md[0] - moff, sizeof(double) * L.nd * (size_t)s->plane, cudaMemcpyDeviceToDevice,
                                     s->stream));
     } else {
         CUDA_TRY(s, cudaMemcpyAsync(solver_alloc_base(s, s->dS0), solver_alloc_base(s, s->dU), sizeof(double) * (size_t)s->plane * s->nv,

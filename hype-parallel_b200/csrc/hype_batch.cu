@@ -31,16 +31,19 @@ namespace {
 
 // kinds: FP64 primitive path 0..11 (3 systems x 4 orders), 12 = mixed Kapila N = 2,
 // conservative path 13..24 (3 systems x 4 orders), viscous Kapila N = 1..3: primitive
-// 25..27, conservative 28..30
-constexpr int NKIND = 31;
+// 25..27, conservative 28..30; mixed Baer-Nunziato and Euler N = 2: 31, 32
+constexpr int NKIND = 33;
 constexpr int KIND_MIXED = 12;
 constexpr int KIND_CONS0 = 13, KIND_VISC0 = 25, KIND_VISC_CONS0 = 28;
+constexpr int KIND_MIXED_BN = 31, KIND_MIXED_EULER = 32;
+bool kind_is_mixed(int id) { return id == KIND_MIXED || id == KIND_MIXED_BN || id == KIND_MIXED_EULER; }
 constexpr int NBUF = 4;                // U, S0, S1, S2
 constexpr int MAX_SUBSTEPS = 16;       // steps an instance may take per batch step
 
 int kind_of(const hype_config &c)
 {
-    if (c.precision == HYPE_PREC_MIXED) return KIND_MIXED;
+    if (c.precision == HYPE_PREC_MIXED)
+        return c.system == HYPE_BAER_NUNZIATO ? KIND_MIXED_BN : c.system == HYPE_EULER ? KIND_MIXED_EULER : KIND_MIXED;
     const bool cons = (c.flags & HYPE_FLAG_CONSERVATIVE) != 0;
     if (c.flags & HYPE_FLAG_VISCOUS) return (cons ? KIND_VISC_CONS0 : KIND_VISC0) + c.order - 1;
     return (cons ? KIND_CONS0 : 0) + c.system * 4 + c.order;
@@ -168,7 +171,10 @@ static int inst_pitch(const hype_config &c)
 static size_t state_bytes(const hype_config &c)
 {
     const long long plane = (long long)inst_pitch(c) * c.ny;
-    if (c.precision == HYPE_PREC_MIXED) return (size_t)3 * plane * (4 * sizeof(float) + 2 * sizeof(double));
+    if (c.precision == HYPE_PREC_MIXED) {
+        const MixedLayout L = mixed_layout(c.system);
+        return (size_t)3 * plane * (L.nf * sizeof(float) + L.nd * sizeof(double));
+    }
     const int nbuf = c.order == 3 ? 4 : 3;
     size_t s = (size_t)nbuf * plane * hype_nvar(c.system) * sizeof(double);
     if (c.bc_left == HYPE_BC_INLET) s += sizeof(double) * 3 * (size_t)(c.ny + 6) * hype_nvar(c.system);
@@ -181,7 +187,7 @@ static size_t state_bytes(const hype_config &c)
 static int kind_blocks_per_sm(const Kind &k, int cells)
 {
     if (k.path >= 0) return cells == STAGE_CELLS ? path_batch_blocks_per_sm(k.path, k.system, k.order) : 0;
-    return k.mixed ? mixed_batch_blocks_per_sm(cells) : stage_batch_blocks_per_sm(k.system, k.order, cells);
+    return k.mixed ? mixed_batch_blocks_per_sm(k.system, cells) : stage_batch_blocks_per_sm(k.system, k.order, cells);
 }
 
 static int sub_init(hype_batch *b, SubList &l)
@@ -202,7 +208,7 @@ static int kind_init(hype_batch *b, int id, const hype_config &c)
     const int M = b->cfg.max_instances;
     k.system = c.system;
     k.order = c.order;
-    k.mixed = id == KIND_MIXED;
+    k.mixed = kind_is_mixed(id);
     k.path = path_of_kind(id);
     k.nstage = ssp_plan(c.order, k.plan, &k.copy_back);
     // the grid form of a path kind's kernel seeds each instance's dt
@@ -275,6 +281,7 @@ static MixedParams inst_mparams(hype_batch *b, const Inst &in, const PlanStage &
     p.nx = c.nx; p.ny = c.ny; p.pitch = in.pitch; p.plane = in.plane;
     p.bc[0] = c.bc_left; p.bc[1] = c.bc_right; p.bc[2] = c.bc_bottom; p.bc[3] = c.bc_top;
     p.eos.g1 = c.gamma1; p.eos.g2 = c.gamma2; p.eos.pi1 = c.pi1; p.eos.pi2 = c.pi2;
+    p.eos.fix_p2 = (c.flags & HYPE_FLAG_BN_FIX_P2) ? 1 : 0;
     p.r1_h = 1. / in.h; p.cfl_h = in.cfl_h;
     p.in_f = in.mf[q.in]; p.in_d = in.md[q.in];
     if (q.x >= 0) { p.xn_f = in.mf[q.x]; p.xn_d = in.md[q.x]; }
@@ -294,8 +301,9 @@ static int inst_maps(hype_batch *b, const Kind &k, const Inst &in, CUtensorMap *
         CUresult r;
         if (k.mixed) {
             const int bw = mixed_box_width(k.cells);
-            r = encode_planes_map(&mmaps[q].f, in.mf[q], true, c.nx, c.ny, 4, in.pitch, in.plane, bw);
-            if (r == CUDA_SUCCESS) r = encode_planes_map(&mmaps[q].d, in.md[q], false, c.nx, c.ny, 2, in.pitch, in.plane, bw);
+            const MixedLayout L = mixed_layout(c.system);
+            r = encode_planes_map(&mmaps[q].f, in.mf[q], true, c.nx, c.ny, L.nf, in.pitch, in.plane, bw);
+            if (r == CUDA_SUCCESS) r = encode_planes_map(&mmaps[q].d, in.md[q], false, c.nx, c.ny, L.nd, in.pitch, in.plane, bw);
         } else {
             r = encode_planes_map(&maps[q], in.buf[q], false, c.nx, c.ny, in.nv, in.pitch, in.plane, stage_box_width(k.cells));
         }
@@ -457,7 +465,7 @@ static cudaError_t enqueue_kind_stage(hype_batch *b, int id, int st, cudaStream_
     const int M = b->cfg.max_instances;
     const int blocks = b->sms * k.bps;
     const PlanStage &q = k.plan[st];
-    if (k.mixed) return launch_mixed_batch(k.cells, k.dMParams + st * M, k.dMMaps + q.in * M, l.dWork, l.dSched, blocks, s);
+    if (k.mixed) return launch_mixed_batch(k.system, k.cells, k.dMParams + st * M, k.dMMaps + q.in * M, l.dWork, l.dSched, blocks, s);
     if (k.path >= 0) return launch_path_batch(k.path, k.system, k.order, k.dParams + st * M, k.dMaps + q.in * M, l.dWork, l.dSched, blocks, s);
     return launch_stage_batch(k.system, k.order, k.cells, k.dParams + st * M, k.dMaps + q.in * M, l.dWork, l.dSched, blocks, s);
 }
@@ -678,12 +686,13 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     in.plane = (long long)in.pitch * cfg->ny;
     in.h = (cfg->x_max - cfg->x_min) / (double)cfg->nx;   // hype.c:57
     in.cfl_h = cfg->cfl * in.h;                           // rhs_function_prim.c:620
-    const bool mixed = in.kind == KIND_MIXED;
+    const bool mixed = kind_is_mixed(in.kind);
     bool ok = true;
     if (mixed) {
+        const MixedLayout L = mixed_layout(cfg->system);
         for (int q = 0; q < 3 && ok; ++q)
-            ok = pool_alloc(b, &in.mf[q], sizeof(float) * 4 * (size_t)in.plane) == cudaSuccess &&
-                 pool_alloc(b, &in.md[q], sizeof(double) * 2 * (size_t)in.plane) == cudaSuccess;
+            ok = pool_alloc(b, &in.mf[q], sizeof(float) * L.nf * (size_t)in.plane) == cudaSuccess &&
+                 pool_alloc(b, &in.md[q], sizeof(double) * L.nd * (size_t)in.plane) == cudaSuccess;
     } else {
         const int nbuf = cfg->order == 3 ? 4 : 3;
         for (int q = 0; q < nbuf && ok; ++q) ok = pool_alloc(b, &in.buf[q], sizeof(double) * in.nv * (size_t)in.plane) == cudaSuccess;
@@ -704,7 +713,7 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
     if (!tab.empty()) BCUDA(b, cudaMemcpyAsync(in.inlet, tab.data(), sizeof(double) * tab.size(), cudaMemcpyHostToDevice, b->stream));
     const size_t aos_bytes = sizeof(double) * (size_t)cfg->nx * cfg->ny * in.nv;
     BCUDA(b, cudaMemcpyAsync(b->dStage, U0, aos_bytes, cudaMemcpyHostToDevice, b->stream));
-    if (mixed) BCUDA(b, launch_aos_to_mixed(b->dStage, in.mf[0], in.md[0], cfg->nx, cfg->ny, in.pitch, in.plane, b->stream));
+    if (mixed) BCUDA(b, launch_aos_to_mixed(cfg->system, b->dStage, in.mf[0], in.md[0], cfg->nx, cfg->ny, in.pitch, in.plane, b->stream));
     else BCUDA(b, launch_aos_to_planes(b->dStage, in.buf[B_U], cfg->nx, cfg->ny, in.nv, in.pitch, in.plane, b->stream));
     // time loop of this instance (hype_begin): t0, t_final, max_steps, dt from the RHS of U0
     DevScalars &h = b->hSc[s];
@@ -732,7 +741,7 @@ int hype_batch_add(hype_batch *b, const hype_config *cfg, const double *U0, doub
         if ((rc = inst_maps(b, k, in, nullptr, mm))) return rc;
         MixedParams p = inst_mparams(b, in, seed);
         p.out_rhs = b->dStage;
-        BCUDA(b, launch_mixed(k.cells, mm[0], p, b->stream));
+        BCUDA(b, launch_mixed(cfg->system, k.cells, mm[0], p, b->stream));
     } else {
         CUtensorMap tm[3];
         if ((rc = inst_maps(b, k, in, tm, nullptr))) return rc;
@@ -845,7 +854,7 @@ int hype_batch_get_state(hype_batch *b, int id, double *U)
     BCUDA(b, cudaSetDevice(b->cfg.device));
     const Inst &in = b->inst[id];
     const hype_config &c = in.cfg;
-    if (in.kind == KIND_MIXED) BCUDA(b, launch_mixed_to_aos(in.mf[0], in.md[0], b->dStage, c.nx, c.ny, in.pitch, in.plane, b->stream));
+    if (kind_is_mixed(in.kind)) BCUDA(b, launch_mixed_to_aos(c.system, in.mf[0], in.md[0], b->dStage, c.nx, c.ny, in.pitch, in.plane, b->stream));
     else BCUDA(b, launch_planes_to_aos(in.buf[B_U], b->dStage, c.nx, c.ny, in.nv, in.pitch, in.plane, b->stream));
     BCUDA(b, cudaMemcpyAsync(U, b->dStage, sizeof(double) * (size_t)c.nx * c.ny * in.nv, cudaMemcpyDeviceToHost, b->stream));
     BCUDA(b, cudaStreamSynchronize(b->stream));

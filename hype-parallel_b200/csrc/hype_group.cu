@@ -334,7 +334,7 @@ int hype_group_set_state(hype_group *g, const double *U)
             r += len;
         }
         if (s->mixed)
-            G_TRY(g, launch_aos_to_mixed(s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[0] - (long long)lo * s->pitch,
+            G_TRY(g, launch_aos_to_mixed(s->cfg.system, s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[0] - (long long)lo * s->pitch,
                                          s->md[0] - (long long)lo * s->pitch, nx, g->rows[k] + lo + hi, s->pitch, s->plane, s->stream));
         else
             G_TRY(g, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dU), nx, 3 - lo, g->rows[k] + lo + hi, nv, s->pitch,
@@ -352,7 +352,7 @@ int hype_group_get_state(hype_group *g, double *U)
     for (int k = 0; k < g->n; ++k) {
         hype_solver *s = g->slab[k];
         G_TRY(g, cudaSetDevice(g->dev[k]));
-        if (s->mixed) G_TRY(g, launch_mixed_to_aos(s->mf[0], s->md[0], s->dAosOut, nx, g->rows[k], s->pitch, s->plane, s->stream));
+        if (s->mixed) G_TRY(g, launch_mixed_to_aos(s->cfg.system, s->mf[0], s->md[0], s->dAosOut, nx, g->rows[k], s->pitch, s->plane, s->stream));
         else G_TRY(g, launch_planes_to_aos(s->dU, s->dAosOut, nx, g->rows[k], nv, s->pitch, s->plane, s->stream));
         G_TRY(g, cudaMemcpyAsync(U + (size_t)g->row0[k] * row_elems, s->dAosOut, sizeof(double) * row_elems * g->rows[k],
                                  cudaMemcpyDeviceToHost, s->stream));

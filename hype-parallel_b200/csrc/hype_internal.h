@@ -155,10 +155,11 @@ cudaError_t launch_totals(const double *planes, double *red, int nx, int ny, int
 constexpr size_t TOTALS_SCRATCH = 64 + 513 * 11;
 
 // ---------------------------------------------------------------------------
-// Mixed precision (Kapila five-equation model, N = 2).  State: four FP32
-// planes (a1 rho1, a2 rho2, rho u, rho v) and two FP64 planes (E, a1) with one
-// element pitch; the FP64 pair carries the quantities whose stiffened-gas
-// cancellation (p from E with P_inf ~ 6e8) FP32 cannot resolve.
+// Mixed precision (N = 2, primitive path; Kapila, Baer-Nunziato, Euler).  State:
+// FP32 planes for densities and momenta, FP64 planes for the energies and the
+// volume fraction (MixedLayout), with one element pitch; the FP64 planes carry
+// the quantities whose stiffened-gas cancellation (p from E with P_inf ~ 6e8)
+// FP32 cannot resolve.
 // ---------------------------------------------------------------------------
 struct MixedParams {
     int nx, ny, pitch;          // element pitch of every plane (multiple of 32)
@@ -185,24 +186,47 @@ struct MixedParams {
     int skip_loads, skip_loads_from;   // test hook, as in StageParams
 };
 struct MixedMaps {
-    CUtensorMap f;              // FP32 planes: (nx, ny, 4), box (cells + 8, 1, 4)
-    CUtensorMap d;              // FP64 planes: (nx, ny, 2), box (cells + 8, 1, 2)
+    CUtensorMap f;              // FP32 planes: (nx, ny, nf), box (cells + 8, 1, nf)
+    CUtensorMap d;              // FP64 planes: (nx, ny, nd), box (cells + 8, 1, nd)
 };
+// Which conserved components a mixed state keeps in FP64 (bit c of dmask): the
+// FP32 planes hold the other components in ascending order, the FP64 planes these.
+//   Kapila:         a1 rho1, a2 rho2, rho u, rho v | E, a1
+//   Baer-Nunziato:  a1 rho1, a1 rho1 u1, a1 rho1 v1, a2 rho2, a2 rho2 u2, a2 rho2 v2 | a1 E1, a2 E2, a1
+//   Euler:          rho, rho u, rho v | E
+struct MixedLayout {
+    int nf, nd;
+    unsigned dmask;
+};
+inline MixedLayout mixed_layout(int sys)
+{
+    if (sys == SYS_BN) return MixedLayout{6, 3, (1u << 3) | (1u << 7) | (1u << 8)};
+    if (sys == SYS_EULER) return MixedLayout{3, 1, 1u << 3};
+    return MixedLayout{4, 2, (1u << 4) | (1u << 5)};
+}
 constexpr int MIXED_CELLS = 128;
 inline int mixed_box_width(int cells) { return cells + 8; }
 // strips with origins 4*floor(s*nx/(4S)) (16-byte aligned FP32 TMA origin):
 // S = ceil(nx/(cells-6)) keeps every strip within cells-2 columns
 inline int mixed_strips(int nx, int cells) { return (nx + (cells - 6) - 1) / (cells - 6); }
-size_t mixed_smem_bytes(int cells);
+size_t mixed_smem_bytes(int sys, int cells);
 int mixed_threads(int cells);
-int mixed_blocks_per_sm(int cells);
-int mixed_batch_blocks_per_sm(int cells);
-cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s);
-cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
+int mixed_blocks_per_sm(int sys, int cells);
+int mixed_batch_blocks_per_sm(int sys, int cells);
+cudaError_t launch_mixed(int sys, int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s);
+cudaError_t launch_mixed_batch(int sys, int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
                                int blocks, cudaStream_t s);
-// layout changes between the interleaved FP64 Vec and the mixed planes
-cudaError_t launch_aos_to_mixed(const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane, cudaStream_t s);
-cudaError_t launch_mixed_to_aos(const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane, cudaStream_t s);
+// the Baer-Nunziato and Euler tiles (hype_stage_mixed_sys.cu), behind the functions above
+size_t mixsys_smem_bytes(int sys, int cells);
+int mixsys_blocks_per_sm(int sys, int cells, bool batch);
+cudaError_t launch_mixsys(int sys, int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s);
+cudaError_t launch_mixsys_batch(int sys, int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
+                                int blocks, cudaStream_t s);
+// layout changes between the interleaved FP64 Vec and the mixed planes of system sys
+cudaError_t launch_aos_to_mixed(int sys, const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane,
+                                cudaStream_t s);
+cudaError_t launch_mixed_to_aos(int sys, const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane,
+                                cudaStream_t s);
 
 // hype_io.cu: PDECons2Prim of every cell, planes -> interleaved primitive variables
 cudaError_t launch_cons2prim(int sys, const Eos &eos, const double *planes, double *prim_aos, int nx, int ny, int pitch,

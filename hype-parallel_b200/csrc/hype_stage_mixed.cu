@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 #include "hype_internal.h"
 #include "hype_tma.cuh"
+#include "hype_mixed_common.cuh"
 
 namespace hype {
 
@@ -65,48 +66,6 @@ struct PrimM {
     float r1, r2, u, v;
     double p, a;
 };
-
-__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
-
-// One direction of WENO3 (reconstruction.c:157-178) on deviations from the
-// cell value, weights gamma_k / (IS_k + eps)^4 scaled by min_k (IS_k + eps)^4.
-__device__ __forceinline__ void weno3_1d_f(float dm2, float dm1, float dp1, float dp2, float &slope, float &curv)
-{
-    const float ux0 = -2.0f * dm1 + 0.5f * dm2, uxx0 = 0.5f * (dm2 - 2.0f * dm1);
-    const float ux1 = 0.5f * (dp1 - dm1), uxx1 = 0.5f * (dm1 + dp1);
-    const float ux2 = 2.0f * dp1 - 0.5f * dp2, uxx2 = 0.5f * (dp2 - 2.0f * dp1);
-    const float r13 = 13.0f / 3.0f, eps = 1.0e-12f;
-    const float a0 = ux0 * ux0 + r13 * uxx0 * uxx0 + eps;
-    const float a1 = ux1 * ux1 + r13 * uxx1 * uxx1 + eps;
-    const float a2 = ux2 * ux2 + r13 * uxx2 * uxx2 + eps;
-    const float mn = fminf(a0, fminf(a1, a2));
-    float q0 = fdiv(mn, a0), q1 = fdiv(mn, a1), q2 = fdiv(mn, a2);
-    q0 *= q0; q1 *= q1; q2 *= q2;
-    const float w0 = q0 * q0, w1 = 100.0f * (q1 * q1), w2 = q2 * q2;
-    const float inv = fdiv(1.0f, w0 + w1 + w2);
-    slope = (w0 * ux0 + w1 * ux1 + w2 * ux2) * inv;
-    curv = (w0 * uxx0 + w1 * uxx1 + w2 * uxx2) * inv;
-}
-
-// reconstruction.c:144-221 on deviations (u_0 = 0): coefficients k = 1..5
-__device__ __forceinline__ void weno3_f(const float *d, float *c)
-{
-    // d: xm2 xm1 xp1 xp2 ym2 ym1 yp1 yp2 pp pm mp mm
-    weno3_1d_f(d[0], d[1], d[2], d[3], c[0], c[2]);
-    weno3_1d_f(d[4], d[5], d[6], d[7], c[1], c[3]);
-    const float c1 = c[0], c2 = c[1], c3 = c[2], c4 = c[3];
-    const float x0 = d[8] - c1 - c2 - c3 - c4;
-    const float x1 = -d[9] + c1 - c2 + c3 + c4;
-    const float x2 = -d[10] - c1 + c2 + c3 + c4;
-    const float x3 = d[11] + c1 + c2 - c3 - c4;
-    const float tmp = 4.0f * (c3 * c3 + c4 * c4) + 1.0e-12f;
-    const float a0 = tmp + x0 * x0, a1 = tmp + x1 * x1, a2 = tmp + x2 * x2, a3 = tmp + x3 * x3;
-    const float mn = fminf(fminf(a0, a1), fminf(a2, a3));
-    float q0 = fdiv(mn, a0), q1 = fdiv(mn, a1), q2 = fdiv(mn, a2), q3 = fdiv(mn, a3);
-    q0 *= q0; q1 *= q1; q2 *= q2; q3 *= q3;
-    const float w0 = q0 * q0, w1 = q1 * q1, w2 = q2 * q2, w3 = q3 * q3;
-    c[4] = (w0 * x0 + w1 * x1 + w2 * x2 + w3 * x3) * fdiv(1.0f, w0 + w1 + w2 + w3);
-}
 
 // sum_{k>=1} c[k-1] phi(k) at face F, Gauss point q (run time 0/1)
 template <int F>
@@ -192,12 +151,6 @@ __device__ __forceinline__ float riemann_mixed(const MixedEos &e, const PrimM &L
     const float da = (float)(R.a - L.a);
     D5 = DIR == 0 ? (uav * da - K * (R.u - L.u)) : (vav * da - K * (R.v - L.v));
     return s;
-}
-
-__device__ __forceinline__ float minmod_f(float a, float b)
-{
-    if (a * b < 0.0f) return 0.0f;
-    return (fabsf(a) < fabsf(b)) ? a : b;
 }
 
 // SLAB: a y-slab of a decomposed grid (row offset, edge rows stored into the
@@ -679,7 +632,7 @@ static MixedEntry mixed_entry_of()
 }
 static MixedEntry mixed_entry(int cells) { return cells == 64 ? mixed_entry_of<64>() : mixed_entry_of<128>(); }
 
-size_t mixed_smem_bytes(int cells) { return mixed_entry(cells).smem; }
+size_t mixed_smem_bytes(int sys, int cells) { return sys == SYS_KAPILA ? mixed_entry(cells).smem : mixsys_smem_bytes(sys, cells); }
 int mixed_threads(int cells) { return 2 * cells; }
 
 static cudaError_t mixed_configure(int cells)
@@ -691,8 +644,9 @@ static cudaError_t mixed_configure(int cells)
     return cudaFuncSetAttribute(e.batch, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)e.smem);
 }
 
-int mixed_blocks_per_sm(int cells)
+int mixed_blocks_per_sm(int sys, int cells)
 {
+    if (sys != SYS_KAPILA) return mixsys_blocks_per_sm(sys, cells, false);
     const MixedEntry e = mixed_entry(cells);
     int nb = 0;
     if (mixed_configure(cells) != cudaSuccess) return 0;
@@ -700,8 +654,9 @@ int mixed_blocks_per_sm(int cells)
     return nb;
 }
 
-int mixed_batch_blocks_per_sm(int cells)
+int mixed_batch_blocks_per_sm(int sys, int cells)
 {
+    if (sys != SYS_KAPILA) return mixsys_blocks_per_sm(sys, cells, true);
     const MixedEntry e = mixed_entry(cells);
     int nb = 0;
     if (mixed_configure(cells) != cudaSuccess) return 0;
@@ -709,8 +664,9 @@ int mixed_batch_blocks_per_sm(int cells)
     return nb;
 }
 
-cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s)
+cudaError_t launch_mixed(int sys, int cells, const MixedMaps &maps, const MixedParams &p, cudaStream_t s)
 {
+    if (sys != SYS_KAPILA) return launch_mixsys(sys, cells, maps, p, s);
     const MixedEntry e = mixed_entry(cells);
     MixedMaps mm = maps;
     MixedParams pp = p;
@@ -718,46 +674,55 @@ cudaError_t launch_mixed(int cells, const MixedMaps &maps, const MixedParams &p,
     return cudaLaunchKernel(p.row_off ? e.slab : e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
-cudaError_t launch_mixed_batch(int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
+cudaError_t launch_mixed_batch(int sys, int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
                                int blocks, cudaStream_t s)
 {
+    if (sys != SYS_KAPILA) return launch_mixsys_batch(sys, cells, inst, maps, work, sched, blocks, s);
     const MixedEntry e = mixed_entry(cells);
     void *args[] = {&inst, &maps, &work, &sched};
     return cudaLaunchKernel(e.batch, dim3((unsigned)blocks, 1, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
-// interleaved FP64 Vec (6 per cell) <-> mixed planes
+// interleaved FP64 Vec (nv per cell) <-> mixed planes: component c goes to FP64
+// plane popc(dmask below c) where bit c of dmask is set, else to FP32 plane
+// popc(~dmask below c) (MixedLayout)
 __global__ void aos_to_mixed_kernel(const double *__restrict__ aos, float *__restrict__ pf, double *__restrict__ pd, int nx,
-                                    int ny, int pitch, long long plane)
+                                    int ny, int pitch, long long plane, int nv, unsigned dmask)
 {
     const long long n = (long long)nx * ny;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * 6; k += (long long)gridDim.x * blockDim.x) {
-        const long long cell = k / 6;
-        const int c = (int)(k % 6);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * nv; k += (long long)gridDim.x * blockDim.x) {
+        const long long cell = k / nv;
+        const int c = (int)(k % nv);
         const long long gi = (cell / nx) * pitch + cell % nx;
-        if (c < 4) pf[c * plane + gi] = (float)aos[k];
-        else pd[(c - 4) * plane + gi] = aos[k];
+        const unsigned below = (1u << c) - 1u;
+        if ((dmask >> c) & 1u) pd[__popc(dmask & below) * plane + gi] = aos[k];
+        else pf[__popc(~dmask & below) * plane + gi] = (float)aos[k];
     }
 }
 __global__ void mixed_to_aos_kernel(const float *__restrict__ pf, const double *__restrict__ pd, double *__restrict__ aos, int nx,
-                                    int ny, int pitch, long long plane)
+                                    int ny, int pitch, long long plane, int nv, unsigned dmask)
 {
     const long long n = (long long)nx * ny;
-    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * 6; k += (long long)gridDim.x * blockDim.x) {
-        const long long cell = k / 6;
-        const int c = (int)(k % 6);
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < n * nv; k += (long long)gridDim.x * blockDim.x) {
+        const long long cell = k / nv;
+        const int c = (int)(k % nv);
         const long long gi = (cell / nx) * pitch + cell % nx;
-        aos[k] = c < 4 ? (double)pf[c * plane + gi] : pd[(c - 4) * plane + gi];
+        const unsigned below = (1u << c) - 1u;
+        aos[k] = ((dmask >> c) & 1u) ? pd[__popc(dmask & below) * plane + gi] : (double)pf[__popc(~dmask & below) * plane + gi];
     }
 }
-cudaError_t launch_aos_to_mixed(const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane, cudaStream_t s)
+cudaError_t launch_aos_to_mixed(int sys, const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane,
+                                cudaStream_t s)
 {
-    aos_to_mixed_kernel<<<1184, 256, 0, s>>>(aos, pf, pd, nx, ny, pitch, plane);
+    const MixedLayout L = mixed_layout(sys);
+    aos_to_mixed_kernel<<<1184, 256, 0, s>>>(aos, pf, pd, nx, ny, pitch, plane, L.nf + L.nd, L.dmask);
     return cudaGetLastError();
 }
-cudaError_t launch_mixed_to_aos(const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane, cudaStream_t s)
+cudaError_t launch_mixed_to_aos(int sys, const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane,
+                                cudaStream_t s)
 {
-    mixed_to_aos_kernel<<<1184, 256, 0, s>>>(pf, pd, aos, nx, ny, pitch, plane);
+    const MixedLayout L = mixed_layout(sys);
+    mixed_to_aos_kernel<<<1184, 256, 0, s>>>(pf, pd, aos, nx, ny, pitch, plane, L.nf + L.nd, L.dmask);
     return cudaGetLastError();
 }
 

@@ -65,7 +65,7 @@ def test_config_defaults_follow_reference_main(hp):
     (dict(cfl=0.0), "CFL"),
     (dict(x_max=0.0), "domain"),
     (dict(precision=7), "precision"),
-    (dict(precision=1, system=2), "Kapila"),
+    (dict(precision=1, system=2, order=3), "N = 2"),
     (dict(precision=1, order=1), "N = 2"),
     (dict(precision=1, order=2, flags=2), "FP64 only"),
     (dict(flags=8), "unknown flags"),
