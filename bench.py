@@ -298,14 +298,19 @@ def batch_leg(hp, args, local_rank):
 
 
 def bn_leg(hp, args, local_rank):
-    """Baer-Nunziato 1024 x 1024, FP64, N = 2, 200 SSPRK(4,3) steps on the seeded
+    """Baer-Nunziato 1024 x 1024, N = 2, 200 SSPRK(4,3) steps on the seeded
     disc state (alpha_1 from 8 tanh discs, Fourier velocities |u| <= 50,
-    p in [1e5, 1e7]; stiffened gases 4.4/6e8 and 1.4/0), in both flux forms:
-    as the reference writes it (phase-2 flux pressure V[8]) and fixed (V[7])."""
+    p in [1e5, 1e7]; stiffened gases 4.4/6e8 and 1.4/0): FP64 in both flux forms,
+    as the reference writes it (phase-2 flux pressure V[8]) and fixed (V[7]), and
+    the fixed form in mixed precision with each field's relative L1 / L-infinity
+    error against the FP64 run after the 200 steps."""
     out = {}
     n = 1024
-    for name, flags in (("reference_form", 0), ("fixed_p2", hp.FLAG_BN_FIX_P2)):
-        cfg = hp.Config(system=hp.BAER_NUNZIATO, order=2, nx=n, ny=n, cfl=0.4, device=local_rank, flags=flags)
+    states = {}
+    runs = (("reference_form", 0, hp.PREC_FP64), ("fixed_p2", hp.FLAG_BN_FIX_P2, hp.PREC_FP64),
+            ("mixed_fixed_p2", hp.FLAG_BN_FIX_P2, hp.PREC_MIXED))
+    for name, flags, prec in runs:
+        cfg = hp.Config(system=hp.BAER_NUNZIATO, order=2, nx=n, ny=n, cfl=0.4, device=local_rank, flags=flags, precision=prec)
         U0 = hp.initial_state(cfg, "bn_discs", seed=SEED)
         with hp.Solver(cfg) as s:
             s.set_state(U0)
@@ -316,12 +321,31 @@ def bn_leg(hp, args, local_rank):
             ms = s.last_elapsed_ms()
             ms_stage = s.time_stage(10)
             tot, amin, amax = s.totals()
+            states[name] = s.get_state().reshape(-1, 9)
+        bpc = 2 * (6 * 4 + 3 * 8) if prec == hp.PREC_MIXED else 2 * 9 * 8
         out[name] = {"steps_done": steps, "status": st, "t_end": t,
                      "value": n * n * steps / (ms * 1e-3) if steps else None, "unit": UNIT,
                      "ms_per_step": ms / steps if steps else None, "stage_ms_per_launch": ms_stage,
-                     "stage_roofline_GBs": (2 * 9 * 8) * n * n / (ms_stage * 1e-3) / 1e9, "autotuned_tile": tile,
+                     "stage_roofline_GBs": bpc * n * n / (ms_stage * 1e-3) / 1e9, "autotuned_tile": tile,
                      "alpha_min": amin, "alpha_max": amax}
-    out["workload"] = "bn9 discs 1024x1024 fp64, N=2 SSPRK(4,3), 200 steps"
+    m, f = out["mixed_fixed_p2"], out["fixed_p2"]
+    if m["value"] and f["value"]:
+        m["speedup_vs_fp64"] = m["value"] / f["value"]
+    if m["steps_done"] == f["steps_done"]:
+        M, F = states["mixed_fixed_p2"], states["fixed_p2"]
+
+        def rel(a, b):
+            return [float(np.abs(a - b).sum() / np.abs(b).sum()), float(np.abs(a - b).max() / np.abs(b).max())]
+        errs = {nm: rel(M[:, c], F[:, c]) for c, nm in ((0, "a1rho1"), (3, "a1E1"), (4, "a2rho2"), (7, "a2E2"), (8, "alpha1"))}
+        errs["rho"] = rel(M[:, 0] + M[:, 4], F[:, 0] + F[:, 4])
+        for nm, cols in (("momentum1_vector", [1, 2]), ("momentum2_vector", [5, 6])):
+            dm = np.sqrt(((M[:, cols] - F[:, cols]) ** 2).sum(axis=1))
+            mag = np.sqrt((F[:, cols] ** 2).sum(axis=1))
+            errs[nm] = [float(dm.sum() / mag.sum()), float(dm.max() / mag.max())]
+        m["rel_error_vs_fp64_after_run"] = {"fields_L1_Linf": errs, "steps": f["steps_done"]}
+    m["precision"] = "FP32 partial densities, momenta, velocities, reconstruction and their fluxes; FP64 phase energies, " \
+                     "alpha1, pressure recovery, totals, dt"
+    out["workload"] = "bn9 discs 1024x1024, N=2 SSPRK(4,3), 200 steps"
     out["note"] = ("the reference's flux form stops where the reference would MPI_Abort (inadmissible face state); "
                    "steps after the stop are skipped on the device, so its value counts the steps taken")
     return out
@@ -388,11 +412,11 @@ def group_leg(hp, args, local_rank, U0, U_ref):
             "bitwise_equal_to_single_solver": same}
 
 
-def euler_rate(hp, local_rank):
-    """FP64 Euler N = 2 at 1024^2 (four-quadrant state), cell-updates/s: the serving
-    mix's third system."""
+def euler_rate(hp, local_rank, prec):
+    """Euler N = 2 at 1024^2 (four-quadrant state) in precision `prec`,
+    cell-updates/s: the serving mix's third system."""
     cfg = hp.Config(system=hp.EULER, order=2, nx=1024, ny=1024, cfl=0.4, device=local_rank, gamma1=1.4, gamma2=1.4, pi1=0.0,
-                    pi2=0.0)
+                    pi2=0.0, precision=prec)
     with hp.Solver(cfg) as s:
         s.set_state(hp.initial_state(cfg, "euler_quadrants", seed=SEED))
         s.begin(0.0, 1e30, 1 << 30)
@@ -418,23 +442,23 @@ def serve_leg(hp, args, local_rank, rates):
     rng = np.random.default_rng(7)
     n = args.serve_requests
     T = hp.BC_TRANSMISSIVE
-    kap_prec = hp.PREC_MIXED if args.serve_kapila == "mixed" else hp.PREC_FP64
+    prec = hp.PREC_MIXED if args.serve_precision == "mixed" else hp.PREC_FP64
     reqs, work = [], []
     for i in range(n):
         u = rng.uniform()
         side = int(round(64 * 32 ** rng.uniform()))
         steps = int(round(50 * 40 ** rng.uniform()))
         if u < 0.7:
-            cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=side, ny=side, cfl=0.4, device=local_rank, precision=kap_prec)
+            cfg = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=side, ny=side, cfl=0.4, device=local_rank, precision=prec)
             ic, par = hp.IC_SHOCK_BUBBLE, int(rng.integers(1, 5))
         elif u < 0.9:
             # phase-2 flux pressure from V[7]; the reference's V[8] (baer_nunziato.c:271) aborts these runs early
             cfg = hp.Config(system=hp.BAER_NUNZIATO, order=2, nx=side, ny=side, cfl=0.4, device=local_rank,
-                            flags=hp.FLAG_BN_FIX_P2)
+                            flags=hp.FLAG_BN_FIX_P2, precision=prec)
             ic, par = hp.IC_BN_DISCS, 0
         else:
             cfg = hp.Config(system=hp.EULER, order=2, nx=side, ny=side, cfl=0.4, device=local_rank, gamma1=1.4, gamma2=1.4,
-                            pi1=0.0, pi2=0.0)
+                            pi1=0.0, pi2=0.0, precision=prec)
             ic, par = hp.IC_EULER_QUADRANTS, 0
         reqs.append(hp.Request(0.0, cfg, 0.0, 1e30, steps, ic, 5000 + i, par))
         work.append(side * side * steps)
@@ -473,7 +497,7 @@ def serve_leg(hp, args, local_rank, rates):
                  "status": res[i]["status"]} for i, r in enumerate(reqs) if res[i]["status"] != hp.OK][:40]
     return {"workload": f"Poisson stream of {n} solves: 70/20/10 kapila5/bn/euler, square grids 64..2048 log-uniform, "
                         "50..2000 steps log-uniform, N=2 SSPRK(4,3), 150 GB HBM budget",
-            "requests": n, "kapila_precision": args.serve_kapila, "active_cells": args.serve_active_cells,
+            "requests": n, "precision": args.serve_precision, "active_cells": args.serve_active_cells,
             "capacity_estimate": capacity, "capacity_from": {"rates": rates, "work_share": share,
                                                              "rule": "work-weighted harmonic mean of the systems' rates"},
             "substep_cells": args.serve_substep_cells, "bn_form": "phase-2 flux pressure from V[7]", "load_factor": rho, "rate_per_s": rate,
@@ -615,14 +639,15 @@ def run_gpu(args, rank, world, local_rank):
     batched = None if args.no_batch else batch_leg(hp, args, local_rank)
     serving = None
     if args.serve_requests > 0:
-        # per-system rates of this run: batched Kapila in the requests' precision, BN in
+        # per-system rates of this run in the requests' precision: batched Kapila, BN in
         # the fixed flux form, Euler measured here (fallbacks when a leg was skipped)
+        mixed_serve = args.serve_precision == "mixed"
         kap = None
         if batched:
-            kap = batched["batched_mixed" if args.serve_kapila == "mixed" else "batched_fp64"]["value"]
-        rates = {"kapila": kap or (value * (2.0 if args.serve_kapila == "mixed" else 1.0)),
-                 "bn": (bn or {}).get("fixed_p2", {}).get("value") or 0.5 * value,
-                 "euler": euler_rate(hp, local_rank)}
+            kap = batched["batched_mixed" if mixed_serve else "batched_fp64"]["value"]
+        rates = {"kapila": kap or (value * (2.0 if mixed_serve else 1.0)),
+                 "bn": (bn or {}).get("mixed_fixed_p2" if mixed_serve else "fixed_p2", {}).get("value") or 0.5 * value,
+                 "euler": euler_rate(hp, local_rank, hp.PREC_MIXED if mixed_serve else hp.PREC_FP64)}
         serving = serve_leg(hp, args, local_rank, rates)
 
     if rank != 0:
@@ -679,7 +704,7 @@ def main():
     ap.add_argument("--group-slabs", type=int, default=2, help="y-slabs of the decomposed leg on this GPU (<= 1: skip)")
     ap.add_argument("--batch-steps", type=int, default=300, help="steps of the batched-grids leg")
     ap.add_argument("--serve-requests", type=int, default=64, help="requests of the serving leg (0: skip)")
-    ap.add_argument("--serve-kapila", default="mixed", choices=["mixed", "fp64"], help="precision of Kapila requests")
+    ap.add_argument("--serve-precision", default="mixed", choices=["mixed", "fp64"], help="precision of the served requests")
     ap.add_argument("--serve-poll-ms", type=float, default=10.0)
     ap.add_argument("--serve-active-cells", type=int, default=4 << 20,
                     help="scheduler: cells stepped at once, least remaining work first (0: all resident requests)")
