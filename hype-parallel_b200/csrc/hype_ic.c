@@ -7,12 +7,17 @@
  * reference counterpart) or use the same 5x5 Gauss average (SmoothVortex,
  * kapila_5eqn.c:527-562, the case behind the reference's convergence table).
  * Deterministic for a given seed on every platform: splitmix64 + integer-exact
- * conversions, libm only for sqrt/tanh/sin/cos/erfc.
+ * conversions, libm only for sqrt/tanh/sin/cos/erfc.  The random parameters are
+ * drawn first; the cells are then filled row band by row band on up to 16 host
+ * threads (a cell's value does not depend on which thread computes it).
  */
+#define _POSIX_C_SOURCE 200809L
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 #include "../../include/hype_gpu.h"
 #include "../../include/hype_ic.h"
 
@@ -25,6 +30,35 @@ static uint64_t next_u64(rng_t *r)
     return z ^ (z >> 31);
 }
 static double unif(rng_t *r, double a, double b) { return a + (b - a) * ((double)(next_u64(r) >> 11) * (1.0 / 9007199254740992.0)); }
+
+/* fill(ctx, j0, j1) over rows 0..ny-1 in bands on host threads: one thread below
+ * 65536 cells, else up to min(16, online cores) */
+typedef void (*rows_fn)(const void *ctx, int j0, int j1);
+typedef struct { rows_fn fn; const void *ctx; int j0, j1; } band_t;
+static void *band_main(void *a)
+{
+    const band_t *b = (const band_t *)a;
+    b->fn(b->ctx, b->j0, b->j1);
+    return NULL;
+}
+static void par_rows(int nx, int ny, rows_fn fn, const void *ctx)
+{
+    long nproc = sysconf(_SC_NPROCESSORS_ONLN);
+    int T = (long long)nx * ny < 65536 ? 1 : (int)(nproc < 1 ? 1 : nproc > 16 ? 16 : nproc);
+    if (T > ny) T = ny;
+    pthread_t th[16];
+    band_t bands[16];
+    int started = 0;
+    for (int t = 1; t < T; ++t) {
+        bands[t] = (band_t){fn, ctx, (int)((long long)ny * t / T), (int)((long long)ny * (t + 1) / T)};
+        if (pthread_create(&th[t], NULL, band_main, &bands[t]) != 0) break;
+        started = t;
+    }
+    /* this thread takes band 0 and every band a thread could not be started for */
+    fn(ctx, 0, (int)((long long)ny / T));
+    if (started + 1 < T) fn(ctx, (int)((long long)ny * (started + 1) / T), ny);
+    for (int t = 1; t <= started; ++t) pthread_join(th[t], NULL);
+}
 
 /* Kapila primitive -> conserved (kapila_5eqn.c:41-61) */
 static void kap_p2c(const hype_config *c, const double *V, double *Q)
@@ -64,6 +98,36 @@ static void rh_state(double g, double pi, double p0, double rho0, double p1, dou
     *u1 = sqrt((p1 - p0) * (1.0 / rho0 - 1.0 / *rho1));
 }
 
+typedef struct {
+    const hype_config *c;
+    double *U;
+    double h, Lx, Ly, eps, p0, rho1, rho2, p1, r1s, u1s, r2s;
+    int nbubbles;
+    double bx[64], by[64], br[64];
+} sb_ctx;
+static void sb_rows(const void *ctx, int j0, int j1)
+{
+    const sb_ctx *k = (const sb_ctx *)ctx;
+    const hype_config *c = k->c;
+    const double h = k->h, Lx = k->Lx, Ly = k->Ly, eps = k->eps;
+    for (int j = j0; j < j1; ++j)
+        for (int i = 0; i < c->nx; ++i) {
+            const double x = c->x_min + (i + 0.5) * h, y = c->y_min + (j + 0.5) * h;
+            const double xn = (x - c->x_min) / Lx, yn = (y - c->y_min) / Ly;   /* unit-square coordinates */
+            double a1 = 1.0 - eps;
+            for (int b = 0; b < k->nbubbles; ++b) {
+                const double d = sqrt((xn - k->bx[b]) * (xn - k->bx[b]) + (yn - k->by[b]) * (yn - k->by[b]));
+                /* alpha_1 (phase 1 = liquid) drops to eps inside the bubble, tanh edge of width 2 cells */
+                const double ab = eps + (1.0 - 2.0 * eps) * 0.5 * (1.0 + tanh((d - k->br[b]) * Lx / (2.0 * h)));
+                if (ab < a1) a1 = ab;
+            }
+            double V[6];
+            if (xn < 0.1) { V[0] = k->r1s; V[1] = k->r2s; V[2] = k->u1s; V[3] = 0.0; V[4] = k->p1; V[5] = 1.0 - eps; }
+            else { V[0] = k->rho1; V[1] = k->rho2; V[2] = 0.0; V[3] = 0.0; V[4] = k->p0; V[5] = a1; }
+            kap_p2c(c, V, k->U + ((size_t)j * c->nx + i) * 6);
+        }
+}
+
 int hype_ic_shock_bubble(const hype_config *c, uint64_t seed, int nbubbles, double *U)
 {
     if (!c || !U || c->system != HYPE_KAPILA_5EQN || nbubbles < 0 || nbubbles > 64) return HYPE_ERR_INVALID;
@@ -77,23 +141,13 @@ int hype_ic_shock_bubble(const hype_config *c, uint64_t seed, int nbubbles, doub
     double r1s, u1s, r2s, u2s;
     rh_state(c->gamma1, c->pi1, p0, rho1, p1, &r1s, &u1s);   /* phase 1 carries the shock */
     rh_state(c->gamma2, c->pi2, p0, rho2, p1, &r2s, &u2s);   /* trace phase 2 compressed by the same jump */
-    const double Lx = c->x_max - c->x_min, Ly = c->y_max - c->y_min;
-    for (int j = 0; j < c->ny; ++j)
-        for (int i = 0; i < c->nx; ++i) {
-            const double x = c->x_min + (i + 0.5) * h, y = c->y_min + (j + 0.5) * h;
-            const double xn = (x - c->x_min) / Lx, yn = (y - c->y_min) / Ly;   /* unit-square coordinates */
-            double a1 = 1.0 - eps;
-            for (int b = 0; b < nbubbles; ++b) {
-                const double d = sqrt((xn - bx[b]) * (xn - bx[b]) + (yn - by[b]) * (yn - by[b]));
-                /* alpha_1 (phase 1 = liquid) drops to eps inside the bubble, tanh edge of width 2 cells */
-                const double ab = eps + (1.0 - 2.0 * eps) * 0.5 * (1.0 + tanh((d - br[b]) * Lx / (2.0 * h)));
-                if (ab < a1) a1 = ab;
-            }
-            double V[6];
-            if (xn < 0.1) { V[0] = r1s; V[1] = r2s; V[2] = u1s; V[3] = 0.0; V[4] = p1; V[5] = 1.0 - eps; }
-            else { V[0] = rho1; V[1] = rho2; V[2] = 0.0; V[3] = 0.0; V[4] = p0; V[5] = a1; }
-            kap_p2c(c, V, U + ((size_t)j * c->nx + i) * 6);
-        }
+    (void)u2s;
+    sb_ctx k = {c, U, h, c->x_max - c->x_min, c->y_max - c->y_min, eps, p0, rho1, rho2, p1, r1s, u1s, r2s, nbubbles,
+                {0}, {0}, {0}};
+    memcpy(k.bx, bx, sizeof(double) * nbubbles);
+    memcpy(k.by, by, sizeof(double) * nbubbles);
+    memcpy(k.br, br, sizeof(double) * nbubbles);
+    par_rows(c->nx, c->ny, sb_rows, &k);
     return HYPE_OK;
 }
 
@@ -116,6 +170,41 @@ static double field_at(const field_t *f, double x, double y, double lo, double h
     return lo + (hi - lo) * 0.5 * (1.0 + s / norm);
 }
 
+typedef struct {
+    const hype_config *c;
+    double *U;
+    double h, Lx, Ly, umax;
+    double dx[8], dy[8], dr[8];
+    field_t fr1, fr2, fu1, fv1, fu2, fv2, fp1, fp2;
+} bn_ctx;
+static void bn_rows(const void *ctx, int j0, int j1)
+{
+    const bn_ctx *K = (const bn_ctx *)ctx;
+    const hype_config *c = K->c;
+    const double h = K->h, Lx = K->Lx, Ly = K->Ly, umax = K->umax;
+    for (int j = j0; j < j1; ++j)
+        for (int i = 0; i < c->nx; ++i) {
+            const double xn = ((i + 0.5) * h) / Lx, yn = ((j + 0.5) * h) / Ly;
+            double a = 0.01;
+            for (int k = 0; k < 8; ++k) {
+                const double d = sqrt((xn - K->dx[k]) * (xn - K->dx[k]) + (yn - K->dy[k]) * (yn - K->dy[k]));
+                a += 0.98 * 0.5 * (1.0 - tanh((d - K->dr[k]) * Lx / (2.0 * h)));
+            }
+            if (a > 0.99) a = 0.99;
+            double V[9];
+            V[0] = 1000.0 * field_at(&K->fr1, xn, yn, 0.5, 2.0);
+            V[1] = field_at(&K->fu1, xn, yn, -umax, umax);
+            V[2] = field_at(&K->fv1, xn, yn, -umax, umax);
+            V[3] = field_at(&K->fp1, xn, yn, 1e5, 1e7);
+            V[4] = 1.0 * field_at(&K->fr2, xn, yn, 0.5, 2.0);
+            V[5] = field_at(&K->fu2, xn, yn, -umax, umax);
+            V[6] = field_at(&K->fv2, xn, yn, -umax, umax);
+            V[7] = field_at(&K->fp2, xn, yn, 1e5, 1e7);
+            V[8] = a;
+            bn_p2c(c, V, K->U + ((size_t)j * c->nx + i) * 9);
+        }
+}
+
 int hype_ic_bn_discs(const hype_config *c, uint64_t seed, double *U)
 {
     if (!c || !U || c->system != HYPE_BAER_NUNZIATO) return HYPE_ERR_INVALID;
@@ -127,28 +216,12 @@ int hype_ic_bn_discs(const hype_config *c, uint64_t seed, double *U)
     field_t fr1, fr2, fu1, fv1, fu2, fv2, fp1, fp2;
     field_init(&fr1, &r); field_init(&fr2, &r); field_init(&fu1, &r); field_init(&fv1, &r);
     field_init(&fu2, &r); field_init(&fv2, &r); field_init(&fp1, &r); field_init(&fp2, &r);
-    const double umax = 50.0 / sqrt(2.0);   /* |u| <= 50 */
-    for (int j = 0; j < c->ny; ++j)
-        for (int i = 0; i < c->nx; ++i) {
-            const double xn = ((i + 0.5) * h) / Lx, yn = ((j + 0.5) * h) / Ly;
-            double a = 0.01;
-            for (int k = 0; k < 8; ++k) {
-                const double d = sqrt((xn - dx[k]) * (xn - dx[k]) + (yn - dy[k]) * (yn - dy[k]));
-                a += 0.98 * 0.5 * (1.0 - tanh((d - dr[k]) * Lx / (2.0 * h)));
-            }
-            if (a > 0.99) a = 0.99;
-            double V[9];
-            V[0] = 1000.0 * field_at(&fr1, xn, yn, 0.5, 2.0);
-            V[1] = field_at(&fu1, xn, yn, -umax, umax);
-            V[2] = field_at(&fv1, xn, yn, -umax, umax);
-            V[3] = field_at(&fp1, xn, yn, 1e5, 1e7);
-            V[4] = 1.0 * field_at(&fr2, xn, yn, 0.5, 2.0);
-            V[5] = field_at(&fu2, xn, yn, -umax, umax);
-            V[6] = field_at(&fv2, xn, yn, -umax, umax);
-            V[7] = field_at(&fp2, xn, yn, 1e5, 1e7);
-            V[8] = a;
-            bn_p2c(c, V, U + ((size_t)j * c->nx + i) * 9);
-        }
+    bn_ctx k = {c, U, h, Lx, Ly, 50.0 / sqrt(2.0) /* |u| <= 50 */, {0}, {0}, {0},
+                fr1, fr2, fu1, fv1, fu2, fv2, fp1, fp2};
+    memcpy(k.dx, dx, sizeof(dx));
+    memcpy(k.dy, dy, sizeof(dy));
+    memcpy(k.dr, dr, sizeof(dr));
+    par_rows(c->nx, c->ny, bn_rows, &k);
     return HYPE_OK;
 }
 

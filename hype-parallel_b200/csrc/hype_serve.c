@@ -2,18 +2,22 @@
  * hype_serve.c -- the request loop of include/hype_serve.h, in C over the
  * batch ABI (include/hype_batch.h).
  *
- * One iteration of the loop:
- *   1. admit, in arrival order, every request that has arrived while the
- *      batch has a free slot and HBM budget for it (its initial state is
- *      built on the host, uploaded, and its dt seeded by one RHS evaluation);
- *      a request that does not fit waits at the head of the queue until
- *      finished instances free their memory;
+ * Initial states are built by a host thread (the stager) into a ring of
+ * pinned buffers, each request from its arrival on and in arrival order, its
+ * cells filled on several threads (hype_ic.c), while the GPU steps the
+ * resident requests; a fill callback (HYPE_IC_CALLBACK) is therefore called
+ * from that thread.  One iteration of the loop:
+ *   1. admit, in arrival order, every request whose initial state is built
+ *      while the batch has a free slot and HBM budget for it (the state is
+ *      uploaded and its dt seeded by one RHS evaluation); a request that does
+ *      not fit waits at the head of the queue until finished instances free
+ *      their memory; the loop waits for the stager only when nothing is
+ *      resident;
  *   2. choose which resident requests step (least remaining work first, up
  *      to active_cells cells; the others are held; a small grid takes up to
  *      substep_cells / cells steps per batch step), enqueue k steps of the
  *      batch (k graph replays, k sized so that they take about poll_ms of GPU
- *      time); while they run, build the initial state of the next waiting
- *      request on the host; then wait;
+ *      time) and wait for them;
  *   3. retire every instance whose time loop ended: copy its state out, hand
  *      it to the sink, free its slot and memory.
  * Instances stop on the device at their own t_final / max_steps, so the k
@@ -21,6 +25,7 @@
  */
 #define _POSIX_C_SOURCE 200809L
 #include <math.h>
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -145,6 +150,85 @@ static int make_initial(const hype_request *r, int index, hype_fill_fn fill, voi
     }
 }
 
+/* the stager: initial states of the requests, in order, from each one's arrival on */
+#define NSTAGE 3
+typedef struct {
+    pthread_t th;
+    int started;
+    pthread_mutex_t mu;
+    pthread_cond_t cv;
+    const hype_request *req;
+    int n;
+    hype_fill_fn fill;
+    void *ctx;
+    int realtime;
+    double t_start;
+    long long max_cells;
+    double *buf[NSTAGE];
+    int req_of[NSTAGE];   /* request index built (or being built) in the buffer; -1: free */
+    int ready[NSTAGE];    /* 1: built, status in rc[] */
+    int rc[NSTAGE];
+    int next;             /* next request to build */
+    int stop;
+} stager_t;
+
+static void *stager_main(void *a)
+{
+    stager_t *g = (stager_t *)a;
+    pthread_mutex_lock(&g->mu);
+    while (!g->stop && g->next < g->n) {
+        int k = -1;
+        for (int q = 0; q < NSTAGE; ++q)
+            if (g->req_of[q] < 0) { k = q; break; }
+        const hype_request *r = &g->req[g->next];
+        const double wait = g->realtime ? r->arrival_s - (now_s() - g->t_start) : 0.0;
+        if (k < 0) {   /* every buffer holds a request not yet admitted */
+            pthread_cond_wait(&g->cv, &g->mu);
+            continue;
+        }
+        if (wait > 0.0) {   /* not arrived yet */
+            struct timespec ts;
+            clock_gettime(CLOCK_REALTIME, &ts);
+            const double until = (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec + (wait < 0.05 ? wait : 0.05);
+            ts.tv_sec = (time_t)until;
+            ts.tv_nsec = (long)((until - (double)ts.tv_sec) * 1e9);
+            pthread_cond_timedwait(&g->cv, &g->mu, &ts);
+            continue;
+        }
+        const int i = g->next++;
+        g->req_of[k] = i;
+        g->ready[k] = 0;
+        pthread_mutex_unlock(&g->mu);
+        int rc = HYPE_OK;
+        if (hype_batch_instance_bytes(&r->cfg) == 0 || (long long)r->cfg.nx * r->cfg.ny > g->max_cells) rc = HYPE_ERR_INVALID;
+        else rc = make_initial(r, i, g->fill, g->ctx, g->buf[k]);
+        pthread_mutex_lock(&g->mu);
+        g->rc[k] = rc;
+        g->ready[k] = 1;
+        pthread_cond_broadcast(&g->cv);
+    }
+    pthread_mutex_unlock(&g->mu);
+    return NULL;
+}
+
+/* the buffer holding request i: -1 if the stager has not reached it; *ready set */
+static int stager_find(stager_t *g, int i, int *ready)
+{
+    for (int q = 0; q < NSTAGE; ++q)
+        if (g->req_of[q] == i) { *ready = g->ready[q]; return q; }
+    *ready = 0;
+    return -1;
+}
+
+static void stager_release(stager_t *g, int k)
+{
+    pthread_mutex_lock(&g->mu);
+    g->req_of[k] = -1;
+    g->ready[k] = 0;
+    pthread_cond_broadcast(&g->cv);
+    pthread_mutex_unlock(&g->mu);
+}
+
 int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, hype_fill_fn fill, hype_sink_fn sink,
                    void *ctx, hype_request_result *res, hype_serve_stats *stats)
 {
@@ -170,49 +254,65 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
     hype_batch_info(b, NULL, NULL, NULL, &budget);
     int *req_of = (int *)malloc(sizeof(int) * (size_t)M);
     pick_t *picks = (pick_t *)malloc(sizeof(pick_t) * (size_t)M);
-    /* pinned host staging: initial states in, final states out */
-    double *host = NULL, *host_out = NULL;
+    /* pinned host staging: initial states in (the stager's ring), final states out */
+    stager_t g;
+    memset(&g, 0, sizeof(g));
+    double *host_out = NULL;
     const size_t hbytes = sizeof(double) * 9 * (size_t)c->max_cells;
-    if (!req_of || !picks || cudaMallocHost((void **)&host, hbytes) != cudaSuccess ||
-        cudaMallocHost((void **)&host_out, hbytes) != cudaSuccess) {
+    int alloc_ok = req_of && picks && cudaMallocHost((void **)&host_out, hbytes) == cudaSuccess;
+    for (int q = 0; q < NSTAGE && alloc_ok; ++q) alloc_ok = cudaMallocHost((void **)&g.buf[q], hbytes) == cudaSuccess;
+    if (!alloc_ok) {
         free(req_of);
         free(picks);
-        if (host) cudaFreeHost(host);
         if (host_out) cudaFreeHost(host_out);
+        for (int q = 0; q < NSTAGE; ++q)
+            if (g.buf[q]) cudaFreeHost(g.buf[q]);
         hype_batch_destroy(b);
         return HYPE_ERR_NOMEM;
     }
     for (int s = 0; s < M; ++s) req_of[s] = -1;
 
-    int next = 0, finished = 0, running = 0, staged = -1;
+    int next = 0, finished = 0, running = 0;
     int steps_per_poll = 1, tuned_at = 0;
     double ms_per_step = -1.0;
     const double t_start = now_s();
     rc = HYPE_OK;
+    g.req = req; g.n = n; g.fill = fill; g.ctx = ctx; g.realtime = c->realtime; g.t_start = t_start;
+    g.max_cells = c->max_cells;
+    for (int q = 0; q < NSTAGE; ++q) g.req_of[q] = -1;
+    pthread_mutex_init(&g.mu, NULL);
+    pthread_cond_init(&g.cv, NULL);
+    g.started = pthread_create(&g.th, NULL, stager_main, &g) == 0;
+    if (!g.started) rc = HYPE_ERR_NOMEM;
 
-    while (finished < n) {
+    while (rc == HYPE_OK && finished < n) {
         double t = now_s() - t_start;
-        /* 1. admission, in arrival order */
+        /* 1. admission, in arrival order, of requests whose initial state is built */
         int admitted = 0;
         while (next < n && (!c->realtime || req[next].arrival_s <= t)) {
             const hype_request *r = &req[next];
             hype_request_result *o = &res[next];
             const size_t need = hype_batch_instance_bytes(&r->cfg);
             const long long cells = (long long)r->cfg.nx * r->cfg.ny;
+            int kbuf = -1, built = 0;
+            pthread_mutex_lock(&g.mu);
+            kbuf = stager_find(&g, next, &built);
+            while (!built && running == 0) {   /* nothing to step meanwhile: wait for the stager */
+                pthread_cond_wait(&g.cv, &g.mu);
+                kbuf = stager_find(&g, next, &built);
+            }
+            pthread_mutex_unlock(&g.mu);
+            if (!built) break;   /* step the resident requests meanwhile */
             if (need == 0 || cells > c->max_cells) {
                 o->status = HYPE_ERR_INVALID;
             } else if (need > budget) {
                 o->status = HYPE_ERR_NOMEM;   /* can never be admitted */
             } else {
-                int st = HYPE_OK;
-                if (staged != next) {   /* build the initial state once, even if admission waits */
-                    st = make_initial(r, next, fill, ctx, host);
-                    if (st == HYPE_OK) staged = next;
-                }
+                int st = g.rc[kbuf];
                 int id = -1;
-                if (st == HYPE_OK) st = hype_batch_add(b, &r->cfg, host, r->t0, r->t_final, r->max_steps, &id);
+                if (st == HYPE_OK) st = hype_batch_add(b, &r->cfg, g.buf[kbuf], r->t0, r->t_final, r->max_steps, &id);
                 if (st == HYPE_ERR_NOMEM || st == HYPE_ERR_BUSY) {
-                    if (running > 0) break;   /* wait for retirements */
+                    if (running > 0) break;   /* wait for retirements; the built state stays staged */
                     st = HYPE_ERR_NOMEM;      /* nothing to wait for: it can never fit */
                 }
                 if (st == HYPE_OK && c->substep_cells > 0) {
@@ -221,6 +321,7 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
                     if (st != HYPE_OK) hype_batch_remove(b, id);
                 }
                 if (st == HYPE_OK) {
+                    stager_release(&g, kbuf);   /* hype_batch_add has copied it to the device */
                     req_of[id] = next;
                     o->admit_s = now_s() - t_start;
                     ++running;
@@ -231,6 +332,7 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
                 }
                 o->status = st;
             }
+            stager_release(&g, kbuf);
             /* rejected request: finished with an error */
             o->admit_s = o->done_s = now_s() - t_start;
             o->latency_s = o->done_s - (c->realtime ? r->arrival_s : 0.0);
@@ -255,13 +357,8 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
             if (ms_per_step < 0.0) steps_per_poll = 1;   /* re-measure the step time */
         }
         if (c->active_cells > 0) schedule(b, req, req_of, M, c->active_cells, picks);
-        /* 2. k steps of every released instance; the next waiting request's
-         *    initial state is built on the host meanwhile */
+        /* 2. k steps of every released instance */
         if ((rc = hype_batch_advance(b, steps_per_poll))) break;
-        if (next < n && staged != next && (!c->realtime || req[next].arrival_s <= now_s() - t_start) &&
-            hype_batch_instance_bytes(&req[next].cfg) != 0 && (long long)req[next].cfg.nx * req[next].cfg.ny <= c->max_cells &&
-            make_initial(&req[next], next, fill, ctx, host) == HYPE_OK)
-            staged = next;
         if ((rc = hype_batch_sync(b))) break;
         stats->polls++;
         stats->steps_replayed += steps_per_poll;
@@ -299,6 +396,15 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
         }
     }
     const double t_end = now_s() - t_start;
+    if (g.started) {
+        pthread_mutex_lock(&g.mu);
+        g.stop = 1;
+        pthread_cond_broadcast(&g.cv);
+        pthread_mutex_unlock(&g.mu);
+        pthread_join(g.th, NULL);
+    }
+    pthread_cond_destroy(&g.cv);
+    pthread_mutex_destroy(&g.mu);
 
     /* statistics over the finished requests */
     double *lat = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
@@ -331,7 +437,7 @@ int hype_serve_run(const hype_serve_config *c, const hype_request *req, int n, h
     free(que);
     free(req_of);
     free(picks);
-    cudaFreeHost(host);
+    for (int q = 0; q < NSTAGE; ++q) cudaFreeHost(g.buf[q]);
     cudaFreeHost(host_out);
     hype_batch_destroy(b);
     return rc;
