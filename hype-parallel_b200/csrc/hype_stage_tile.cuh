@@ -52,13 +52,17 @@ struct StageKernel {
     static constexpr int COEF_ELEMS = (NC > 2 ? NC : 2) * NV * CELLS;         // also the x-flux exchange (2 NV)
     static constexpr int YT_ELEMS = 2 * NV * CELLS;                            // top-face values, by Gauss point
     static constexpr int CARRY_ELEMS = 4 * NV * CELLS;                         // ncp, t1, G below, E below
-    static constexpr int MIN_BLOCKS = (NV <= 6 ? 2 : 1) * (128 / CELLS);
-    static constexpr size_t smem_bytes()
-    {
-        // the ring, the per-cell arrays and one more row slot: the conserved input of the row
-        // being finished (row r-1), for the RK combination
-        return 128 /* barriers */ + (size_t)(SLOTS + 1) * SLOT_STRIDE * 8 + (size_t)(COEF_ELEMS + YT_ELEMS + CARRY_ELEMS) * 8 + 64;
-    }
+    // the ring, the per-cell arrays and one more row slot: the conserved input of the row
+    // being finished (row r-1), for the RK combination
+    static constexpr size_t SMEM = 128 /* barriers */ + (size_t)(SLOTS + 1) * SLOT_STRIDE * 8 +
+                                   (size_t)(COEF_ELEMS + YT_ELEMS + CARRY_ELEMS) * 8 + 64;
+    // blocks the 228 KB of an SM's shared memory holds (1 KB reserved per block); the
+    // launch bound asks for no more than that, so no register limit is paid for blocks
+    // that could not be resident anyway (Kapila N = 3 at 128-column tiles: 1)
+    static constexpr int SMEM_FIT = (int)(233472 / (SMEM + 1024));
+    static constexpr int REG_TARGET = (NV <= 6 ? 2 : 1) * (128 / CELLS);
+    static constexpr int MIN_BLOCKS = SMEM_FIT < 1 ? 1 : (SMEM_FIT < REG_TARGET ? SMEM_FIT : REG_TARGET);
+    static constexpr size_t smem_bytes() { return SMEM; }
 };
 
 // Value of one variable's polynomial cf[0..NDOF) at Gauss point q (0/1, run
