@@ -160,6 +160,8 @@ def lib() -> ctypes.CDLL:
         L.hype_totals.argtypes = [vp, ctypes.c_int, _DP, _DP, _DP]
         L.hype_launch_info.argtypes = [vp] + [ctypes.POINTER(ctypes.c_int)] * 3 + [ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_int)]
         L.hype_last_elapsed_ms.argtypes = [vp, _DP]
+        L.hype_test_division.argtypes = [ctypes.c_int, ctypes.c_longlong, ctypes.c_ulonglong, ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.POINTER(ctypes.c_longlong)]
         L.hype_test_skip_row_loads.argtypes = [vp, ctypes.c_int]
         L.hype_test_fast_rcp.argtypes = [ctypes.c_int, _DP, ctypes.c_int, _DP, _DP]
         L.hype_time_stage.argtypes = [vp, ctypes.c_int, _DP]

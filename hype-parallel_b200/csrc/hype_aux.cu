@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 #include <algorithm>
 #include "hype_internal.h"
+#include "hype_div.cuh"
 
 namespace hype {
 
@@ -367,6 +368,87 @@ int fp64_rate_of(bool fused, int device, int reps, double *ops_per_s)
     return rc;
 }
 }  // namespace
+
+namespace {
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+// a double of random sign, significand and a binary exponent in [-1100, 1100] (subnormal
+// and out-of-range exponents clamp to zero / infinity through ldexp)
+__device__ __forceinline__ double wide_double(unsigned long long u, unsigned long long v)
+{
+    const double m = 1.0 + (double)(u >> 12) * (1.0 / 4503599627370496.0);
+    const int ex = (int)(v % 2201ull) - 1100;
+    const double x = ldexp(m, ex);
+    return (v >> 63) ? -x : x;
+}
+// the cases of hype_test_division, by index: 0 raw bit patterns, 1 operands of every
+// exponent, 2 quotients next to a midpoint of two doubles, 3 all-ones divisors
+__global__ void division_check_kernel(long long n, unsigned long long seed, unsigned long long *counts)
+{
+    unsigned long long mism = 0, spec = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const unsigned long long k = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+        const unsigned long long u0 = mix64(k), u1 = mix64(k ^ 0x5851F42D4C957F2Dull), u2 = mix64(k + 0x14057B7EF767814Full),
+                                 u3 = mix64(k * 3 + 1);
+        double a, b;
+        switch ((int)(i & 3)) {
+        case 0: a = __longlong_as_double((long long)u0); b = __longlong_as_double((long long)u1); break;
+        case 1: a = wide_double(u0, u1); b = wide_double(u2, u3); break;
+        case 2: {   // a = RN(b * q_mid), q_mid = 1 + (2m + 1) 2^-53: a/b lies within an ulp or so of a midpoint
+            b = wide_double(u2, u3 % 1601ull + ((u3 >> 63) << 63));   // exponents [-1100, 500]
+            const double qmid = 1.0 + (double)(2 * (u0 >> 12) + 1) * (1.0 / 9007199254740992.0);
+            a = b * qmid;
+            break;
+        }
+        default: {   // divisor with an all-ones significand
+            const long long eb = (long long)(u3 % 2000ull) + 20;
+            b = __longlong_as_double((long long)(((u1 >> 63) << 63) | ((unsigned long long)eb << 52) | 0x000FFFFFFFFFFFFFull));
+            a = wide_double(u0, u2);
+            break;
+        }
+        }
+        bool sp = false;
+        const double q = hype::cr_div(a, b, sp);
+        const double ref = a / b;
+        if (sp) ++spec;
+        else if (__double_as_longlong(q) != __double_as_longlong(ref)) ++mism;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mism += __shfl_xor_sync(0xffffffffu, mism, o);
+        spec += __shfl_xor_sync(0xffffffffu, spec, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&counts[0], mism);
+        atomicAdd(&counts[1], spec);
+    }
+}
+}  // namespace
+
+extern "C" int hype_test_division(int device, long long n, unsigned long long seed, long long *mismatches, long long *specials)
+{
+    if (!mismatches || !specials || n < 0) return HYPE_ERR_INVALID;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return HYPE_ERR_NO_DEVICE;
+    if (cudaSetDevice(device) != cudaSuccess) return HYPE_ERR_CUDA;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    unsigned long long *d = nullptr, h[2] = {0, 0};
+    if (cudaMalloc(&d, sizeof(h)) != cudaSuccess) return HYPE_ERR_NOMEM;
+    int rc = HYPE_OK;
+    if (cudaMemset(d, 0, sizeof(h)) != cudaSuccess) rc = HYPE_ERR_CUDA;
+    if (rc == HYPE_OK) {
+        division_check_kernel<<<sms * 8, 256>>>(n, seed, d);
+        if (cudaGetLastError() != cudaSuccess || cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) rc = HYPE_ERR_CUDA;
+    }
+    cudaFree(d);
+    *mismatches = (long long)h[0];
+    *specials = (long long)h[1];
+    return rc;
+}
 
 extern "C" int hype_fp64_rate(int device, int reps, double *ops_per_s) { return fp64_rate_of(false, device, reps, ops_per_s); }
 extern "C" int hype_fp64_fma_rate(int device, int reps, double *flops_per_s) { return fp64_rate_of(true, device, reps, flops_per_s); }

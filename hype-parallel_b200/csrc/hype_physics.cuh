@@ -8,6 +8,7 @@
 // rounds on its own exactly as the reference's `gcc -O2` code does on x86-64.
 // IEEE division and square root are correctly rounded on both sides.
 #pragma once
+#include "hype_div.cuh"
 #include <cstdint>
 #include <utility>
 #include <type_traits>
@@ -689,6 +690,60 @@ __device__ __forceinline__ void weno3_1d(double u_m2, double u_m1, double u_0, d
     slope = w0 * ux0 + w1 * ux1 + w2 * ux2;
     curv = w0 * uxx0 + w1 * uxx1 + w2 * uxx2;
 }
+
+// reconstruction.c:157-178 and :144-221 with the branch-free correctly rounded
+// division of hype_div.cuh: the bits of weno3_1d / Recon<2>.  Every weight is
+// gamma_k / d_k with d_k = (IS_k + 1e-12)^4 and is then divided by the weights'
+// sum; with every d_k in [2^-400, 2^400] all those operands and quotients lie in
+// cr_div_core's range (w_k in [2^-400, 100 2^400], w_k / sum >= 2^-810), so one
+// check per stencil direction replaces one per division.  Outside it (or for a
+// NaN) `special` is set and the caller recomputes with Recon<2>.
+__device__ __forceinline__ bool cr_denominator_ok(double d) { return d >= 0x1p-400 && d <= 0x1p400; }
+
+__device__ __forceinline__ void weno3_1d_cr(double u_m2, double u_m1, double u_0, double u_p1, double u_p2, double &slope,
+                                            double &curv, bool &sp)
+{
+    const double central_cell_wt = 100.0;
+    double ux0 = -2.0 * u_m1 + 0.5 * u_m2 + 1.5 * u_0, uxx0 = 0.5 * (u_m2 - 2.0 * u_m1 + u_0);
+    double ux1 = 0.5 * (u_p1 - u_m1),                  uxx1 = 0.5 * (u_m1 - 2.0 * u_0 + u_p1);
+    double ux2 = -1.5 * u_0 + 2.0 * u_p1 - 0.5 * u_p2, uxx2 = 0.5 * (u_0 - 2.0 * u_p1 + u_p2);
+    double IS0 = ux0 * ux0 + R13_3 * uxx0 * uxx0; const double d0 = pow4(IS0 + SMALL_NUM);
+    double IS1 = ux1 * ux1 + R13_3 * uxx1 * uxx1; const double d1 = pow4(IS1 + SMALL_NUM);
+    double IS2 = ux2 * ux2 + R13_3 * uxx2 * uxx2; const double d2 = pow4(IS2 + SMALL_NUM);
+    sp |= !(cr_denominator_ok(d0) && cr_denominator_ok(d1) && cr_denominator_ok(d2));
+    double w0 = cr_div_core(1.0, d0);
+    double w1 = cr_div_core(central_cell_wt, d1);
+    double w2 = cr_div_core(1.0, d2);
+    double total = w0 + w1 + w2;
+    w0 = cr_div_core(w0, total);
+    w1 = cr_div_core(w1, total);
+    w2 = cr_div_core(w2, total);
+    slope = w0 * ux0 + w1 * ux1 + w2 * ux2;
+    curv = w0 * uxx0 + w1 * uxx1 + w2 * uxx2;
+}
+struct Recon2Cr {
+    __device__ __forceinline__ static void run(const Stencil &s, double *c, bool &sp)
+    {
+        double u_0 = s.c;
+        c[0] = u_0;
+        weno3_1d_cr(s.xm2, s.xm1, u_0, s.xp1, s.xp2, c[1], c[3], sp);
+        weno3_1d_cr(s.ym2, s.ym1, u_0, s.yp1, s.yp2, c[2], c[4], sp);
+        double uxy0 =  s.pp - u_0 - c[1] - c[2] - c[3] - c[4];
+        double uxy1 = -s.pm + u_0 + c[1] - c[2] + c[3] + c[4];
+        double uxy2 = -s.mp + u_0 - c[1] + c[2] + c[3] + c[4];
+        double uxy3 =  s.mm - u_0 + c[1] + c[2] - c[3] - c[4];
+        double temp = 4.0 * (c[3] * c[3] + c[4] * c[4]);
+        double IS0 = temp + uxy0 * uxy0; const double d0 = pow4(IS0 + SMALL_NUM);
+        double IS1 = temp + uxy1 * uxy1; const double d1 = pow4(IS1 + SMALL_NUM);
+        double IS2 = temp + uxy2 * uxy2; const double d2 = pow4(IS2 + SMALL_NUM);
+        double IS3 = temp + uxy3 * uxy3; const double d3 = pow4(IS3 + SMALL_NUM);
+        sp |= !(cr_denominator_ok(d0) && cr_denominator_ok(d1) && cr_denominator_ok(d2) && cr_denominator_ok(d3));
+        double w0 = cr_div_core(1.0, d0), w1 = cr_div_core(1.0, d1), w2 = cr_div_core(1.0, d2), w3 = cr_div_core(1.0, d3);
+        double total = w0 + w1 + w2 + w3;
+        w0 = cr_div_core(w0, total); w1 = cr_div_core(w1, total); w2 = cr_div_core(w2, total); w3 = cr_div_core(w3, total);
+        c[5] = w0 * uxy0 + w1 * uxy1 + w2 * uxy2 + w3 * uxy3;
+    }
+};
 
 template <int N> struct Recon;
 template <> struct Recon<0> {

@@ -369,8 +369,18 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 st.ym2 = w_m2[c * BW + ccm]; st.ym1 = w_m1[c * BW + ccm]; st.yp1 = w_p1[c * BW + ccm]; st.yp2 = w_p2[c * BW + ccm];
                 st.pp = w_p1[c * BW + ccm + 1]; st.pm = w_m1[c * BW + ccm + 1]; st.mp = w_p1[c * BW + ccm - 1]; st.mm = w_m1[c * BW + ccm - 1];
                 double cf[NDOF];
-                if constexpr (FAST) ReconFast<N>::run(st, cf);
-                else Recon<N>::run(st, cf);
+                if constexpr (FAST) {
+                    ReconFast<N>::run(st, cf);
+                } else if constexpr (SYS == SYS_BN && N == 2) {
+                    // branch-free correctly rounded divisions let the weights' chains overlap
+                    // (the Baer-Nunziato tile runs 8 warps per SM); the compiler's division
+                    // where an operand is outside their range
+                    bool special = false;
+                    Recon2Cr::run(st, cf, special);
+                    if (special) Recon<N>::run(st, cf);
+                } else {
+                    Recon<N>::run(st, cf);
+                }
 #pragma unroll
                 for (int k = 1; k < NDOF; ++k) coef_s[cidx(k - 1, c, m)] = cf[k];
             }

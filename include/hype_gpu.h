@@ -311,6 +311,19 @@ HYPE_API int hype_fp64_fma_rate(int device, int reps, double *flops_per_s);
  */
 HYPE_API int hype_test_skip_row_loads(hype_solver *s, int row);
 
+/*
+ * Test hook for the branch-free correctly rounded FP64 division the bit-exact
+ * Baer-Nunziato reconstruction uses (csrc/hype_div.cuh); no counterpart in the
+ * reference.  On device `device`, n operand pairs drawn from `seed` -- random
+ * bit patterns (zeros, subnormals, infinities and NaNs included), random
+ * operands of every exponent, near-midpoint quotients and divisors with an
+ * all-ones significand -- are divided both ways.  *mismatches counts pairs whose
+ * result differs from IEEE division bit for bit although the function reported
+ * them in range, *specials the pairs it reported out of range (where its caller
+ * uses IEEE division).
+ */
+HYPE_API int hype_test_division(int device, long long n, unsigned long long seed, long long *mismatches, long long *specials);
+
 #ifdef __cplusplus
 }
 #endif
