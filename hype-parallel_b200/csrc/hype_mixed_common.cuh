@@ -4,6 +4,7 @@
 // deviations from the cell value, and minmod.
 #pragma once
 #include <cuda_runtime.h>
+#include "hype_physics.cuh"
 
 namespace hype {
 
@@ -47,6 +48,29 @@ __device__ __forceinline__ void weno3_f(const float *d, float *c)
     q0 *= q0; q1 *= q1; q2 *= q2; q3 *= q3;
     const float w0 = q0 * q0, w1 = q1 * q1, w2 = q2 * q2, w3 = q3 * q3;
     c[4] = (w0 * x0 + w1 * x1 + w2 * x2 + w3 * x3) * fdiv(1.0f, w0 + w1 + w2 + w3);
+}
+
+// sum over k = 1..5 of cf(k-1) phi(k) for the two halves of a thread pair: half 0
+// takes the basis values of B0, half 1 those of B1 (PhiFace, PhiNode, PhiVol,
+// DPhiVolX, DPhiVolY of Quad<2>).  A term whose basis value is below 1e-9 in both
+// halves is dropped (y^2 - 1/12 at y = +-1/(2 sqrt 3) and the like: below FP32
+// resolution of the sum), and a value both halves share needs no selection.
+constexpr double cabs_c(double x) { return x < 0.0 ? -x : x; }
+template <class B0, class B1, class CF>
+__device__ __forceinline__ float pair_poly(CF cf, int h)
+{
+    float v = 0.0f;
+    static_for<5>([&](auto kk) {
+        constexpr int k = decltype(kk)::value + 1;
+        constexpr double a0 = B0::template at<k>(), a1 = B1::template at<k>();
+        if constexpr (cabs_c(a0) < 1e-9 && cabs_c(a1) < 1e-9) {
+        } else if constexpr (a0 == a1) {
+            v += cf(k - 1) * (float)a0;
+        } else {
+            v += cf(k - 1) * (h ? (float)a1 : (float)a0);
+        }
+    });
+    return v;
 }
 
 __device__ __forceinline__ float minmod_f(float a, float b)

@@ -347,15 +347,12 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         }
         __syncwarp();
         // point value of the reconstruction of cell `cell` with basis values phi[k] (k = 1..5)
-        auto prim_at = [&](int cell, auto phi_of) -> PrimM {
+        auto prim_at = [&](int cell, auto b0, auto b1) -> PrimM {
+            using B0 = decltype(b0);
+            using B1 = decltype(b1);
             float pv[NV];
 #pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                float v = 0.0f;
-#pragma unroll
-                for (int k = 0; k < 5; ++k) v += cf_at(k, c, cell) * phi_of(k + 1);
-                pv[c] = v;
-            }
+            for (int c = 0; c < NV; ++c) pv[c] = pair_poly<B0, B1>([&](int k1) { return cf_at(k1, c, cell); }, h);
             PrimM V;
             V.r1 = center(0, cell) + pv[0];
             V.r2 = center(1, cell) + pv[1];
@@ -371,10 +368,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
             static_for<4>([&](auto sq) {
                 constexpr int s0 = decltype(sq)::value, s1 = 4 + s0;
                 if (!ok) return;
-                const PrimM V = prim_at(m, [&](int k) {
-                    const float p0 = (float)QD::phi_node(s0, k), p1 = (float)QD::phi_node(s1, k);
-                    return h ? p1 : p0;
-                });
+                const PrimM V = prim_at(m, PhiNode<2, s0>{}, PhiNode<2, s1>{});
                 ok = pad_mixed(e, V);
             });
         }
@@ -412,10 +406,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
             float Dq = 0.0f;
             const bool doit = owned && in_rows;
             if (doit) {
-                PrimM VR = prim_at(m, [&](int k) {
-                    const float p0 = (float)QD::phi_face(2, 0, k), p1 = (float)QD::phi_face(2, 1, k);
-                    return h ? p1 : p0;
-                });
+                PrimM VR = prim_at(m, PhiFace<2, 2, 0>{}, PhiFace<2, 2, 1>{});
                 PrimM VL;
                 VL.r1 = ytf[(q * 4 + 0) * CELLS + m]; VL.r2 = ytf[(q * 4 + 1) * CELLS + m];
                 VL.u = ytf[(q * 4 + 2) * CELLS + m]; VL.v = ytf[(q * 4 + 3) * CELLS + m];
@@ -480,10 +471,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
 
         // ---------------- D. top-face values at Gauss point q for row r+1
         if (owned && r >= y0 - 1 && r < y0 + H) {
-            const PrimM VT = prim_at(m, [&](int k) {
-                const float p0 = (float)QD::phi_face(3, 0, k), p1 = (float)QD::phi_face(3, 1, k);
-                return h ? p1 : p0;
-            });
+            const PrimM VT = prim_at(m, PhiFace<2, 3, 0>{}, PhiFace<2, 3, 1>{});
             ytf[(q * 4 + 0) * CELLS + m] = VT.r1; ytf[(q * 4 + 1) * CELLS + m] = VT.r2;
             ytf[(q * 4 + 2) * CELLS + m] = VT.u; ytf[(q * 4 + 3) * CELLS + m] = VT.v;
             ytd[(q * 2 + 0) * CELLS + m] = VT.p; ytd[(q * 2 + 1) * CELLS + m] = VT.a;
@@ -495,20 +483,15 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
             if (owned && full_row) {
                 static_for<2>([&](auto sa) {
                     constexpr int qa = decltype(sa)::value, qb = 2 + qa;
-                    const PrimM V = prim_at(m, [&](int k) {
-                        const float p0 = (float)QD::phi_vol(qa, k), p1 = (float)QD::phi_vol(qb, k);
-                        return h ? p1 : p0;
-                    });
-                    float ux = 0.f, vy = 0.f, ax = 0.f, ay = 0.f;
-#pragma unroll
-                    for (int k = 0; k < 5; ++k) {
-                        const float gxk = h ? (float)QD::dphi_vol_x(qb, k + 1) : (float)QD::dphi_vol_x(qa, k + 1);
-                        const float gyk = h ? (float)QD::dphi_vol_y(qb, k + 1) : (float)QD::dphi_vol_y(qa, k + 1);
-                        ux += cf_at(k, 2, m) * gxk;
-                        vy += cf_at(k, 3, m) * gyk;
-                        ax += cf_at(k, 5, m) * gxk;
-                        ay += cf_at(k, 5, m) * gyk;
-                    }
+                    const PrimM V = prim_at(m, PhiVol<2, qa>{}, PhiVol<2, qb>{});
+                    using GX0 = DPhiVolX<2, qa>;
+                    using GX1 = DPhiVolX<2, qb>;
+                    using GY0 = DPhiVolY<2, qa>;
+                    using GY1 = DPhiVolY<2, qb>;
+                    float ux = pair_poly<GX0, GX1>([&](int k1) { return cf_at(k1, 2, m); }, h);
+                    float vy = pair_poly<GY0, GY1>([&](int k1) { return cf_at(k1, 3, m); }, h);
+                    float ax = pair_poly<GX0, GX1>([&](int k1) { return cf_at(k1, 5, m); }, h);
+                    float ay = pair_poly<GY0, GY1>([&](int k1) { return cf_at(k1, 5, m); }, h);
                     const float r1hf = (float)r1_h;
                     ux *= r1hf; vy *= r1hf; ax *= r1hf; ay *= r1hf;
                     const float K = kapila_K(e, V.r1, V.r2, V.p, V.a);
@@ -527,14 +510,8 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
             double Fq[NV];
             float Dq = 0.0f;
             if (xface && full_row) {
-                const PrimM VL = prim_at(m - 1, [&](int k) {
-                    const float p0 = (float)QD::phi_face(1, 0, k), p1 = (float)QD::phi_face(1, 1, k);
-                    return h ? p1 : p0;
-                });
-                const PrimM VR = prim_at(m, [&](int k) {
-                    const float p0 = (float)QD::phi_face(0, 0, k), p1 = (float)QD::phi_face(0, 1, k);
-                    return h ? p1 : p0;
-                });
+                const PrimM VL = prim_at(m - 1, PhiFace<2, 1, 0>{}, PhiFace<2, 1, 1>{});
+                const PrimM VR = prim_at(m, PhiFace<2, 0, 0>{}, PhiFace<2, 0, 1>{});
                 const float sp = riemann_mixed<0>(e, VL, VR, Fq, Dq, bad);
                 smax_loc = fmaxf(smax_loc, sp);
                 if (bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);

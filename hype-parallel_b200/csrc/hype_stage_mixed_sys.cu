@@ -452,14 +452,14 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
         }
         __syncwarp();
         // point value of the reconstruction of cell `cell` with basis values phi_of(k), k = 1..5
-        auto prim_at = [&](int cell, auto phi_of) -> Pt {
+        auto prim_at = [&](int cell, auto b0, auto b1) -> Pt {
+            using B0 = decltype(b0);
+            using B1 = decltype(b1);
             Pt V;
             static_for<NV>([&](auto cc_) {
                 constexpr int c = decltype(cc_)::value;
                 constexpr int sl = slot_of_comp<M>(c);
-                float v = 0.0f;
-#pragma unroll
-                for (int k = 0; k < 5; ++k) v += cf_at(k, c, cell) * phi_of(k + 1);
+                const float v = pair_poly<B0, B1>([&](int k1) { return cf_at(k1, c, cell); }, h);
                 if constexpr (is_d<M>(c)) V.d[sl] = d_0[sl * BW + cell + 3] + (double)v;
                 else V.f[sl] = f_0[sl * BW + cell + 3] + v;
             });
@@ -471,10 +471,7 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
             static_for<4>([&](auto sq) {
                 constexpr int s0 = decltype(sq)::value, s1 = 4 + s0;
                 if (!ok) return;
-                const Pt V = prim_at(m, [&](int k) {
-                    const float p0 = (float)QD::phi_node(s0, k), p1 = (float)QD::phi_node(s1, k);
-                    return h ? p1 : p0;
-                });
+                const Pt V = prim_at(m, PhiNode<2, s0>{}, PhiNode<2, s1>{});
                 ok = M::pad(e, V);
             });
         }
@@ -513,10 +510,7 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
             double Fq[NV], Dq[NNCP > 0 ? NNCP : 1];
             const bool doit = owned && in_rows;
             if (doit) {
-                const Pt VR = prim_at(m, [&](int k) {
-                    const float p0 = (float)QD::phi_face(2, 0, k), p1 = (float)QD::phi_face(2, 1, k);
-                    return h ? p1 : p0;
-                });
+                const Pt VR = prim_at(m, PhiFace<2, 2, 0>{}, PhiFace<2, 2, 1>{});
                 Pt VL;
 #pragma unroll
                 for (int c = 0; c < NF; ++c) VL.f[c] = ytf[(q * NF + c) * CELLS + m];
@@ -590,10 +584,7 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
 
         // ---------------- D. top-face values at Gauss point q for row r+1
         if (owned && r >= y0 - 1 && r < y0 + H) {
-            const Pt VT = prim_at(m, [&](int k) {
-                const float p0 = (float)QD::phi_face(3, 0, k), p1 = (float)QD::phi_face(3, 1, k);
-                return h ? p1 : p0;
-            });
+            const Pt VT = prim_at(m, PhiFace<2, 3, 0>{}, PhiFace<2, 3, 1>{});
 #pragma unroll
             for (int c = 0; c < NF; ++c) ytf[(q * NF + c) * CELLS + m] = VT.f[c];
 #pragma unroll
@@ -608,22 +599,13 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
             if (owned && full_row) {
                 static_for<2>([&](auto sa) {
                     constexpr int qa = decltype(sa)::value, qb = 2 + qa;
-                    const Pt V = prim_at(m, [&](int k) {
-                        const float p0 = (float)QD::phi_vol(qa, k), p1 = (float)QD::phi_vol(qb, k);
-                        return h ? p1 : p0;
-                    });
+                    const Pt V = prim_at(m, PhiVol<2, qa>{}, PhiVol<2, qb>{});
                     float gx[NG], gy[NG];
 #pragma unroll
                     for (int gg = 0; gg < NG; ++gg) {
                         const int c = M::grad_comp(gg);
-                        float ax = 0.f, ay = 0.f;
-#pragma unroll
-                        for (int k = 0; k < 5; ++k) {
-                            const float gxk = h ? (float)QD::dphi_vol_x(qb, k + 1) : (float)QD::dphi_vol_x(qa, k + 1);
-                            const float gyk = h ? (float)QD::dphi_vol_y(qb, k + 1) : (float)QD::dphi_vol_y(qa, k + 1);
-                            ax += cf_at(k, c, m) * gxk;
-                            ay += cf_at(k, c, m) * gyk;
-                        }
+                        const float ax = pair_poly<DPhiVolX<2, qa>, DPhiVolX<2, qb>>([&](int k1) { return cf_at(k1, c, m); }, h);
+                        const float ay = pair_poly<DPhiVolY<2, qa>, DPhiVolY<2, qb>>([&](int k1) { return cf_at(k1, c, m); }, h);
                         gx[gg] = ax * (float)r1_h;
                         gy[gg] = ay * (float)r1_h;
                     }
@@ -647,14 +629,8 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
         {
             double Fq[NV], Dq[NNCP > 0 ? NNCP : 1];
             if (xface && full_row) {
-                const Pt VL = prim_at(m - 1, [&](int k) {
-                    const float p0 = (float)QD::phi_face(1, 0, k), p1 = (float)QD::phi_face(1, 1, k);
-                    return h ? p1 : p0;
-                });
-                const Pt VR = prim_at(m, [&](int k) {
-                    const float p0 = (float)QD::phi_face(0, 0, k), p1 = (float)QD::phi_face(0, 1, k);
-                    return h ? p1 : p0;
-                });
+                const Pt VL = prim_at(m - 1, PhiFace<2, 1, 0>{}, PhiFace<2, 1, 1>{});
+                const Pt VR = prim_at(m, PhiFace<2, 0, 0>{}, PhiFace<2, 0, 1>{});
                 const float sp = M::template riemann<0>(e, VL, VR, Fq, Dq, bad);
                 smax_loc = fmaxf(smax_loc, sp);
                 if (bad && bad_cell == 0xffffffffu) bad_cell = (unsigned)(r * p.nx + i);
