@@ -87,7 +87,7 @@ CUresult encode_planes_map(CUtensorMap *m, const void *base, bool fp32, int nx, 
 static int make_tmap(hype_solver *s, CUtensorMap *m, double *base)
 {
     CUresult r = encode_planes_map(m, base - (long long)s->row_off * s->pitch - s->col_off, false, s->cfg.nx + 2 * s->col_off,
-                                   s->cfg.ny + 2 * s->row_off, s->nv, s->pitch, s->plane, stage_box_width(s->cells));
+                                   s->cfg.ny + 2 * s->row_off, s->nv, s->pitch, s->plane, stage_box_width(s->cells, s->nv));
     if (r != CUDA_SUCCESS) return fail(s, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return HYPE_OK;
 }

@@ -305,7 +305,7 @@ static int inst_maps(hype_batch *b, const Kind &k, const Inst &in, CUtensorMap *
             r = encode_planes_map(&mmaps[q].f, in.mf[q], true, c.nx, c.ny, L.nf, in.pitch, in.plane, bw);
             if (r == CUDA_SUCCESS) r = encode_planes_map(&mmaps[q].d, in.md[q], false, c.nx, c.ny, L.nd, in.pitch, in.plane, bw);
         } else {
-            r = encode_planes_map(&maps[q], in.buf[q], false, c.nx, c.ny, in.nv, in.pitch, in.plane, stage_box_width(k.cells));
+            r = encode_planes_map(&maps[q], in.buf[q], false, c.nx, c.ny, in.nv, in.pitch, in.plane, stage_box_width(k.cells, in.nv));
         }
         if (r != CUDA_SUCCESS) return bfail(b, HYPE_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     }

@@ -81,7 +81,17 @@ struct StageParams {
 // 128 (chosen per grid by the autotuner, 128 by default).
 constexpr int STAGE_CELLS = 128;
 constexpr int STAGE_SLOTS = 6;              // prim row ring
-inline int stage_box_width(int cells) { return cells + 6; }   // TMA box: columns x0-4 .. x0+cells+1
+// TMA box of the FP64 stage tile: columns x0-4 .. x0+cells+1 (cells + 6), widened by
+// pairs of columns until nvh * width = 8 (mod 16) doubles, nvh = (nv + 1) / 2: the two
+// threads of a pair read stencil rows nvh planes apart, which then fall on disjoint halves
+// of the shared-memory banks (e.g. Kapila: 136 instead of 134 for 128-cell tiles)
+constexpr int stage_box_width(int cells, int nv)
+{
+    const int nvh = (nv + 1) / 2;
+    for (int w = cells + 6; w < cells + 6 + 32; w += 2)
+        if ((nvh * w) % 16 == 8) return w;
+    return cells + 6;
+}
 
 size_t stage_smem_bytes(int sys, int order, int cells);
 int stage_threads(int cells);

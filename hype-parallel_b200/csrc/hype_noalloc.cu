@@ -118,7 +118,7 @@ extern "C" HYPE_API int hype_rhs_prim_noalloc(const hype_config *cfg, double t, 
     CUtensorMap tm;
     cuuint64_t dims[3] = {(cuuint64_t)cfg->nx, (cuuint64_t)cfg->ny, (cuuint64_t)nv};
     cuuint64_t strides[2] = {(cuuint64_t)pitch * 8ull, (cuuint64_t)plane * 8ull};
-    cuuint32_t box[3] = {(cuuint32_t)stage_box_width(STAGE_CELLS), 1u, (cuuint32_t)nv};
+    cuuint32_t box[3] = {(cuuint32_t)stage_box_width(STAGE_CELLS, nv), 1u, (cuuint32_t)nv};
     cuuint32_t estr[3] = {1u, 1u, 1u};
     if (reinterpret_cast<PFN_encodeTiled>(fn)(&tm, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, planes, dims, strides, box, estr,
                                               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,

@@ -41,7 +41,7 @@ struct StageKernel {
     static constexpr int NV = S::NV;
     static constexpr int CELLS = CELLS_;         // reconstruction columns per tile
     static constexpr int NT = 2 * CELLS;         // two threads per cell
-    static constexpr int BW = CELLS + 6;         // TMA box width
+    static constexpr int BW = stage_box_width(CELLS, NV);   // TMA box width
     static constexpr int SLOTS = STAGE_SLOTS;
     static constexpr int NDOF = QD::NDOF;
     static constexpr int NC = NDOF - 1;                    // stored coefficients (k >= 1)
