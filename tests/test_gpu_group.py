@@ -286,3 +286,58 @@ def test_rhs_prim_slab_mixed_precision(hp):
         dts.append(dt.value)
     assert R.tobytes() == Rf.tobytes()
     assert min(dts) == dtf
+
+
+BLOCK_CASES = [("kapila_37x23_rough_mixed_bc", 2, 2), ("kapila_24x24_periodic", 3, 2), ("kapila_18x14_inlet", 3, 1),
+               ("kapila_15x13_N3", 2, 2), ("bn_13x21_periodic_N1", 2, 3), ("euler_21x19_reflective_N1", 3, 3),
+               ("kapila_cons_37x23_rough", 4, 2), ("kapila_visc_37x23_rough", 2, 2)]
+
+
+@pytest.mark.parametrize("name,px,py", BLOCK_CASES)
+def test_rhs_prim_block_reads_only_its_halo(name, px, py, hp, orc):
+    """hype_create_block + hype_rhs_prim_slab on DMDA-style local arrays of a grid
+    split px x py: the rank's block, 3 ghost rows and columns (corners included)
+    from the neighbours where a neighbour exists (periodic axes wrap), NaN in every
+    ghost cell on a physical boundary -- the kernel must fill those itself.  The
+    blocks' RHS make the reference's RHS bit for bit and the least of their dt is its
+    dt (inviscid)."""
+    import ctypes
+    _, cfg, kind, seed = cases.case_by_name(name)
+    U = cases.state(cfg, kind, seed)
+    Ro, dto, _ = orc.rhs(cfg, U)
+    nv, nx, ny = cfg.nvar, cfg.nx, cfg.ny
+    Ug = U.reshape(ny, nx, nv)
+    L = hp.lib()
+    DP = ctypes.POINTER(ctypes.c_double)
+    L.hype_create_block.argtypes = [ctypes.POINTER(hp._Cfg), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p)]
+    L.hype_rhs_prim_slab.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong, DP, DP]
+    perx, pery = cfg.bc_left == O.PERIODIC, cfg.bc_bottom == O.PERIODIC
+
+    def split(n, p):   # PETSc's: the first n % p ranks one more
+        sizes = [n // p + (1 if r < n % p else 0) for r in range(p)]
+        return [(sum(sizes[:r]), sizes[r]) for r in range(p)]
+    R = np.full((ny, nx, nv), np.nan)
+    dts = []
+    for ys, ym in split(ny, py):
+        for xs, xm in split(nx, px):
+            loc = np.full((ym + 6, xm + 6, nv), np.nan)
+            for j in range(-3, ym + 3):
+                for i in range(-3, xm + 3):
+                    gj, gi = ys + j, xs + i
+                    if (0 <= gj < ny or pery) and (0 <= gi < nx or perx):
+                        loc[j + 3, i + 3] = Ug[gj % ny, gi % nx]
+            h = ctypes.c_void_p()
+            st = L.hype_create_block(ctypes.byref(cases.to_pkg(cfg).c_struct()), xs, xm, ys, ym, ctypes.byref(h))
+            assert st == hp.OK, L.hype_last_error(h)
+            Rr = np.empty(ym * xm * nv)
+            dt = ctypes.c_double()
+            base = loc.ctypes.data + ((3 * (xm + 6) + 3) * nv) * 8
+            st = L.hype_rhs_prim_slab(h, 0.0, base, (xm + 6) * nv, Rr.ctypes.data_as(DP), ctypes.byref(dt))
+            L.hype_destroy(h)
+            assert st == hp.OK
+            R[ys:ys + ym, xs:xs + xm] = Rr.reshape(ym, xm, nv)
+            dts.append(dt.value)
+    assert R.reshape(-1).tobytes() == Ro.tobytes()
+    if not cfg.viscous:
+        assert min(dts) == dto
