@@ -49,8 +49,8 @@ RHS_FLOPS_2048 = 20067647618
 # and the AXPBYPCZ stage (3 mul + 2 add per field), 6 fields
 RK_FLOPS_PER_CELL = 3 * 2 * 6 + 5 * 6
 # DRAM bytes of one stage-kernel launch on this workload, from an ncu capture of the
-# kernel (dram__bytes_read.sum + dram__bytes_write.sum: 211,361,536 + 160,634,624)
-STAGE_TRAFFIC_BYTES = 211361536 + 160634624
+# kernel (dram__bytes_read.sum + dram__bytes_write.sum: 210,945,536 + 159,174,656)
+STAGE_TRAFFIC_BYTES = 210945536 + 159174656
 NBUB = 4
 SEED = 0
 BYTES_PER_CELL_UPDATE = 9 * 6 * 8    # SSPRK(4,3): 5 state reads + 4 state writes of 6 FP64 fields
