@@ -589,8 +589,8 @@ def run_gpu(args, rank, world, local_rank):
     e2e = {"value": (world * cells * e2e_steps / e2e_s) if e2e_steps else None, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
            "d2h_bytes_per_step": state_bytes,
            "how": "per step: hype_advance_host(U_in, U_out, 1): the state from pinned host memory, one SSPRK(4,3) "
-                  "step, the state back to pinned host memory (row bands of the copies overlap the first and last "
-                  "stages); wall clock"}
+                  "step, the state back to pinned host memory (every stage a wavefront of row bands behind the "
+                  "band-by-band upload, bands copied out as they finish); wall clock"}
     info = solver.launch_info()
     solver.close()
 

@@ -388,34 +388,47 @@ static int check_config(const hype_config *c, hype_solver *s)
 }
 
 // ---------------------------------------------------------------------------
-// Banded host calls.  The stages next to a host copy run on a finer row
-// decomposition (up to 8x the runs, at least 8 rows each) grouped into up to
-// 8 bands of rows, launched band by band so that each band fills the GPU and
-// finishes early: the host->device copy of later bands overlaps the launches on
-// earlier ones (band k's stencils read rows of bands k-1..k+1), and the
-// device->host copy of a band overlaps the launches on the bands after it
-// (hype_rhs_prim: its one RHS launch; hype_advance_host: every stage of the
-// step, enqueue_step_banded).  Copies go on their own streams (cin, cout),
-// ordered to the compute streams by events.  Results do not depend on the
-// decomposition.
+// Banded host calls.  The grid's rows are split into row bands, each a set of
+// row runs launched on its own, so that device work starts before the whole
+// state has arrived and the result leaves band by band:
+//  - host->device: every band's rows are copied back to back on `cin`; the
+//    conversion to planes runs on `cvin` behind each copy, so the copy engine
+//    never waits for SM slots (ev_cp: copied, ev_in: converted);
+//  - device->host: a band's result is converted on `cvout` once computed and
+//    copied out on `cout` (ev_dc: converted);
+//  - hype_rhs_prim: its one RHS launch, 8 bands of one full wave each, band
+//    by band behind the uploads (banded_upload_stage);
+//  - hype_advance_host: every stage of the step as a wavefront over 16 bands
+//    (enqueue_step_banded).  Stage s runs on compute stream s % 4, so the four
+//    SSPRK(4,3) stages advance together, each band of stage s waiting only for
+//    the bands of stage s-1 its stencils read (band k-1..k+1); each launch
+//    covers half a wave of blocks, so launches of neighbouring stages share the
+//    SMs.  On a 2048^2 Kapila grid, one step with its copies took 12.0-12.6 ms
+//    with 8 full-wave bands and alternating stages on two streams, and
+//    10.2-10.5 ms this way (the device-only step: 8.6 ms).
+// Results do not depend on the decomposition.
 // ---------------------------------------------------------------------------
 struct Bands {
     int n;
-    int runs;     // runs of the banded launches
-    int run[9];   // band k: runs run[k] .. run[k+1]-1
-    int row[9];   //         rows row[k] .. row[k+1]-1 (those runs' own rows)
-    int order[8]; // launch order: band 0 last on a periodic y axis (it reads the last band)
+    int runs;                              // runs of the banded launches
+    int run[hype_solver::MAX_BANDS + 1];   // band k: runs run[k] .. run[k+1]-1
+    int row[hype_solver::MAX_BANDS + 1];   //         rows row[k] .. row[k+1]-1 (those runs' own rows)
+    int order[hype_solver::MAX_BANDS];     // launch order: band 0 last on a periodic y axis (it reads the last band)
 };
 
-static Bands make_bands(const hype_solver *s)
+// up to `max_bands` bands of `per` runs each, at least 8 rows per run
+static Bands make_bands(const hype_solver *s, int max_bands, int per)
 {
     Bands b;
     const int ny = s->cfg.ny;
-    int runs = 8 * s->runs;
-    if (runs > ny / 8) runs = ny / 8 > s->runs ? ny / 8 : s->runs;
+    if (max_bands > hype_solver::MAX_BANDS) max_bands = hype_solver::MAX_BANDS;
+    if (per < 1) per = 1;
+    int runs = max_bands * per;
+    const int cap = ny / 8 > s->runs ? ny / 8 : s->runs;
+    if (runs > cap) runs = cap;
     if (runs < 1) runs = 1;
     b.runs = runs;
-    b.n = runs < 8 ? runs : 8;
+    b.n = runs < max_bands ? runs : max_bands;
     for (int k = 0; k <= b.n; ++k) {
         b.run[k] = (int)(((long long)k * runs) / b.n);
         b.row[k] = (int)(((long long)b.run[k] * ny) / runs);
@@ -424,6 +437,17 @@ static Bands make_bands(const hype_solver *s)
     for (int k = 0; k < b.n; ++k) b.order[k] = py ? (k + 1) % b.n : k;
     return b;
 }
+
+// row runs of one wave of stage blocks
+static int wave_runs(const hype_solver *s)
+{
+    const int r = s->sms * s->bps / (s->strips > 0 ? s->strips : 1);
+    return r > 0 ? r : 1;
+}
+
+// the bands of hype_rhs_prim (one full wave per band) and of hype_advance_host (half a wave)
+static Bands rhs_bands(const hype_solver *s) { return make_bands(s, 8, s->runs); }
+static Bands step_bands(const hype_solver *s) { return make_bands(s, hype_solver::MAX_BANDS, wave_runs(s) / 2); }
 
 // the last band whose rows band k's stencils read (the halo is 3 rows, bands are >= 8)
 static int band_needs(const hype_solver *s, const Bands &b, int k)
@@ -438,6 +462,8 @@ static int fence_copy_streams(hype_solver *s)
     CUDA_TRY(s, cudaEventRecord(s->ev_fence, s->stream));
     CUDA_TRY(s, cudaStreamWaitEvent(s->cin, s->ev_fence, 0));
     CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_fence, 0));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->cvin, s->ev_fence, 0));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->cvout, s->ev_fence, 0));
     return HYPE_OK;
 }
 
@@ -448,8 +474,10 @@ static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, d
     const int r0 = b.row[k], nr = b.row[k + 1] - r0;
     CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn + r0 * row_elems, U + r0 * row_elems, sizeof(double) * row_elems * nr,
                                 cudaMemcpyHostToDevice, s->cin));
-    CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, dst, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cin));
-    CUDA_TRY(s, cudaEventRecord(s->ev_in[k], s->cin));
+    CUDA_TRY(s, cudaEventRecord(s->ev_cp[k], s->cin));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->cvin, s->ev_cp[k], 0));
+    CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, dst, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cvin));
+    CUDA_TRY(s, cudaEventRecord(s->ev_in[k], s->cvin));
     return HYPE_OK;
 }
 
@@ -556,15 +584,16 @@ int hype_destroy(hype_solver *s)
     if (s->hSc) cudaFreeHost(s->hSc);
     if (s->ev0) cudaEventDestroy(s->ev0);
     if (s->ev1) cudaEventDestroy(s->ev1);
-    for (int k = 0; k < 8; ++k) {
+    for (int k = 0; k < hype_solver::MAX_BANDS; ++k) {
+        if (s->ev_cp[k]) cudaEventDestroy(s->ev_cp[k]);
         if (s->ev_in[k]) cudaEventDestroy(s->ev_in[k]);
+        if (s->ev_dc[k]) cudaEventDestroy(s->ev_dc[k]);
         if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
     }
     if (s->ev_fence) cudaEventDestroy(s->ev_fence);
     for (cudaEvent_t e : s->ev_sb) if (e) cudaEventDestroy(e);
-    if (s->stream2) { cudaStreamSynchronize(s->stream2); cudaStreamDestroy(s->stream2); }
-    if (s->cin) { cudaStreamSynchronize(s->cin); cudaStreamDestroy(s->cin); }
-    if (s->cout) { cudaStreamSynchronize(s->cout); cudaStreamDestroy(s->cout); }
+    for (cudaStream_t *q : {&s->stream2, &s->stream3, &s->stream4, &s->cin, &s->cout, &s->cvin, &s->cvout})
+        if (*q) { cudaStreamSynchronize(*q); cudaStreamDestroy(*q); }
     if (s->stream) cudaStreamDestroy(s->stream);
     delete s;
     return HYPE_OK;
@@ -604,14 +633,12 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(s, cudaEventCreate(&s->ev0));
     CUDA_TRY(s, cudaEventCreate(&s->ev1));
-    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->cin, cudaStreamNonBlocking));
-    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->cout, cudaStreamNonBlocking));
-    for (int k = 0; k < 8; ++k) {
-        CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_in[k], cudaEventDisableTiming));
-        CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_done[k], cudaEventDisableTiming));
-    }
+    for (cudaStream_t *q : {&s->cin, &s->cout, &s->cvin, &s->cvout, &s->stream2, &s->stream3, &s->stream4})
+        CUDA_TRY(s, cudaStreamCreateWithFlags(q, cudaStreamNonBlocking));
+    for (int k = 0; k < hype_solver::MAX_BANDS; ++k)
+        for (cudaEvent_t *e : {&s->ev_cp[k], &s->ev_in[k], &s->ev_dc[k], &s->ev_done[k]})
+            CUDA_TRY(s, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_fence, cudaEventDisableTiming));
-    CUDA_TRY(s, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
     for (cudaEvent_t &e : s->ev_sb) CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     double **bufs[] = {&s->dU, &s->dS0, &s->dS1, &s->dS2};
     const long long off = (long long)row_off * s->pitch + col_off;   // the buffers point at cell (0, 0)
@@ -805,7 +832,7 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
         return rc;
     }
     // banded: U's rows stream in while earlier bands compute, RHS rows stream out
-    const Bands b = make_bands(s);
+    const Bands b = rhs_bands(s);
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
     const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
@@ -979,16 +1006,14 @@ int hype_advance(hype_solver *s, int nsteps)
 // One step enqueued by hand (the graph's content) as a wavefront of row bands:
 // band k of stage s reads the rows of bands k-1..k+1 of stage s-1 (3-row stencils,
 // bands of >= 8 rows; bands 0 and n-1 are neighbours on a periodic y axis) and
-// is launched once those are enqueued, stage 0 once the uploads of those bands are
-// (U_in).  Stage s writes a buffer that only stage s-1 (or, for the combination's
-// second operand, the same band of an earlier stage) still reads, so the same
-// dependency covers every overwrite.  After each band's upload every launch that
-// became ready is enqueued, lowest stage first, so all stages run behind the
-// host->device copy, and the last stage's bands go to the copy-out stream as they
-// finish (U_out).  Even stages run on the compute stream, odd ones on a second
-// stream, each launch waiting for the events of the bands it reads, so that a
-// band's launch fills the SMs that the tail of another leaves idle.  Results equal
-// the unbanded step's.
+// waits for their events, stage 0 for the uploads of those bands (U_in).  Stage s
+// writes a buffer that only stage s-1 (or, for the combination's second operand,
+// the same band of an earlier stage) still reads, so the same dependency covers
+// every overwrite.  Stage s is enqueued band by band on compute stream s % 4, in
+// b.order (band 0 last on a periodic y axis, where it reads the last band), so no
+// band waits behind another that is not ready; the last stage's bands are
+// converted and copied out as they finish (U_out).  Results equal the unbanded
+// step's.
 static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_in, double *U_out)
 {
     PlanStage plan[MAX_PLAN];
@@ -996,68 +1021,43 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
     const int ns = ssp_plan(s->cfg.order, plan, &copy_back);
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     const bool py = s->cfg.bc_bottom == HYPE_BC_PERIODIC && b.n > 1;
-    bool done[MAX_PLAN][8] = {};
-    auto nbrs = [&](int k, int *out) -> int {   // bands whose rows band k's stencils read
-        int m = 0;
-        out[m++] = k;
-        if (k > 0) out[m++] = k - 1; else if (py) out[m++] = b.n - 1;
-        if (k + 1 < b.n) out[m++] = k + 1; else if (py) out[m++] = 0;
-        return m;
-    };
-    int uploaded = U_in ? 0 : b.n;
-    auto ready = [&](int st, int k) -> bool {
-        int nb[3];
-        const int m = nbrs(k, nb);
-        for (int j = 0; j < m; ++j)
-            if (st == 0 ? nb[j] >= uploaded : !done[st - 1][nb[j]]) return false;
-        return true;
-    };
-    auto launch = [&](int st, int k) -> int {
-        const PlanStage &q = plan[st];
-        cudaStream_t on = (st & 1) ? s->stream2 : s->stream;
-        int nb[3];
-        const int m = nbrs(k, nb);
-        for (int j = 0; j < m; ++j) {
-            if (st == 0 && U_in) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_in[nb[j]], 0));
-            if (st > 0) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_sb[(st - 1) * 8 + nb[j]], 0));
-        }
-        CUDA_TRY(s, stage_band(s, b, k, q, 0, nullptr, on));
-        CUDA_TRY(s, cudaEventRecord(s->ev_sb[st * 8 + k], on));
-        if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
-            const int r0 = b.row[k], nr = b.row[k + 1] - r0;
-            CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_sb[st * 8 + k], 0));
-            CUDA_TRY(s, launch_planes_to_aos_rows(buf_of(s, q.out), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cout));
-            CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
-                                        cudaMemcpyDeviceToHost, s->cout));
-        }
-        done[st][k] = true;
-        return HYPE_OK;
-    };
+    cudaStream_t on_stage[4] = {s->stream, s->stream2, s->stream3, s->stream4};
     CUDA_TRY(s, launch_begin_step(s->dSc, s->stream));
-    CUDA_TRY(s, cudaEventRecord(s->ev_fence, s->stream));   // the second stream starts behind begin_step
-    CUDA_TRY(s, cudaStreamWaitEvent(s->stream2, s->ev_fence, 0));
-    for (int u = 0;; ++u) {
-        if (U_in && u < b.n) {
-            if ((rc = upload_band(s, b, u, U_in, buf_of(s, plan[0].in)))) return rc;
-            uploaded = u + 1;
-        }
-        for (bool progress = true; progress;) {
-            progress = false;
-            for (int st = 0; st < ns; ++st)
-                for (int k = 0; k < b.n; ++k)
-                    if (!done[st][k] && ready(st, k)) {
-                        if ((rc = launch(st, k))) return rc;
-                        progress = true;
-                    }
-        }
-        if (uploaded >= b.n) break;
-    }
-    for (int st = 0; st < ns; ++st)
+    CUDA_TRY(s, cudaEventRecord(s->ev_fence, s->stream));   // the other compute streams start behind begin_step
+    for (int j = 1; j < 4; ++j) CUDA_TRY(s, cudaStreamWaitEvent(on_stage[j], s->ev_fence, 0));
+    if (U_in)
         for (int k = 0; k < b.n; ++k)
-            if (!done[st][k]) return fail(s, HYPE_ERR_CUDA, "banded step: stage %d band %d never became ready", st, k);
-    for (int k = 0; k < b.n; ++k)   // end_step and everything after it behind both streams
-        for (int st = ns - 2; st < ns; ++st)
-            if (st >= 0) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_sb[st * 8 + k], 0));
+            if ((rc = upload_band(s, b, k, U_in, buf_of(s, plan[0].in)))) return rc;
+    for (int st = 0; st < ns; ++st) {
+        const PlanStage &q = plan[st];
+        cudaStream_t on = on_stage[st % 4];
+        for (int i = 0; i < b.n; ++i) {
+            const int k = b.order[i];
+            int nb[3], m = 0;   // bands whose rows band k's stencils read
+            nb[m++] = k;
+            if (k > 0) nb[m++] = k - 1; else if (py) nb[m++] = b.n - 1;
+            if (k + 1 < b.n) nb[m++] = k + 1; else if (py) nb[m++] = 0;
+            for (int j = 0; j < m; ++j) {
+                if (st == 0 && U_in) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_in[nb[j]], 0));
+                if (st > 0) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_sb[(st - 1) * hype_solver::MAX_BANDS + nb[j]], 0));
+            }
+            CUDA_TRY(s, stage_band(s, b, k, q, 0, nullptr, on));
+            cudaEvent_t done = s->ev_sb[st * hype_solver::MAX_BANDS + k];
+            CUDA_TRY(s, cudaEventRecord(done, on));
+            if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
+                const int r0 = b.row[k], nr = b.row[k + 1] - r0;
+                CUDA_TRY(s, cudaStreamWaitEvent(s->cvout, done, 0));
+                CUDA_TRY(s, launch_planes_to_aos_rows(buf_of(s, q.out), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cvout));
+                CUDA_TRY(s, cudaEventRecord(s->ev_dc[k], s->cvout));
+                CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_dc[k], 0));
+                CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
+                                            cudaMemcpyDeviceToHost, s->cout));
+            }
+        }
+    }
+    for (int k = 0; k < b.n; ++k)   // end_step and everything after it behind every compute stream
+        for (int st = ns - 4 > 0 ? ns - 4 : 0; st < ns; ++st)
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_sb[st * hype_solver::MAX_BANDS + k], 0));
     CUDA_TRY(s, launch_end_step(s->dSc, s->cfl_h, s->stream));
     return HYPE_OK;
 }
@@ -1078,7 +1078,7 @@ int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nst
         return rc ? rc : rc2;
     }
     if ((rc = ensure_step_graph(s))) return rc;
-    const Bands b = make_bands(s);
+    const Bands b = step_bands(s);
     if ((rc = fence_copy_streams(s))) return rc;
     CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
     if ((rc = enqueue_step_banded(s, b, U_in, nsteps == 1 ? U_out : nullptr))) return rc;

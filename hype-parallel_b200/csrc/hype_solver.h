@@ -20,13 +20,19 @@ struct hype_solver {
     hype::DevScalars *hSc = nullptr;        // pinned mirror
     CUtensorMap tmU, tmS0, tmS1;
     cudaStream_t stream = nullptr;
-    cudaStream_t cin = nullptr, cout = nullptr;   // host<->device copy streams of the banded calls
-    cudaEvent_t ev_in[8] = {}, ev_done[8] = {};   // per row band: uploaded, computed
-    cudaEvent_t ev_fence = nullptr;               // the compute stream's work so far
-    // banded steps: odd stages on a second compute stream, band k of stage s marked by
-    // ev_sb[s * 8 + k], so that one band's launch fills the tail of another's
-    cudaStream_t stream2 = nullptr;
-    cudaEvent_t ev_sb[hype::MAX_PLAN * 8] = {};
+    // banded host calls (row bands of the grid, at most MAX_BANDS)
+    static constexpr int MAX_BANDS = 16;
+    cudaStream_t cin = nullptr, cout = nullptr;     // host<->device copies, back to back
+    cudaStream_t cvin = nullptr, cvout = nullptr;   // the layout conversions beside those copies
+    cudaEvent_t ev_cp[MAX_BANDS] = {};              // per row band: host rows copied in
+    cudaEvent_t ev_in[MAX_BANDS] = {};              //               converted to planes
+    cudaEvent_t ev_dc[MAX_BANDS] = {};              //               result converted for the copy out
+    cudaEvent_t ev_done[MAX_BANDS] = {};            //               computed
+    cudaEvent_t ev_fence = nullptr;                 // the compute stream's work so far
+    // banded steps: stage s on compute stream s % 4 (stream, stream2, stream3, stream4),
+    // band k of stage s marked by ev_sb[s * MAX_BANDS + k]
+    cudaStream_t stream2 = nullptr, stream3 = nullptr, stream4 = nullptr;
+    cudaEvent_t ev_sb[hype::MAX_PLAN * MAX_BANDS] = {};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaGraphExec_t step_exec = nullptr;
     int cells = hype::STAGE_CELLS;          // tile width of the stage kernel

@@ -259,8 +259,9 @@ def test_autotuned_tiles_give_identical_bits(hp, orc):
                                          ("kapila_16x16_solve_N3", 2), ("kapila_24x20_bubble_solve_N1", 2),
                                          ("bn_20x20_solve", 1), ("euler_32x24_solve", 4), ("kapila_cons_32x32_solve", 2)])
 def test_advance_host_equals_set_advance_get(name, nsteps, hp):
-    """hype_advance_host (copies overlapped with the stages of the first and last steps) gives
-    the bits of set_state + advance + wait + get_state."""
+    """hype_advance_host (copies overlapped with the stages of the first and last steps; on
+    these small grids a few bands of one 8-row run each) gives the bits of set_state +
+    advance + wait + get_state."""
     (_, cfg, kind, seed), t0, tf, nmax = cases.case_by_name(name)
     U = cases.state(cfg, kind, seed)
     pc = cases.to_pkg(cfg)
@@ -279,7 +280,8 @@ def test_advance_host_equals_set_advance_get(name, nsteps, hp):
 
 
 def test_advance_host_large_grid_banded(hp):
-    """A grid large enough for 8 row bands, periodic in y (band 0 reads the last band)."""
+    """A grid large enough for 16 row bands in the step and 8 in the RHS call, periodic in y
+    (band 0 reads the last band)."""
     P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
     c = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=700, ny=900, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=P, bc_top=P)
     U = hp.initial_state(c, "shock_bubble", seed=12, nbubbles=3)
@@ -303,9 +305,10 @@ def test_advance_host_large_grid_banded(hp):
 @pytest.mark.parametrize("order,periodic,nsteps,flags", [(2, False, 1, 0), (3, False, 1, 0), (1, True, 3, 0), (2, True, 1, 0),
                                                         (2, False, 2, 4), (2, False, 1, 2)])
 def test_advance_host_wavefront(order, periodic, nsteps, flags, hp):
-    """8 row bands, every stage launched band by band behind the upload and the
-    result downloaded band by band (one-step calls do both): the bits of the
-    unbanded step, for N = 1..3, periodic y, the viscous and the conservative paths."""
+    """16 row bands, every stage launched band by band on its own stream behind the
+    upload and the result downloaded band by band (one-step calls do both): the bits
+    of the unbanded step, for N = 1..3 (N = 3: ten stages on four streams), periodic y,
+    the viscous and the conservative paths."""
     P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
     yb = P if periodic else hp.BC_REFLECTIVE
     c = hp.Config(system=hp.KAPILA_5EQN, order=order, nx=640, ny=720, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=yb, bc_top=yb,
