@@ -591,6 +591,23 @@ def run_gpu(args, rank, world, local_rank):
            "how": "per step: hype_advance_host(U_in, U_out, 1): the state from pinned host memory, one SSPRK(4,3) "
                   "step, the state back to pinned host memory (every stage a wavefront of row bands behind the "
                   "band-by-band upload, bands copied out as they finish); wall clock"}
+    # the drop-in's per-stage call: RHSFunctionPrim through the C ABI with host
+    # buffers (petsc_glue.c makes this call once per TS stage)
+    rhs_host = None
+    if e2e_steps:
+        pin_rhs = torch.empty_like(pin_in).pin_memory()
+        solver.rhs_function_prim(0.0, pin_in.numpy(), pin_rhs.numpy())
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            solver.rhs_function_prim(0.0, pin_in.numpy(), pin_rhs.numpy())
+        barrier()
+        rhs_s = max_over_ranks(max(time.perf_counter() - t0, 1e-9), world)
+        rhs_host = {"ms_per_call": rhs_s / e2e_steps * 1e3, "value": world * cells * e2e_steps / rhs_s, "unit": "cell-RHS/s",
+                    "calls": e2e_steps, "h2d_bytes_per_call": state_bytes, "d2h_bytes_per_call": state_bytes,
+                    "how": "hype_rhs_prim(t, U, RHS, &dt) from and to pinned host memory, the call RHSFunctionPrim "
+                           "(petsc_glue.c) makes once per TS stage: row bands of U stream in, each band's RHS launch "
+                           "runs once its rows are there, RHS rows stream out; wall clock"}
     info = solver.launch_info()
     solver.close()
 
@@ -679,7 +696,7 @@ def run_gpu(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "checks": {"alpha_min": amin, "alpha_max": amax, "steps_done": steps2, "t": t2},
             "forms": {"fp64_fast": fast, "mixed": mixed, "bn1024": bn, "batched": batched, "serving": serving,
-                      "y_slabs": group}}
+                      "y_slabs": group, "rhs_host": rhs_host}}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -396,16 +396,18 @@ static int check_config(const hype_config *c, hype_solver *s)
 //    never waits for SM slots (ev_cp: copied, ev_in: converted);
 //  - device->host: a band's result is converted on `cvout` once computed and
 //    copied out on `cout` (ev_dc: converted);
-//  - hype_rhs_prim: its one RHS launch, 8 bands of one full wave each, band
-//    by band behind the uploads (banded_upload_stage);
-//  - hype_advance_host: every stage of the step as a wavefront over 16 bands
+//  - up to 16 bands, each launch covering half a wave of blocks (host_bands);
+//  - hype_rhs_prim: its one RHS launch, band by band behind the uploads
+//    (banded_upload_stage).  On a 2048^2 Kapila grid a call took 5.4-5.5 ms
+//    with 8 full-wave bands and 4.8 ms this way (the copies alone: 3.6 ms each
+//    way, 4.1 ms both ways at once);
+//  - hype_advance_host: every stage of the step as a wavefront over the bands
 //    (enqueue_step_banded).  Stage s runs on compute stream s % 4, so the four
 //    SSPRK(4,3) stages advance together, each band of stage s waiting only for
-//    the bands of stage s-1 its stencils read (band k-1..k+1); each launch
-//    covers half a wave of blocks, so launches of neighbouring stages share the
-//    SMs.  On a 2048^2 Kapila grid, one step with its copies took 12.0-12.6 ms
-//    with 8 full-wave bands and alternating stages on two streams, and
-//    10.2-10.5 ms this way (the device-only step: 8.6 ms).
+//    the bands of stage s-1 its stencils read (band k-1..k+1), and launches of
+//    neighbouring stages share the SMs.  On the same grid one step with its
+//    copies took 12.0-12.6 ms with 8 full-wave bands and alternating stages on
+//    two streams, and 10.2-10.5 ms this way (the device-only step: 8.6 ms).
 // Results do not depend on the decomposition.
 // ---------------------------------------------------------------------------
 struct Bands {
@@ -445,9 +447,8 @@ static int wave_runs(const hype_solver *s)
     return r > 0 ? r : 1;
 }
 
-// the bands of hype_rhs_prim (one full wave per band) and of hype_advance_host (half a wave)
-static Bands rhs_bands(const hype_solver *s) { return make_bands(s, 8, s->runs); }
-static Bands step_bands(const hype_solver *s) { return make_bands(s, hype_solver::MAX_BANDS, wave_runs(s) / 2); }
+// the bands of the host calls: launches of half a wave of blocks
+static Bands host_bands(const hype_solver *s) { return make_bands(s, hype_solver::MAX_BANDS, wave_runs(s) / 2); }
 
 // the last band whose rows band k's stencils read (the halo is 3 rows, bands are >= 8)
 static int band_needs(const hype_solver *s, const Bands &b, int k)
@@ -832,7 +833,7 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
         return rc;
     }
     // banded: U's rows stream in while earlier bands compute, RHS rows stream out
-    const Bands b = rhs_bands(s);
+    const Bands b = host_bands(s);
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
     const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
@@ -1078,7 +1079,7 @@ int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nst
         return rc ? rc : rc2;
     }
     if ((rc = ensure_step_graph(s))) return rc;
-    const Bands b = step_bands(s);
+    const Bands b = host_bands(s);
     if ((rc = fence_copy_streams(s))) return rc;
     CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
     if ((rc = enqueue_step_banded(s, b, U_in, nsteps == 1 ? U_out : nullptr))) return rc;

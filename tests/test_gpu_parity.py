@@ -280,7 +280,7 @@ def test_advance_host_equals_set_advance_get(name, nsteps, hp):
 
 
 def test_advance_host_large_grid_banded(hp):
-    """A grid large enough for 16 row bands in the step and 8 in the RHS call, periodic in y
+    """A grid large enough for 16 row bands in the step and in the RHS call, periodic in y
     (band 0 reads the last band)."""
     P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
     c = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=700, ny=900, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=P, bc_top=P)
