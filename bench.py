@@ -633,6 +633,21 @@ def run_gpu(args, rank, world, local_rank):
         M = sm.get_state().reshape(-1, 6)
         F = U_err.reshape(-1, 6)
         ms_stage_m = sm.time_stage(20)
+        e2e_m = None
+        if e2e_steps:   # host buffers, as the FP64 e2e leg: FP64 cell-major state in and out per step
+            min_ = torch.from_numpy(M.reshape(-1).copy()).pin_memory()
+            mout = torch.empty_like(min_).pin_memory()
+            sm.advance_host(min_.numpy(), mout.numpy(), 1)
+            barrier()
+            t0 = time.perf_counter()
+            for _ in range(e2e_steps):
+                sm.advance_host(min_.numpy(), mout.numpy(), 1)
+            barrier()
+            em_s = max_over_ranks(max(time.perf_counter() - t0, 1e-9), world)
+            e2e_m = {"value": world * cells * e2e_steps / em_s, "unit": UNIT, "ms_per_step": em_s / e2e_steps * 1e3,
+                     "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                     "how": "hype_advance_host(U_in, U_out, 1) of the mixed solver, FP64 host state converted band by "
+                            "band on the device; wall clock"}
         sm.close()
 
         def rel(a, b):
@@ -648,7 +663,7 @@ def run_gpu(args, rank, world, local_rank):
                  "status": stm, "stage_ms_per_launch": ms_stage_m, "autotuned_tile": mtile,
                  "bytes_per_cell_update": 9 * (4 * 4 + 2 * 8),
                  "rel_error_vs_fp64_after_run": {"fields_L1_Linf": errs, "steps": err_steps},
-                 "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt"}
+                 "precision": "FP32 state/recon/flux; FP64 E, alpha1, pressure recovery, totals, dt", "e2e": e2e_m}
 
     fast = None if args.no_fast else fast_leg(hp, args, local_rank, world, U0, U_fp64, n_done, value, ms_stage)
     group = None if args.group_slabs <= 1 else group_leg(hp, args, local_rank, U0, U_fp64)

@@ -261,7 +261,7 @@ static cudaError_t stage(hype_solver *s, const double *in, double *out, int mode
 // mixed-precision stage: input state k_in, output k_out (or the interleaved
 // FP64 RHS for OUT_RHS), second state k_x
 static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double ka, double kb, double kc, int k_x, int reduce,
-                           double *out_rhs = nullptr, bool push = false)
+                           double *out_rhs = nullptr, bool push = false, int run0 = 0, int run_count = 0)
 {
     MixedParams p;
     std::memset(&p, 0, sizeof(p));
@@ -277,6 +277,7 @@ static cudaError_t stage_m(hype_solver *s, int k_in, int k_out, int mode, double
     p.mode = mode; p.ka = ka; p.kb = kb; p.kc = kc;
     p.sc = s->dSc; p.reduce_smax = reduce;
     p.strips = s->strips; p.runs = s->runs;
+    p.run0 = run0; p.run_count = run_count;
     p.row_off = s->row_off;
     if (s->test_skip_row >= 0) { p.skip_loads = 1; p.skip_loads_from = s->test_skip_row; }
     if (push && k_out >= 0 && mode != OUT_RHS) {   // a slab's state output: edge rows to the neighbours' halos
@@ -468,8 +469,31 @@ static int fence_copy_streams(hype_solver *s)
     return HYPE_OK;
 }
 
-// host Vec rows of band k -> planes `dst` (via the staging array); ev_in[k] marks them ready
-static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, double *dst)
+// rows r0 .. r0+nr-1 of the input staging array (cell-major) -> state buffer `role`
+// (FP64 planes, or the FP32 and FP64 planes of the mixed state)
+static cudaError_t rows_to_state(hype_solver *s, int role, int r0, int nr, cudaStream_t on)
+{
+    if (s->mixed) {
+        const long long o = (long long)r0 * s->pitch;
+        return launch_aos_to_mixed(s->cfg.system, s->dAosIn + (size_t)r0 * s->cfg.nx * s->nv, s->mf[role] + o, s->md[role] + o,
+                                   s->cfg.nx, nr, s->pitch, s->plane, on);
+    }
+    return launch_aos_to_planes_rows(s->dAosIn, buf_of(s, role), s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, on);
+}
+
+// rows r0 .. r0+nr-1 of state buffer `role` -> the output staging array (cell-major)
+static cudaError_t state_to_rows(hype_solver *s, int role, int r0, int nr, cudaStream_t on)
+{
+    if (s->mixed) {
+        const long long o = (long long)r0 * s->pitch;
+        return launch_mixed_to_aos(s->cfg.system, s->mf[role] + o, s->md[role] + o, s->dAosOut + (size_t)r0 * s->cfg.nx * s->nv,
+                                   s->cfg.nx, nr, s->pitch, s->plane, on);
+    }
+    return launch_planes_to_aos_rows(buf_of(s, role), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, on);
+}
+
+// host Vec rows of band k -> state buffer `role` (via the staging array); ev_in[k] marks them ready
+static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, int role)
 {
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     const int r0 = b.row[k], nr = b.row[k + 1] - r0;
@@ -477,13 +501,14 @@ static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, d
                                 cudaMemcpyHostToDevice, s->cin));
     CUDA_TRY(s, cudaEventRecord(s->ev_cp[k], s->cin));
     CUDA_TRY(s, cudaStreamWaitEvent(s->cvin, s->ev_cp[k], 0));
-    CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, dst, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cvin));
+    CUDA_TRY(s, rows_to_state(s, role, r0, nr, s->cvin));
     CUDA_TRY(s, cudaEventRecord(s->ev_in[k], s->cvin));
     return HYPE_OK;
 }
 
 // one stage of `q` over band k's runs of the banded decomposition, on stream `on`
-// (the solver's compute stream by default)
+// (the solver's compute stream by default); `out` (with out_aos) replaces q.out,
+// for the mixed state an RHS output (OUT_RHS) only
 static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanStage &q, int out_aos = 0, double *out = nullptr,
                               cudaStream_t on = nullptr)
 {
@@ -491,8 +516,10 @@ static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanS
     cudaStream_t saved_stream = s->stream;
     s->runs = b.runs;
     if (on) s->stream = on;
-    const cudaError_t e = stage(s, buf_of(s, q.in), out ? out : buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x),
-                                buf_of(s, q.out2), q.reduce, out_aos, b.run[k], b.run[k + 1] - b.run[k]);
+    const int r0 = b.run[k], nr = b.run[k + 1] - b.run[k];
+    const cudaError_t e = s->mixed ? stage_m(s, q.in, out ? -1 : q.out, q.mode, q.ka, q.kb, q.kc, q.x, q.reduce, out, false, r0, nr)
+                                   : stage(s, buf_of(s, q.in), out ? out : buf_of(s, q.out), q.mode, q.ka, q.kb, q.kc, buf_of(s, q.x),
+                                           buf_of(s, q.out2), q.reduce, out_aos, r0, nr);
     s->runs = saved;
     s->stream = saved_stream;
     return e;
@@ -502,12 +529,12 @@ static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanS
 // launched as soon as the uploads it reads are enqueued (and waited for);
 // `after` runs behind every band launch (e.g. its download).
 template <typename After>
-static int banded_upload_stage(hype_solver *s, const Bands &b, const double *U, double *dst, const PlanStage &q, int out_aos,
+static int banded_upload_stage(hype_solver *s, const Bands &b, const double *U, int role, const PlanStage &q, int out_aos,
                                double *out, After after)
 {
     int rc, next = 0;
     for (int u = 0; u < b.n; ++u) {
-        if ((rc = upload_band(s, b, u, U, dst))) return rc;
+        if ((rc = upload_band(s, b, u, U, role))) return rc;
         while (next < b.n && band_needs(s, b, b.order[next]) <= u) {
             const int k = b.order[next++];
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_in[band_needs(s, b, k)], 0));
@@ -822,22 +849,12 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
     if (!s->dSc) return fail(s, HYPE_ERR_INVALID, "solver not created");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     int rc;
-    if (s->mixed) {   // whole-array copies around the mixed kernel
-        const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
-        CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
-        CUDA_TRY(s, load_state(s, s->dAosIn, 1));
-        rc = rhs_common(s, s->dAosOut, dt);
-        if (rc && rc != HYPE_ERR_INADMISSIBLE) return rc;
-        CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-        return rc;
-    }
     // banded: U's rows stream in while earlier bands compute, RHS rows stream out
     const Bands b = host_bands(s);
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
     const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
-    rc = banded_upload_stage(s, b, U, s->dS0, q, 1, s->dAosOut, [&](int k) -> int {
+    rc = banded_upload_stage(s, b, U, B_S0, q, 1, s->dAosOut, [&](int k) -> int {
         // band k's RHS rows are final: copy them out while later bands compute
         const int r0 = b.row[k], nr = b.row[k + 1] - r0;
         CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
@@ -1028,7 +1045,7 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
     for (int j = 1; j < 4; ++j) CUDA_TRY(s, cudaStreamWaitEvent(on_stage[j], s->ev_fence, 0));
     if (U_in)
         for (int k = 0; k < b.n; ++k)
-            if ((rc = upload_band(s, b, k, U_in, buf_of(s, plan[0].in)))) return rc;
+            if ((rc = upload_band(s, b, k, U_in, plan[0].in))) return rc;
     for (int st = 0; st < ns; ++st) {
         const PlanStage &q = plan[st];
         cudaStream_t on = on_stage[st % 4];
@@ -1048,7 +1065,7 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
             if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
                 const int r0 = b.row[k], nr = b.row[k + 1] - r0;
                 CUDA_TRY(s, cudaStreamWaitEvent(s->cvout, done, 0));
-                CUDA_TRY(s, launch_planes_to_aos_rows(buf_of(s, q.out), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, s->cvout));
+                CUDA_TRY(s, state_to_rows(s, q.out, r0, nr, s->cvout));
                 CUDA_TRY(s, cudaEventRecord(s->ev_dc[k], s->cvout));
                 CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_dc[k], 0));
                 CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
@@ -1070,7 +1087,7 @@ int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nst
     if (!s->began) return fail(s, HYPE_ERR_INVALID, "hype_begin not called");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     int rc;
-    const bool banded = !s->mixed && s->cfg.order != 0;   // forward Euler's last write is a copy, not a stage
+    const bool banded = s->cfg.order != 0;   // forward Euler's last write is a copy, not a stage
     if (!banded) {
         if ((rc = hype_set_state(s, U_in)) || (rc = hype_advance(s, nsteps))) return rc;
         rc = hype_wait(s, steps_done, t_end, dt_next);

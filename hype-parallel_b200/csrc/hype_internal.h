@@ -186,6 +186,7 @@ struct MixedParams {
     DevScalars *sc;
     int reduce_smax;
     int strips, runs;
+    int run0, run_count;        // grid form: the launch covers runs run0 .. run0+run_count-1 (0: all runs)
     // y-slab of a decomposed grid, as StageParams: row_off halo rows below and above in
     // every plane; state rows 0..2 and ny-3..ny-1 also go to the neighbours' halo rows
     int row_off;

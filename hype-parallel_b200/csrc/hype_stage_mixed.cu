@@ -564,7 +564,7 @@ mixed_kernel(const __grid_constant__ MixedMaps maps, const MixedParams p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    mixed_tile<CELLS, SLAB>(p, &maps, blockIdx.x, blockIdx.y, smem_raw, red_s);
+    mixed_tile<CELLS, SLAB>(p, &maps, blockIdx.x, p.run0 + (int)blockIdx.y, smem_raw, red_s);
 }
 
 template <int CELLS>
@@ -648,7 +648,8 @@ cudaError_t launch_mixed(int sys, int cells, const MixedMaps &maps, const MixedP
     MixedMaps mm = maps;
     MixedParams pp = p;
     void *args[] = {&mm, &pp};
-    return cudaLaunchKernel(p.row_off ? e.slab : e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
+    const unsigned gy = (unsigned)(p.run_count > 0 ? p.run_count : p.runs);
+    return cudaLaunchKernel(p.row_off ? e.slab : e.single, dim3((unsigned)p.strips, gy, 1), dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
 }
 
 cudaError_t launch_mixed_batch(int sys, int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,

@@ -694,7 +694,7 @@ mixsys_kernel(const __grid_constant__ MixedMaps maps, const MixedParams p)
 {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ double red_s[2 * CELLS / 32];
-    mixsys_tile<SYS, CELLS, SLAB>(p, &maps, blockIdx.x, blockIdx.y, smem_raw, red_s);
+    mixsys_tile<SYS, CELLS, SLAB>(p, &maps, blockIdx.x, p.run0 + (int)blockIdx.y, smem_raw, red_s);
 }
 
 template <int SYS, int CELLS>
@@ -772,8 +772,9 @@ cudaError_t launch_mixsys(int sys, int cells, const MixedMaps &maps, const Mixed
     MixedMaps mm = maps;
     MixedParams pp = p;
     void *args[] = {&mm, &pp};
-    return cudaLaunchKernel(p.row_off ? e.slab : e.single, dim3((unsigned)p.strips, (unsigned)p.runs, 1),
-                            dim3((unsigned)e.threads, 1, 1), args, e.smem, s);
+    const unsigned gy = (unsigned)(p.run_count > 0 ? p.run_count : p.runs);
+    return cudaLaunchKernel(p.row_off ? e.slab : e.single, dim3((unsigned)p.strips, gy, 1), dim3((unsigned)e.threads, 1, 1), args,
+                            e.smem, s);
 }
 
 cudaError_t launch_mixsys_batch(int sys, int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,

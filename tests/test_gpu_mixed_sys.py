@@ -194,3 +194,49 @@ def test_mixed_bn_and_euler_slabs_equal_lone(hp, system, nslabs):
         U2 = grp.get_state()
     assert st1 == st2 == hp.OK and (k1, t1, dt1) == (k2, t2, dt2)
     assert U1.tobytes() == U2.tobytes()
+
+
+HOST_BAND_CASES = [
+    # system, kind, nx, ny, periodic y
+    (O.KAPILA, "bubble", 640, 720, False),
+    (O.KAPILA, "bubble", 600, 704, True),
+    (O.BN, "discs", 480, 512, False),
+    (O.EULER, "quadrants", 512, 600, True),
+]
+
+
+@pytest.mark.parametrize("system,kind,nx,ny,periodic", HOST_BAND_CASES)
+def test_mixed_host_calls_banded_equal_unbanded(hp, system, kind, nx, ny, periodic):
+    """The host-buffer calls of a mixed solver run band by band (16 row bands, every
+    stage a wavefront on four streams, copies overlapped): hype_advance_host gives the
+    bits of set_state + advance + wait + get_state (1 and 2 steps), and hype_rhs_prim
+    from host arrays the bits and dt of the whole-grid call on device pointers."""
+    import torch
+    eos = cases.KAPILA_EOS if system != O.EULER else dict(gamma1=1.4, gamma2=1.4, pi1=0.0, pi2=0.0)
+    yb = P_ if periodic else R_
+    cfg = O.Config(system=system, order=2, nx=nx, ny=ny, bc_left=T_, bc_right=T_, bc_bottom=yb, bc_top=yb, **eos)
+    U = cases.state(cfg, kind, 70 + nx % 7)
+    pc = cases.to_pkg(cfg)
+    pc.precision = hp.PREC_MIXED
+    for nsteps in (1, 2):
+        with hp.Solver(pc) as s:
+            s.set_state(U)
+            s.begin(0.0, 1e30, 100)
+            s.advance(nsteps)
+            ref = (s.wait(), s.get_state())
+        out = np.empty_like(U)
+        with hp.Solver(pc) as s:
+            assert s.launch_info()["grid"][1] >= 8
+            s.set_state(U)
+            s.begin(0.0, 1e30, 100)
+            got = s.advance_host(U, out, nsteps)
+        assert got[3] == hp.OK and got[:3] == ref[0][:3]
+        assert out.tobytes() == ref[1].tobytes()
+    dU = torch.from_numpy(U).cuda()
+    dR = torch.empty_like(dU)
+    torch.cuda.synchronize()
+    with hp.Solver(pc) as s:
+        dt_d, st_d = s.rhs_function_prim_device(0.0, dU.data_ptr(), dR.data_ptr())
+        R, dt_h, st_h = s.rhs_function_prim(0.0, U)
+    assert st_d == hp.OK and st_h == hp.OK and dt_h == dt_d
+    assert R.tobytes() == dR.cpu().numpy().tobytes()
