@@ -419,7 +419,8 @@ struct Bands {
     int order[hype_solver::MAX_BANDS];     // launch order: band 0 last on a periodic y axis (it reads the last band)
 };
 
-// up to `max_bands` bands of `per` runs each, at least 8 rows per run
+// up to `max_bands` bands of at least `per` runs each (fewer bands on short grids,
+// so that no launch shrinks below `per` runs), at least 8 rows per run
 static Bands make_bands(const hype_solver *s, int max_bands, int per)
 {
     Bands b;
@@ -431,7 +432,7 @@ static Bands make_bands(const hype_solver *s, int max_bands, int per)
     if (runs > cap) runs = cap;
     if (runs < 1) runs = 1;
     b.runs = runs;
-    b.n = runs < max_bands ? runs : max_bands;
+    b.n = runs / per < 1 ? 1 : (runs / per > max_bands ? max_bands : runs / per);
     for (int k = 0; k <= b.n; ++k) {
         b.run[k] = (int)(((long long)k * runs) / b.n);
         b.row[k] = (int)(((long long)b.run[k] * ny) / runs);
@@ -525,16 +526,17 @@ static cudaError_t stage_band(hype_solver *s, const Bands &b, int k, const PlanS
     return e;
 }
 
-// First stage of a banded call: uploads of bands 0..n-1 in order, each band
-// launched as soon as the uploads it reads are enqueued (and waited for);
-// `after` runs behind every band launch (e.g. its download).
-template <typename After>
-static int banded_upload_stage(hype_solver *s, const Bands &b, const double *U, int role, const PlanStage &q, int out_aos,
-                               double *out, After after)
+// First stage of a banded call: uploads of bands 0..n-1 in order (`upload(k)`,
+// which records ev_in[k]), each band launched as soon as the uploads it reads
+// are enqueued (and waited for); `after` runs behind every band launch (e.g. its
+// download).
+template <typename Upload, typename After>
+static int banded_upload_stage(hype_solver *s, const Bands &b, Upload upload, const PlanStage &q, int out_aos, double *out,
+                               After after)
 {
     int rc, next = 0;
     for (int u = 0; u < b.n; ++u) {
-        if ((rc = upload_band(s, b, u, U, role))) return rc;
+        if ((rc = upload(u))) return rc;
         while (next < b.n && band_needs(s, b, b.order[next]) <= u) {
             const int k = b.order[next++];
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_in[band_needs(s, b, k)], 0));
@@ -854,7 +856,7 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
     const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
-    rc = banded_upload_stage(s, b, U, B_S0, q, 1, s->dAosOut, [&](int k) -> int {
+    rc = banded_upload_stage(s, b, [&](int k) { return upload_band(s, b, k, U, B_S0); }, q, 1, s->dAosOut, [&](int k) -> int {
         // band k's RHS rows are final: copy them out while later bands compute
         const int r0 = b.row[k], nr = b.row[k + 1] - r0;
         CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
@@ -895,45 +897,50 @@ int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_
     (void)t;
     if (!s || !U || !RHS) return fail(s, HYPE_ERR_INVALID, "null argument");
     if (!s->dSc || s->row_off == 0) return fail(s, HYPE_ERR_INVALID, "not a slab or block solver (hype_create_slab, hype_create_block)");
-    const int nx = s->cfg.nx, rows = s->cfg.ny;
+    const int nx = s->cfg.nx;
     const int lo = s->cfg.bc_bottom == BC_HALO ? 3 : 0, hi = s->cfg.bc_top == BC_HALO ? 3 : 0;
     const int cl = s->cfg.bc_left == BC_HALO ? 3 : 0, cr = s->cfg.bc_right == BC_HALO ? 3 : 0;
     const int width = cl + nx + cr;   // cells per staged row
     if (row_stride < (long long)width * s->nv) return fail(s, HYPE_ERR_INVALID, "row_stride below the staged row width * nvar");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
-    const size_t row_bytes = sizeof(double) * (size_t)nx * s->nv;
+    const size_t srow = (size_t)width * s->nv;   // elements per staged row; staging row j + 3 holds local row j
     int rc;
-    if (s->col_off) {   // a block: rows -lo .. rows+hi-1, columns -cl .. nx+cr-1, compact, then planes
-        const size_t wide_bytes = sizeof(double) * (size_t)width * s->nv;
-        CUDA_TRY(s, cudaMemcpy2DAsync(s->dAosIn, wide_bytes, U - (long long)lo * row_stride - (long long)cl * s->nv,
-                                      sizeof(double) * (size_t)row_stride, wide_bytes, (size_t)(rows + lo + hi),
-                                      cudaMemcpyHostToDevice, s->stream));
-        CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, s->dS0 - (long long)lo * s->pitch - cl, width, 0, rows + lo + hi, s->nv,
-                                              s->pitch, s->plane, s->stream));
-        if ((rc = reset_scalars(s))) return rc;
-        CUDA_TRY(s, stage(s, s->dS0, s->dAosOut, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
-        CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, row_bytes * rows, cudaMemcpyDeviceToHost, s->stream));
-        if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
-        if (dt) *dt = host_dt(s);
-        return rc;
-    }
-    // the slab's rows and its ghost rows into the staging array (local row -3 first), then planes
-    CUDA_TRY(s, cudaMemcpy2DAsync(s->dAosIn + (size_t)(3 - lo) * nx * s->nv, row_bytes, U - (long long)lo * row_stride,
-                                  sizeof(double) * (size_t)row_stride, row_bytes, (size_t)(rows + lo + hi), cudaMemcpyHostToDevice,
-                                  s->stream));
-    if (s->mixed) {   // rows -lo .. rows+hi-1 into the mixed state S0 (FP32 and FP64 planes)
-        const size_t row_elems = (size_t)nx * s->nv;
-        CUDA_TRY(s, launch_aos_to_mixed(s->cfg.system, s->dAosIn + (size_t)(3 - lo) * row_elems, s->mf[1] - (long long)lo * s->pitch,
-                                        s->md[1] - (long long)lo * s->pitch, nx, rows + lo + hi, s->pitch, s->plane, s->stream));
-        if ((rc = reset_scalars(s))) return rc;
-        CUDA_TRY(s, stage_m(s, 1, -1, OUT_RHS, 0, 1.0, 0, -1, 1, s->dAosOut));
-    } else {
-        CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, solver_alloc_base(s, s->dS0), nx, 3 - lo, rows + lo + hi, s->nv, s->pitch,
-                                              s->plane, s->stream));
-        if ((rc = reset_scalars(s))) return rc;
-        CUDA_TRY(s, stage(s, s->dS0, s->dAosOut, OUT_RHS, 0, 1.0, 0, nullptr, nullptr, 1, 1));
-    }
-    CUDA_TRY(s, cudaMemcpyAsync(RHS, s->dAosOut, row_bytes * rows, cudaMemcpyDeviceToHost, s->stream));
+    // banded as hype_rhs_prim: band k's rows (with the ghost rows below band 0 and above
+    // the last band) are copied from the local array and converted, its RHS launch runs
+    // once the rows its stencils read are there, and its RHS rows go to the host while
+    // later bands compute
+    const Bands b = host_bands(s);
+    if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
+    auto upload = [&](int k) -> int {
+        const int a = b.row[k] - (k == 0 ? lo : 0), e = b.row[k + 1] + (k == b.n - 1 ? hi : 0);   // local rows a .. e-1
+        double *stg = s->dAosIn + (size_t)(a + 3) * srow;
+        CUDA_TRY(s, cudaMemcpy2DAsync(stg, sizeof(double) * srow, U + (long long)a * row_stride - (long long)cl * s->nv,
+                                      sizeof(double) * (size_t)row_stride, sizeof(double) * srow, (size_t)(e - a),
+                                      cudaMemcpyHostToDevice, s->cin));
+        CUDA_TRY(s, cudaEventRecord(s->ev_cp[k], s->cin));
+        CUDA_TRY(s, cudaStreamWaitEvent(s->cvin, s->ev_cp[k], 0));
+        if (s->mixed) {   // FP32 and FP64 planes of S0 (a mixed solver is never split in x)
+            const long long o = (long long)a * s->pitch;
+            CUDA_TRY(s, launch_aos_to_mixed(s->cfg.system, stg, s->mf[1] + o, s->md[1] + o, nx, e - a, s->pitch, s->plane, s->cvin));
+        } else {          // planes of S0 from local row -3, column -cl on
+            CUDA_TRY(s, launch_aos_to_planes_rows(s->dAosIn, s->dS0 - 3LL * s->pitch - cl, width, a + 3, e - a, s->nv, s->pitch,
+                                                  s->plane, s->cvin));
+        }
+        CUDA_TRY(s, cudaEventRecord(s->ev_in[k], s->cvin));
+        return HYPE_OK;
+    };
+    const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
+    const size_t row_elems = (size_t)nx * s->nv;
+    rc = banded_upload_stage(s, b, upload, q, 1, s->dAosOut, [&](int k) -> int {
+        const int r0 = b.row[k], nr = b.row[k + 1] - r0;
+        CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
+        CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
+        CUDA_TRY(s, cudaMemcpyAsync(RHS + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
+                                    cudaMemcpyDeviceToHost, s->cout));
+        return HYPE_OK;
+    });
+    if (rc) return rc;
+    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
     if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
     if (dt) *dt = host_dt(s);
     return rc;

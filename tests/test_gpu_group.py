@@ -341,3 +341,84 @@ def test_rhs_prim_block_reads_only_its_halo(name, px, py, hp, orc):
     assert R.reshape(-1).tobytes() == Ro.tobytes()
     if not cfg.viscous:
         assert min(dts) == dto
+
+
+def _local_arrays(Ug, ys, ym, xs, xm, perx, pery):
+    """DMDA-style local array of block (ys, ym) x (xs, xm): 3 ghost rows and columns
+    from the neighbours (periodic axes wrap), NaN where the grid ends."""
+    ny, nx, _ = Ug.shape
+    rr, cc = np.arange(ys - 3, ys + ym + 3), np.arange(xs - 3, xs + xm + 3)
+    loc = Ug[np.ix_(rr % ny, cc % nx)].copy()
+    if not pery:
+        loc[(rr < 0) | (rr >= ny)] = np.nan
+    if not perx:
+        loc[:, (cc < 0) | (cc >= nx)] = np.nan
+    return np.ascontiguousarray(loc)
+
+
+LARGE_SPLITS = [
+    # system, nx, ny, px, py, periodic x, periodic y, mixed, anchor
+    (O.KAPILA, 300, 420, 1, 3, False, False, False, "reference"),
+    (O.BN, 260, 300, 3, 2, False, True, False, "reference"),
+    (O.KAPILA, 1100, 1200, 1, 2, False, False, False, "device"),
+    (O.KAPILA, 1100, 1200, 2, 2, True, True, False, "device"),
+    (O.BN, 1024, 1400, 1, 2, False, True, False, "device"),
+    (O.KAPILA, 1100, 1200, 1, 2, False, True, True, "device"),
+]
+
+
+@pytest.mark.parametrize("system,nx,ny,px,py,perx,pery,mixed,anchor", LARGE_SPLITS)
+def test_rhs_prim_slab_banded_large(system, nx, ny, px, py, perx, pery, mixed, anchor, hp, orc):
+    """hype_rhs_prim_slab on blocks of 130-700 rows, which run as 1-5 row bands (each
+    band's rows copied from the local array, converted and launched as they arrive,
+    its RHS rows copied out while later bands compute): the blocks make, bit for bit,
+    the reference's RHS, or the whole-grid RHS on device pointers (itself the
+    reference's bits in FP64, test_gpu_parity.py), and the least of their dt its dt."""
+    import ctypes
+    import torch
+    bx = P if perx else T
+    by = P if pery else R
+    cfg = O.Config(system=system, order=2, nx=nx, ny=ny, bc_left=bx, bc_right=bx, bc_bottom=by, bc_top=by, **cases.KAPILA_EOS)
+    U = cases.state(cfg, "bubble" if system == O.KAPILA else "discs", 90 + px + 3 * py)
+    pc = cases.to_pkg(cfg)
+    if mixed:
+        pc.precision = hp.PREC_MIXED
+    if anchor == "reference":
+        Ro, dto, sto = orc.rhs(cfg, U)
+    else:
+        dU = torch.from_numpy(U).cuda()
+        dR = torch.empty_like(dU)
+        torch.cuda.synchronize()
+        with hp.Solver(pc) as s:
+            dto, sto = s.rhs_function_prim_device(0.0, dU.data_ptr(), dR.data_ptr())
+        Ro = dR.cpu().numpy()
+    assert sto == hp.OK
+    nv = cfg.nvar
+    Ug = U.reshape(ny, nx, nv)
+    L = hp.lib()
+    DP = ctypes.POINTER(ctypes.c_double)
+    L.hype_create_block.argtypes = [ctypes.POINTER(hp._Cfg), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(ctypes.c_void_p)]
+    L.hype_rhs_prim_slab.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong, DP, DP]
+
+    def split(n, p):
+        sizes = [n // p + (1 if r < n % p else 0) for r in range(p)]
+        return [(sum(sizes[:r]), sizes[r]) for r in range(p)]
+    Rg = np.full((ny, nx, nv), np.nan)
+    dts = []
+    for ys, ym in split(ny, py):
+        for xs, xm in split(nx, px):
+            loc = _local_arrays(Ug, ys, ym, xs, xm, perx, pery)
+            h = ctypes.c_void_p()
+            st = L.hype_create_block(ctypes.byref(pc.c_struct()), xs, xm, ys, ym, ctypes.byref(h))
+            assert st == hp.OK, L.hype_last_error(h)
+            Rr = np.empty(ym * xm * nv)
+            dt = ctypes.c_double()
+            base = loc.ctypes.data + ((3 * (xm + 6) + 3) * nv) * 8
+            st = L.hype_rhs_prim_slab(h, 0.0, base, (xm + 6) * nv, Rr.ctypes.data_as(DP), ctypes.byref(dt))
+            L.hype_destroy(h)
+            assert st == hp.OK
+            Rg[ys:ys + ym, xs:xs + xm] = Rr.reshape(ym, xm, nv)
+            dts.append(dt.value)
+    assert Rg.reshape(-1).tobytes() == Ro.tobytes()
+    assert min(dts) == dto

@@ -207,7 +207,7 @@ HOST_BAND_CASES = [
 
 @pytest.mark.parametrize("system,kind,nx,ny,periodic", HOST_BAND_CASES)
 def test_mixed_host_calls_banded_equal_unbanded(hp, system, kind, nx, ny, periodic):
-    """The host-buffer calls of a mixed solver run band by band (16 row bands, every
+    """The host-buffer calls of a mixed solver run band by band (row bands, every
     stage a wavefront on four streams, copies overlapped): hype_advance_host gives the
     bits of set_state + advance + wait + get_state (1 and 2 steps), and hype_rhs_prim
     from host arrays the bits and dt of the whole-grid call on device pointers."""

@@ -280,8 +280,8 @@ def test_advance_host_equals_set_advance_get(name, nsteps, hp):
 
 
 def test_advance_host_large_grid_banded(hp):
-    """A grid large enough for 16 row bands in the step and in the RHS call, periodic in y
-    (band 0 reads the last band)."""
+    """A grid large enough for several row bands in the step and in the RHS call, periodic
+    in y (band 0 reads the last band)."""
     P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
     c = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=700, ny=900, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=P, bc_top=P)
     U = hp.initial_state(c, "shock_bubble", seed=12, nbubbles=3)
@@ -305,7 +305,7 @@ def test_advance_host_large_grid_banded(hp):
 @pytest.mark.parametrize("order,periodic,nsteps,flags", [(2, False, 1, 0), (3, False, 1, 0), (1, True, 3, 0), (2, True, 1, 0),
                                                         (2, False, 2, 4), (2, False, 1, 2)])
 def test_advance_host_wavefront(order, periodic, nsteps, flags, hp):
-    """16 row bands, every stage launched band by band on its own stream behind the
+    """Row bands, every stage launched band by band on its own stream behind the
     upload and the result downloaded band by band (one-step calls do both): the bits
     of the unbanded step, for N = 1..3 (N = 3: ten stages on four streams), periodic y,
     the viscous and the conservative paths."""
