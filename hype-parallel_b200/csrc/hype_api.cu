@@ -493,13 +493,72 @@ static cudaError_t state_to_rows(hype_solver *s, int role, int r0, int nr, cudaS
     return launch_planes_to_aos_rows(buf_of(s, role), s->dAosOut, s->cfg.nx, r0, nr, s->nv, s->pitch, s->plane, on);
 }
 
+// Host side of a banded call: a pageable caller array goes through pinned staging
+// (its bands copied by the host copy pool, hype_hostcopy.cu), a pinned one is
+// copied directly.  Downloads into staging are finished on the host, band by
+// band as they land, by finish_downloads.
+struct HostIO {
+    bool stage_in = false, stage_out = false;
+    int nd = 0;   // staged downloads enqueued
+    struct Pending { int k; size_t off, n; } d[hype_solver::MAX_BANDS];
+};
+
+static HostIO host_io(hype_solver *s, const void *in, const void *out)
+{
+    HostIO io;
+    const bool want_in = in && host_is_pageable(in), want_out = out && host_is_pageable(out);
+    if ((want_in || want_out) && !s->hStageIn) {   // first use; without pinned memory the copies stay direct
+        if (cudaHostAlloc(&s->hStageIn, s->aos_bytes, cudaHostAllocDefault) != cudaSuccess ||
+            cudaHostAlloc(&s->hStageOut, s->aos_bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            if (s->hStageIn) cudaFreeHost(s->hStageIn);
+            s->hStageIn = nullptr;
+            s->hStageOut = nullptr;
+        }
+    }
+    io.stage_in = want_in && s->hStageIn;
+    io.stage_out = want_out && s->hStageOut;
+    return io;
+}
+
+// n elements at element offset `off` of the output staging array (dAosOut) to
+// dst + off, on `cout` behind what it waits for (band k of the call)
+static int download_rows(hype_solver *s, HostIO &io, int k, double *dst, size_t off, size_t n)
+{
+    if (!io.stage_out) {
+        CUDA_TRY(s, cudaMemcpyAsync(dst + off, s->dAosOut + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->cout));
+        return HYPE_OK;
+    }
+    CUDA_TRY(s, cudaMemcpyAsync(s->hStageOut + off, s->dAosOut + off, sizeof(double) * n, cudaMemcpyDeviceToHost, s->cout));
+    CUDA_TRY(s, cudaEventRecord(s->ev_dl[k], s->cout));
+    io.d[io.nd++] = {k, off, n};
+    return HYPE_OK;
+}
+
+// the staged downloads to dst as they land, then every copy of the call done
+static int finish_downloads(hype_solver *s, HostIO &io, double *dst)
+{
+    for (int j = 0; j < io.nd; ++j) {
+        const HostIO::Pending &d = io.d[j];
+        CUDA_TRY(s, cudaEventSynchronize(s->ev_dl[d.k]));
+        host_copy(dst + d.off, s->hStageOut + d.off, sizeof(double) * d.n);
+    }
+    io.nd = 0;
+    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
+    return HYPE_OK;
+}
+
 // host Vec rows of band k -> state buffer `role` (via the staging array); ev_in[k] marks them ready
-static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, int role)
+static int upload_band(hype_solver *s, const Bands &b, int k, const double *U, int role, const HostIO &io)
 {
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     const int r0 = b.row[k], nr = b.row[k + 1] - r0;
-    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn + r0 * row_elems, U + r0 * row_elems, sizeof(double) * row_elems * nr,
-                                cudaMemcpyHostToDevice, s->cin));
+    const double *from = U + r0 * row_elems;
+    if (io.stage_in) {
+        host_copy(s->hStageIn + r0 * row_elems, from, sizeof(double) * row_elems * nr);
+        from = s->hStageIn + r0 * row_elems;
+    }
+    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn + r0 * row_elems, from, sizeof(double) * row_elems * nr, cudaMemcpyHostToDevice, s->cin));
     CUDA_TRY(s, cudaEventRecord(s->ev_cp[k], s->cin));
     CUDA_TRY(s, cudaStreamWaitEvent(s->cvin, s->ev_cp[k], 0));
     CUDA_TRY(s, rows_to_state(s, role, r0, nr, s->cvin));
@@ -619,7 +678,10 @@ int hype_destroy(hype_solver *s)
         if (s->ev_in[k]) cudaEventDestroy(s->ev_in[k]);
         if (s->ev_dc[k]) cudaEventDestroy(s->ev_dc[k]);
         if (s->ev_done[k]) cudaEventDestroy(s->ev_done[k]);
+        if (s->ev_dl[k]) cudaEventDestroy(s->ev_dl[k]);
     }
+    if (s->hStageIn) cudaFreeHost(s->hStageIn);
+    if (s->hStageOut) cudaFreeHost(s->hStageOut);
     if (s->ev_fence) cudaEventDestroy(s->ev_fence);
     for (cudaEvent_t e : s->ev_sb) if (e) cudaEventDestroy(e);
     for (cudaStream_t *q : {&s->stream2, &s->stream3, &s->stream4, &s->cin, &s->cout, &s->cvin, &s->cvout})
@@ -666,7 +728,7 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     for (cudaStream_t *q : {&s->cin, &s->cout, &s->cvin, &s->cvout, &s->stream2, &s->stream3, &s->stream4})
         CUDA_TRY(s, cudaStreamCreateWithFlags(q, cudaStreamNonBlocking));
     for (int k = 0; k < hype_solver::MAX_BANDS; ++k)
-        for (cudaEvent_t *e : {&s->ev_cp[k], &s->ev_in[k], &s->ev_dc[k], &s->ev_done[k]})
+        for (cudaEvent_t *e : {&s->ev_cp[k], &s->ev_in[k], &s->ev_dc[k], &s->ev_done[k], &s->ev_dl[k]})
             CUDA_TRY(s, cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     CUDA_TRY(s, cudaEventCreateWithFlags(&s->ev_fence, cudaEventDisableTiming));
     for (cudaEvent_t &e : s->ev_sb) CUDA_TRY(s, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
@@ -692,6 +754,7 @@ static int create_common(hype_solver *s, const hype_config *cfg, int row_off, co
     }
     if (cudaMalloc(&s->dAosIn, aos_bytes) != cudaSuccess || cudaMalloc(&s->dAosOut, aos_bytes) != cudaSuccess)
         return fail(s, HYPE_ERR_NOMEM, "cudaMalloc(%zu) failed", aos_bytes);
+    s->aos_bytes = aos_bytes;
     CUDA_TRY(s, cudaMalloc(&s->dRed, sizeof(double) * TOTALS_SCRATCH));
     CUDA_TRY(s, cudaMalloc(&s->dSc, sizeof(DevScalars)));
     CUDA_TRY(s, cudaMemset(s->dSc, 0, sizeof(DevScalars)));
@@ -856,17 +919,16 @@ int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
     const PlanStage q{B_S0, B_NONE, OUT_RHS, 0.0, 1.0, 0.0, B_NONE, B_NONE, 1};
-    rc = banded_upload_stage(s, b, [&](int k) { return upload_band(s, b, k, U, B_S0); }, q, 1, s->dAosOut, [&](int k) -> int {
+    HostIO io = host_io(s, U, RHS);
+    rc = banded_upload_stage(s, b, [&](int k) { return upload_band(s, b, k, U, B_S0, io); }, q, 1, s->dAosOut, [&](int k) -> int {
         // band k's RHS rows are final: copy them out while later bands compute
         const int r0 = b.row[k], nr = b.row[k + 1] - r0;
         CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
         CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
-        CUDA_TRY(s, cudaMemcpyAsync(RHS + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
-                                    cudaMemcpyDeviceToHost, s->cout));
-        return HYPE_OK;
+        return download_rows(s, io, k, RHS, r0 * row_elems, row_elems * nr);
     });
     if (rc) return rc;
-    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
+    if ((rc = finish_downloads(s, io, RHS))) return rc;
     if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
     if (dt) {
         *dt = host_dt(s);
@@ -911,12 +973,19 @@ int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_
     // later bands compute
     const Bands b = host_bands(s);
     if ((rc = fence_copy_streams(s)) || (rc = reset_scalars(s))) return rc;
+    HostIO io = host_io(s, U, RHS);
     auto upload = [&](int k) -> int {
         const int a = b.row[k] - (k == 0 ? lo : 0), e = b.row[k + 1] + (k == b.n - 1 ? hi : 0);   // local rows a .. e-1
         double *stg = s->dAosIn + (size_t)(a + 3) * srow;
-        CUDA_TRY(s, cudaMemcpy2DAsync(stg, sizeof(double) * srow, U + (long long)a * row_stride - (long long)cl * s->nv,
-                                      sizeof(double) * (size_t)row_stride, sizeof(double) * srow, (size_t)(e - a),
-                                      cudaMemcpyHostToDevice, s->cin));
+        const double *from = U + (long long)a * row_stride - (long long)cl * s->nv;
+        if (io.stage_in) {   // the rows compacted into pinned staging, then one contiguous copy
+            double *h = s->hStageIn + (size_t)(a + 3) * srow;
+            host_copy_2d(h, sizeof(double) * srow, from, sizeof(double) * (size_t)row_stride, sizeof(double) * srow, (size_t)(e - a));
+            CUDA_TRY(s, cudaMemcpyAsync(stg, h, sizeof(double) * srow * (e - a), cudaMemcpyHostToDevice, s->cin));
+        } else {
+            CUDA_TRY(s, cudaMemcpy2DAsync(stg, sizeof(double) * srow, from, sizeof(double) * (size_t)row_stride, sizeof(double) * srow,
+                                          (size_t)(e - a), cudaMemcpyHostToDevice, s->cin));
+        }
         CUDA_TRY(s, cudaEventRecord(s->ev_cp[k], s->cin));
         CUDA_TRY(s, cudaStreamWaitEvent(s->cvin, s->ev_cp[k], 0));
         if (s->mixed) {   // FP32 and FP64 planes of S0 (a mixed solver is never split in x)
@@ -935,12 +1004,10 @@ int hype_rhs_prim_slab(hype_solver *s, double t, const double *U, long long row_
         const int r0 = b.row[k], nr = b.row[k + 1] - r0;
         CUDA_TRY(s, cudaEventRecord(s->ev_done[k], s->stream));
         CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_done[k], 0));
-        CUDA_TRY(s, cudaMemcpyAsync(RHS + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
-                                    cudaMemcpyDeviceToHost, s->cout));
-        return HYPE_OK;
+        return download_rows(s, io, k, RHS, r0 * row_elems, row_elems * nr);
     });
     if (rc) return rc;
-    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
+    if ((rc = finish_downloads(s, io, RHS))) return rc;
     if ((rc = read_scalars(s)) && rc != HYPE_ERR_INADMISSIBLE) return rc;
     if (dt) *dt = host_dt(s);
     return rc;
@@ -1036,10 +1103,11 @@ int hype_advance(hype_solver *s, int nsteps)
 // the same band of an earlier stage) still reads, so the same dependency covers
 // every overwrite.  Stage s is enqueued band by band on compute stream s % 4, in
 // b.order (band 0 last on a periodic y axis, where it reads the last band), so no
-// band waits behind another that is not ready; the last stage's bands are
-// converted and copied out as they finish (U_out).  Results equal the unbanded
-// step's.
-static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_in, double *U_out)
+// band waits behind another that is not ready.  After each band's upload every
+// launch whose inputs are enqueued is enqueued too, so the device starts while
+// the host still stages later bands; the last stage's bands are converted and
+// copied out as they finish (U_out).  Results equal the unbanded step's.
+static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_in, double *U_out, HostIO &io)
 {
     PlanStage plan[MAX_PLAN];
     int copy_back = 0, rc;
@@ -1047,39 +1115,63 @@ static int enqueue_step_banded(hype_solver *s, const Bands &b, const double *U_i
     const size_t row_elems = (size_t)s->cfg.nx * s->nv;
     const bool py = s->cfg.bc_bottom == HYPE_BC_PERIODIC && b.n > 1;
     cudaStream_t on_stage[4] = {s->stream, s->stream2, s->stream3, s->stream4};
+    bool done[MAX_PLAN][hype_solver::MAX_BANDS] = {};
+    int next[MAX_PLAN] = {};   // per stage: the position in b.order of its next band
+    int uploaded = U_in ? 0 : b.n;
+    auto nbrs = [&](int k, int *nb) -> int {   // bands whose rows band k's stencils read
+        int m = 0;
+        nb[m++] = k;
+        if (k > 0) nb[m++] = k - 1; else if (py) nb[m++] = b.n - 1;
+        if (k + 1 < b.n) nb[m++] = k + 1; else if (py) nb[m++] = 0;
+        return m;
+    };
+    auto ready = [&](int st, int k) -> bool {
+        int nb[3];
+        const int m = nbrs(k, nb);
+        for (int j = 0; j < m; ++j)
+            if (st == 0 ? nb[j] >= uploaded : !done[st - 1][nb[j]]) return false;
+        return true;
+    };
+    auto launch = [&](int st, int k) -> int {
+        const PlanStage &q = plan[st];
+        cudaStream_t on = on_stage[st % 4];
+        int nb[3];
+        const int m = nbrs(k, nb);
+        for (int j = 0; j < m; ++j) {
+            if (st == 0 && U_in) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_in[nb[j]], 0));
+            if (st > 0) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_sb[(st - 1) * hype_solver::MAX_BANDS + nb[j]], 0));
+        }
+        CUDA_TRY(s, stage_band(s, b, k, q, 0, nullptr, on));
+        cudaEvent_t ev = s->ev_sb[st * hype_solver::MAX_BANDS + k];
+        CUDA_TRY(s, cudaEventRecord(ev, on));
+        done[st][k] = true;
+        if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
+            const int r0 = b.row[k], nr = b.row[k + 1] - r0;
+            CUDA_TRY(s, cudaStreamWaitEvent(s->cvout, ev, 0));
+            CUDA_TRY(s, state_to_rows(s, q.out, r0, nr, s->cvout));
+            CUDA_TRY(s, cudaEventRecord(s->ev_dc[k], s->cvout));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_dc[k], 0));
+            return download_rows(s, io, k, U_out, r0 * row_elems, row_elems * nr);
+        }
+        return HYPE_OK;
+    };
     CUDA_TRY(s, launch_begin_step(s->dSc, s->stream));
     CUDA_TRY(s, cudaEventRecord(s->ev_fence, s->stream));   // the other compute streams start behind begin_step
     for (int j = 1; j < 4; ++j) CUDA_TRY(s, cudaStreamWaitEvent(on_stage[j], s->ev_fence, 0));
-    if (U_in)
-        for (int k = 0; k < b.n; ++k)
-            if ((rc = upload_band(s, b, k, U_in, plan[0].in))) return rc;
-    for (int st = 0; st < ns; ++st) {
-        const PlanStage &q = plan[st];
-        cudaStream_t on = on_stage[st % 4];
-        for (int i = 0; i < b.n; ++i) {
-            const int k = b.order[i];
-            int nb[3], m = 0;   // bands whose rows band k's stencils read
-            nb[m++] = k;
-            if (k > 0) nb[m++] = k - 1; else if (py) nb[m++] = b.n - 1;
-            if (k + 1 < b.n) nb[m++] = k + 1; else if (py) nb[m++] = 0;
-            for (int j = 0; j < m; ++j) {
-                if (st == 0 && U_in) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_in[nb[j]], 0));
-                if (st > 0) CUDA_TRY(s, cudaStreamWaitEvent(on, s->ev_sb[(st - 1) * hype_solver::MAX_BANDS + nb[j]], 0));
-            }
-            CUDA_TRY(s, stage_band(s, b, k, q, 0, nullptr, on));
-            cudaEvent_t done = s->ev_sb[st * hype_solver::MAX_BANDS + k];
-            CUDA_TRY(s, cudaEventRecord(done, on));
-            if (st == ns - 1 && U_out) {   // band k of the result: to the host while later bands compute
-                const int r0 = b.row[k], nr = b.row[k + 1] - r0;
-                CUDA_TRY(s, cudaStreamWaitEvent(s->cvout, done, 0));
-                CUDA_TRY(s, state_to_rows(s, q.out, r0, nr, s->cvout));
-                CUDA_TRY(s, cudaEventRecord(s->ev_dc[k], s->cvout));
-                CUDA_TRY(s, cudaStreamWaitEvent(s->cout, s->ev_dc[k], 0));
-                CUDA_TRY(s, cudaMemcpyAsync(U_out + r0 * row_elems, s->dAosOut + r0 * row_elems, sizeof(double) * row_elems * nr,
-                                            cudaMemcpyDeviceToHost, s->cout));
-            }
+    for (int u = 0;; ++u) {
+        if (u < b.n && U_in) {
+            if ((rc = upload_band(s, b, u, U_in, plan[0].in, io))) return rc;
+            uploaded = u + 1;
         }
+        for (int st = 0; st < ns; ++st)
+            while (next[st] < b.n && ready(st, b.order[next[st]])) {
+                if ((rc = launch(st, b.order[next[st]]))) return rc;
+                ++next[st];
+            }
+        if (uploaded >= b.n) break;
     }
+    for (int st = 0; st < ns; ++st)
+        if (next[st] < b.n) return fail(s, HYPE_ERR_CUDA, "banded step: stage %d band %d never became ready", st, b.order[next[st]]);
     for (int k = 0; k < b.n; ++k)   // end_step and everything after it behind every compute stream
         for (int st = ns - 4 > 0 ? ns - 4 : 0; st < ns; ++st)
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_sb[st * hype_solver::MAX_BANDS + k], 0));
@@ -1105,12 +1197,13 @@ int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nst
     if ((rc = ensure_step_graph(s))) return rc;
     const Bands b = host_bands(s);
     if ((rc = fence_copy_streams(s))) return rc;
+    HostIO io = host_io(s, U_in, U_out);
     CUDA_TRY(s, cudaEventRecord(s->ev0, s->stream));
-    if ((rc = enqueue_step_banded(s, b, U_in, nsteps == 1 ? U_out : nullptr))) return rc;
+    if ((rc = enqueue_step_banded(s, b, U_in, nsteps == 1 ? U_out : nullptr, io))) return rc;
     for (int k = 1; k + 1 < nsteps; ++k) CUDA_TRY(s, cudaGraphLaunch(s->step_exec, s->stream));
-    if (nsteps > 1 && (rc = enqueue_step_banded(s, b, nullptr, U_out))) return rc;
+    if (nsteps > 1 && (rc = enqueue_step_banded(s, b, nullptr, U_out, io))) return rc;
     CUDA_TRY(s, cudaEventRecord(s->ev1, s->stream));
-    CUDA_TRY(s, cudaStreamSynchronize(s->cout));
+    if ((rc = finish_downloads(s, io, U_out))) return rc;
     return hype_wait(s, steps_done, t_end, dt_next);
 }
 

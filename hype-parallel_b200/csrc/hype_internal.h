@@ -234,6 +234,12 @@ cudaError_t launch_mixsys(int sys, int cells, const MixedMaps &maps, const Mixed
 cudaError_t launch_mixsys_batch(int sys, int cells, const MixedParams *inst, const MixedMaps *maps, const int2 *work, int *sched,
                                 int blocks, cudaStream_t s);
 // layout changes between the interleaved FP64 Vec and the mixed planes of system sys
+// hype_hostcopy.cu: host copies split over a small thread pool (between a caller's
+// pageable arrays and pinned staging), and whether a host pointer is pageable
+void host_copy(void *dst, const void *src, size_t bytes);
+void host_copy_2d(void *dst, size_t dpitch, const void *src, size_t spitch, size_t width, size_t rows);
+bool host_is_pageable(const void *p);
+
 cudaError_t launch_aos_to_mixed(int sys, const double *aos, float *pf, double *pd, int nx, int ny, int pitch, long long plane,
                                 cudaStream_t s);
 cudaError_t launch_mixed_to_aos(int sys, const float *pf, const double *pd, double *aos, int nx, int ny, int pitch, long long plane,

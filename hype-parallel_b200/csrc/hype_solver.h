@@ -28,6 +28,11 @@ struct hype_solver {
     cudaEvent_t ev_in[MAX_BANDS] = {};              //               converted to planes
     cudaEvent_t ev_dc[MAX_BANDS] = {};              //               result converted for the copy out
     cudaEvent_t ev_done[MAX_BANDS] = {};            //               computed
+    cudaEvent_t ev_dl[MAX_BANDS] = {};              //               copied into the host staging
+    // pinned host staging of the banded calls for pageable caller arrays (allocated on
+    // first use, aos_bytes each)
+    double *hStageIn = nullptr, *hStageOut = nullptr;
+    size_t aos_bytes = 0;
     cudaEvent_t ev_fence = nullptr;                 // the compute stream's work so far
     // banded steps: stage s on compute stream s % 4 (stream, stream2, stream3, stream4),
     // band k of stage s marked by ev_sb[s * MAX_BANDS + k]

@@ -129,7 +129,12 @@ HYPE_API const char *hype_last_error(const hype_solver *s);
  * the reference leaves in Ctx->dt (rhs_function_prim.c:620-623).  U and RHS are
  * host arrays in the Vec layout above.  t is accepted for the TS signature (the
  * inlet profile is time independent).  Thread-compatible, not reentrant on one
- * solver (as the reference, which shares AppCtx scratch).
+ * solver (as the reference, which shares AppCtx scratch).  The copies overlap the
+ * launch, band of rows by band of rows.  Pinned (page-locked) U and RHS go to the
+ * copy engines directly; pageable ones (PETSc's Vec arrays) are staged through
+ * two pinned buffers of the state's size that the solver allocates on first use
+ * (direct copies if that allocation fails).  The same holds for
+ * hype_rhs_prim_slab and hype_advance_host.
  */
 HYPE_API int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double *dt);
 
@@ -258,7 +263,8 @@ HYPE_API int hype_wait(hype_solver *s, int *steps_done, double *t_end, double *d
  * and the rows of U_out stream out while the last step finishes the rows after
  * them.  Needs hype_begin.  U_in
  * and U_out may be the same array; pinned (page-locked) host memory gives the
- * overlap its full effect.  Returns what hype_wait returns.
+ * overlap its full effect (pageable arrays: see hype_rhs_prim).  Returns what
+ * hype_wait returns.
  */
 HYPE_API int hype_advance_host(hype_solver *s, const double *U_in, double *U_out, int nsteps, int *steps_done, double *t_end,
                                double *dt_next);

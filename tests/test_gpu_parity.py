@@ -349,3 +349,42 @@ def test_full_size_conservation_periodic(hp):
         assert abs(tot1[c] - tot0[c]) <= 1e-12 * scale[c], (c, tot0[c], tot1[c])
     assert 0.0 <= amin1 and amax1 <= 1.0, (amin1, amax1)
     assert amin1 > 0.5e-6 and amax1 < 1 - 1e-9, (amin1, amax1)   # pure phases stay distinct
+
+
+def test_host_calls_pinned_and_pageable_agree(hp):
+    """Pageable caller arrays go through pinned staging (copied by the host copy pool),
+    pinned ones straight to the copy engines: hype_advance_host (1 and 3 steps, input
+    and output the same array too) and hype_rhs_prim give the same bits either way,
+    and the same as the unbanded device path."""
+    import torch
+    P, T = hp.BC_PERIODIC, hp.BC_TRANSMISSIVE
+    c = hp.Config(system=hp.KAPILA_5EQN, order=2, nx=900, ny=1100, cfl=0.4, bc_left=T, bc_right=T, bc_bottom=P, bc_top=P)
+    U = hp.initial_state(c, "shock_bubble", seed=44, nbubbles=3)
+    for nsteps in (1, 3):
+        with hp.Solver(c) as s:
+            s.set_state(U)
+            s.begin(0.0, 1e30, 100)
+            s.advance(nsteps)
+            ref = (s.wait(), s.get_state())
+        outs = []
+        for pinned, alias in ((False, False), (True, False), (False, True), (True, True)):
+            src = torch.from_numpy(U.copy()).pin_memory().numpy() if pinned else U.copy()
+            dst = src if alias else (torch.empty(U.shape, dtype=torch.float64).pin_memory().numpy() if pinned else np.empty_like(U))
+            with hp.Solver(c) as s:
+                s.set_state(U)
+                s.begin(0.0, 1e30, 100)
+                got = s.advance_host(src, dst, nsteps)
+            assert got[:3] == ref[0][:3], (pinned, alias)
+            outs.append(dst.tobytes())
+        assert all(o == ref[1].tobytes() for o in outs)
+    with hp.Solver(c) as s:
+        Rp, dtp, _ = s.rhs_function_prim(0.0, U)
+        Up = torch.from_numpy(U.copy()).pin_memory().numpy()
+        Rpin = torch.empty(U.shape, dtype=torch.float64).pin_memory().numpy()
+        _, dtq, _ = s.rhs_function_prim(0.0, Up, Rpin)
+        dU = torch.from_numpy(U).cuda()
+        dR = torch.empty_like(dU)
+        torch.cuda.synchronize()
+        dtd, _ = s.rhs_function_prim_device(0.0, dU.data_ptr(), dR.data_ptr())
+    assert dtp == dtq == dtd
+    assert Rp.tobytes() == Rpin.tobytes() == dR.cpu().numpy().tobytes()
