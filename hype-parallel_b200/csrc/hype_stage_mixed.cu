@@ -193,6 +193,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
     const bool touches_x = (x0 == 0) || (x1 >= p.nx);
     const int bcL = p.bc[0], bcR = p.bc[1], bcB = p.bc[2], bcT = p.bc[3];
     const double dt = (p.mode == OUT_RHS) ? 0.0 : p.sc->dt;
+    const double b = dt / p.kb;
     const MixedEos e(p.eos);
     const double r1_h = p.r1_h;
 
@@ -324,7 +325,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         if (active) {
 #pragma unroll 1
             for (int kv = 0; kv < 3; ++kv) {
-                const int c = 3 * h + kv;
+                const int c = kv < 2 ? 2 * h + kv : 4 + h;   // half 0: rho1 rho2 p, half 1: u v a1 (no FP32/FP64 split in a pass)
                 float d[12];
                 if (c < 4) {
                     const int o = c * BW + ccm;
@@ -379,7 +380,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         if (!ok && active) {   // rhs_function_prim.c:407-421 in deviation form
 #pragma unroll 1
             for (int kv = 0; kv < 3; ++kv) {
-                const int c = 3 * h + kv;
+                const int c = kv < 2 ? 2 * h + kv : 4 + h;   // half 0: rho1 rho2 p, half 1: u v a1 (no FP32/FP64 split in a pass)
                 float dxp, dxm, dyp, dym;
                 if (c < 4) {
                     const int o = c * BW + ccm;
@@ -426,11 +427,11 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 if (r > y0) {
                     const int jo = r - 1;
                     const size_t gidx = (size_t)jo * p.pitch + i;
-                    const double b = dt / p.kb;
+                    // the halves take alternate variables, c = 2 j + h, so every lane works in every pass
 #pragma unroll
-                    for (int c = 0; c < NV; ++c) {
-                        if ((c & 1) != h) continue;
-                        double Y = G[c] - carry[(6 + c) * CELLS + m];
+                    for (int j = 0; j < 3; ++j) {
+                        const int c = 2 * j + h;
+                        double Y = (h ? G[2 * j + 1] : G[2 * j]) - carry[(6 + c) * CELLS + m];
                         if (c == 5) Y += 0.5 * (E5 + carry[12 * CELLS + m]);
                         const double rhs = (c == 5 ? carry[13 * CELLS + m] : 0.0) + (carry[c * CELLS + m] - r1_h * Y);
                         if (p.mode == OUT_RHS) {
@@ -463,8 +464,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                     }
                 }
 #pragma unroll
-                for (int c = 0; c < NV; ++c)
-                    if ((c & 1) == h) carry[(6 + c) * CELLS + m] = G[c];
+                for (int j = 0; j < 3; ++j) carry[(6 + 2 * j + h) * CELLS + m] = h ? G[2 * j + 1] : G[2 * j];
                 if (h == 1) carry[12 * CELLS + m] = E5;
             }
         }
@@ -526,16 +526,15 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
         __syncthreads();   // S3
         if (xface && full_row) {
 #pragma unroll
-            for (int c = 0; c < NV; ++c)
-                if ((c & 1) == h) exch[c * CELLS + m] = Fx[c];
+            for (int j = 0; j < 3; ++j) exch[(2 * j + h) * CELLS + m] = h ? Fx[2 * j + 1] : Fx[2 * j];
             if (h == 1) exch[6 * CELLS + m] = Dx5;
         }
         __syncthreads();   // S4
         if (owned && full_row) {
 #pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if ((c & 1) != h) continue;
-                double X = exch[c * CELLS + m + 1] - Fx[c];
+            for (int j = 0; j < 3; ++j) {
+                const int c = 2 * j + h;
+                double X = exch[c * CELLS + m + 1] - (h ? Fx[2 * j + 1] : Fx[2 * j]);
                 if (c == 5) X += 0.5 * (exch[6 * CELLS + m + 1] + Dx5);
                 carry[c * CELLS + m] = -r1_h * X;
             }

@@ -304,6 +304,7 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
     const bool touches_x = (x0 == 0) || (x1 >= p.nx);
     const int bcL = p.bc[0], bcR = p.bc[1], bcB = p.bc[2], bcT = p.bc[3];
     const double dt = (p.mode == OUT_RHS) ? 0.0 : p.sc->dt;
+    const double b = dt / p.kb;
     const MixEos e(p.eos);
     const double r1_h = p.r1_h;
 
@@ -534,20 +535,16 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
                 if (r > y0) {
                     const int jo = r - 1;
                     const size_t gidx = (size_t)jo * p.pitch + i;
-                    const double b = dt / p.kb;
-                    static_for<NV>([&](auto cc_) {
-                        constexpr int c = decltype(cc_)::value;
-                        if ((c & 1) != h) return;
-                        double Y = G[c] - gbelow[c * CELLS + m];
-                        constexpr int jn = ncp_slot<M>(c);
-                        if constexpr (jn >= 0) Y += 0.5 * (E[jn] + ebelow[jn * CELLS + m]);
+                    // one variable of row r-1: c, its plane kind and slot, its non-conservative slot jn
+                    auto finish_one = [&](int c, auto dcomp_, auto ncp_, int sl, int jn, double Gc, double Ec) {
+                        constexpr bool dcomp = decltype(dcomp_)::value != 0, has_ncp = decltype(ncp_)::value != 0;
+                        double Y = Gc - gbelow[c * CELLS + m];
+                        if constexpr (has_ncp) Y += 0.5 * (Ec + ebelow[jn * CELLS + m]);
                         const double rhs = pre[c * CELLS + m] - r1_h * Y;
                         if (p.mode == OUT_RHS) {
                             p.out_rhs[((size_t)jo * p.nx + i) * NV + c] = rhs;
                             return;
                         }
-                        constexpr bool dcomp = is_d<M>(c);
-                        constexpr int sl = slot_of_comp<M>(c);
                         const double Sv = dcomp ? orowd[sl * BW + ccm] : (double)orowf[sl * BW + ccm];
                         double o;
                         if (p.mode == OUT_AXPY) {
@@ -570,14 +567,35 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
                                 else p.push_hi_f[sl * p.push_plane_hi + at] = (float)o;
                             }
                         }
+                    };
+                    // the halves take variables 2 j and 2 j + 1 of pair j: one code path when
+                    // the two are of one kind (plane type, non-conservative term), so that
+                    // every lane works in the same pass
+                    static_for<(NV + 1) / 2>([&](auto jj_) {
+                        constexpr int c0 = 2 * decltype(jj_)::value, c1 = c0 + 1;
+                        constexpr bool two = c1 < NV;
+                        constexpr bool d0 = is_d<M>(c0), d1 = is_d<M>(c1);
+                        constexpr int n0 = ncp_slot<M>(c0), n1 = two ? ncp_slot<M>(c1) : -1;
+                        constexpr int s0 = slot_of_comp<M>(c0), s1 = slot_of_comp<M>(c1);
+                        constexpr int e0 = n0 >= 0 ? n0 : 0, e1 = n1 >= 0 ? n1 : 0;
+                        constexpr int g1 = two ? c1 : c0;
+                        if constexpr (two && d0 == d1 && ((n0 >= 0) == (n1 >= 0))) {
+                            finish_one(h ? c1 : c0, ic<d0 ? 1 : 0>{}, ic<(n0 >= 0) ? 1 : 0>{}, h ? s1 : s0, h ? n1 : n0,
+                                       h ? G[g1] : G[c0], h ? E[e1] : E[e0]);
+                        } else {
+                            if (h == 0) finish_one(c0, ic<d0 ? 1 : 0>{}, ic<(n0 >= 0) ? 1 : 0>{}, s0, n0, G[c0], E[e0]);
+                            else if (two) finish_one(c1, ic<d1 ? 1 : 0>{}, ic<(n1 >= 0) ? 1 : 0>{}, s1, n1, G[g1], E[e1]);
+                        }
                     });
                 }
-                static_for<NV>([&](auto cc_) {
-                    constexpr int c = decltype(cc_)::value;
-                    if ((c & 1) != h) return;
-                    gbelow[c * CELLS + m] = G[c];
-                    constexpr int jn = ncp_slot<M>(c);
-                    if constexpr (jn >= 0) ebelow[jn * CELLS + m] = E[jn];
+                static_for<(NV + 1) / 2>([&](auto jj_) {
+                    constexpr int c0 = 2 * decltype(jj_)::value, c1 = c0 + 1;
+                    constexpr bool two = c1 < NV;
+                    constexpr int g1 = two ? c1 : c0;
+                    constexpr int n0 = ncp_slot<M>(c0), n1 = two ? ncp_slot<M>(c1) : -1;
+                    if (h == 0 || two) gbelow[(h ? g1 : c0) * CELLS + m] = h ? G[g1] : G[c0];
+                    if constexpr (n0 >= 0) if (h == 0) ebelow[n0 * CELLS + m] = E[n0];
+                    if constexpr (n1 >= 0) if (h == 1) ebelow[n1 * CELLS + m] = E[n1];
                 });
             }
         }
@@ -647,12 +665,14 @@ __device__ __forceinline__ void mixsys_tile(const MixedParams &p, const MixedMap
         }
         __syncthreads();   // S3
         if (xface && full_row) {
-            static_for<NV>([&](auto cc_) {
-                constexpr int c = decltype(cc_)::value;
-                if ((c & 1) != h) return;
-                exch[c * CELLS + m] = Fx[c];
-                constexpr int jn = ncp_slot<M>(c);
-                if constexpr (jn >= 0) exch[(NV + jn) * CELLS + m] = Dx[jn];
+            static_for<(NV + 1) / 2>([&](auto jj_) {
+                constexpr int c0 = 2 * decltype(jj_)::value, c1 = c0 + 1;
+                constexpr bool two = c1 < NV;
+                constexpr int g1 = two ? c1 : c0;
+                constexpr int n0 = ncp_slot<M>(c0), n1 = two ? ncp_slot<M>(c1) : -1;
+                if (h == 0 || two) exch[(h ? g1 : c0) * CELLS + m] = h ? Fx[g1] : Fx[c0];
+                if constexpr (n0 >= 0) if (h == 0) exch[(NV + n0) * CELLS + m] = Dx[n0];
+                if constexpr (n1 >= 0) if (h == 1) exch[(NV + n1) * CELLS + m] = Dx[n1];
             });
         }
         __syncthreads();   // S4

@@ -537,10 +537,14 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     // row r-1: rhs = ncp + ((-1/h) X - (1/h) Y)  (rhs_function_prim.c:589-602), then the RK combination
                     const int jo = r - 1;
                     const size_t gidx = (size_t)jo * p.pitch + i;
+                    // the halves take alternate variables, c = 2 j + h, so every lane works in every pass
 #pragma unroll
-                    for (int c = 0; c < NV; ++c) {
-                        if ((c & 1) != h) continue;
-                        const double Y = G[c] - carry(2, c) + 0.5 * (E[c] + carry(3, c));
+                    for (int j = 0; j < (NV + 1) / 2; ++j) {
+                        if (2 * j + 1 >= NV && h) continue;   // odd NV: the last variable is half 0's alone
+                        const int c = 2 * j + h;
+                        const double Gc = h ? G[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : G[2 * j];
+                        const double Ec = h ? E[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : E[2 * j];
+                        const double Y = Gc - carry(2, c) + 0.5 * (Ec + carry(3, c));
                         const double ty = r1_h * Y;
                         const double rhs = carry(0, c) + (carry(1, c) - ty);
                         if (p.mode == OUT_RHS) {
@@ -577,10 +581,11 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                     }
                 }
 #pragma unroll
-                for (int c = 0; c < NV; ++c) {
-                    if ((c & 1) != h) continue;
-                    carry(2, c) = G[c];
-                    carry(3, c) = E[c];
+                for (int j = 0; j < (NV + 1) / 2; ++j) {
+                    if (2 * j + 1 >= NV && h) continue;
+                    const int c = 2 * j + h;
+                    carry(2, c) = h ? G[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : G[2 * j];
+                    carry(3, c) = h ? E[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : E[2 * j];
                 }
             }
         }
@@ -745,19 +750,23 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
         __syncthreads();   // S3: coefficient reads done; the buffer now carries face fluxes
         if (xface && full_row) {
 #pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if ((c & 1) != h) continue;
-                coef_s[c * CELLS + m] = Fx[c];
-                coef_s[(NV + c) * CELLS + m] = Dx[c];
+            for (int j = 0; j < (NV + 1) / 2; ++j) {
+                if (2 * j + 1 >= NV && h) continue;
+                const int c = 2 * j + h;
+                coef_s[c * CELLS + m] = h ? Fx[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : Fx[2 * j];
+                coef_s[(NV + c) * CELLS + m] = h ? Dx[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : Dx[2 * j];
             }
         }
         __syncthreads();   // S4
         if (owned && full_row) {
 #pragma unroll
-            for (int c = 0; c < NV; ++c) {
-                if ((c & 1) != h) continue;
+            for (int j = 0; j < (NV + 1) / 2; ++j) {
+                if (2 * j + 1 >= NV && h) continue;
+                const int c = 2 * j + h;
+                const double Fc = h ? Fx[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : Fx[2 * j];
+                const double Dc = h ? Dx[2 * j + 1 < NV ? 2 * j + 1 : 2 * j] : Dx[2 * j];
                 const double F1 = coef_s[c * CELLS + m + 1], D1 = coef_s[(NV + c) * CELLS + m + 1];
-                const double X = F1 - Fx[c] + 0.5 * (D1 + Dx[c]);
+                const double X = F1 - Fc + 0.5 * (D1 + Dc);
                 carry(1, c) = -r1_h * X;
             }
         }
