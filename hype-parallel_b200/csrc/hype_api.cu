@@ -1023,13 +1023,63 @@ int hype_rhs_prim_device(hype_solver *s, double t, const double *dU, double *dRH
     return rhs_common(s, dRHS, dt);
 }
 
+// A whole cell-major array from the caller into dAosIn, or from dAosOut to the caller,
+// on the solver's stream.  Pageable arrays go through the pinned staging in up to
+// MAX_BANDS chunks, so that the host copy of one chunk overlaps the DMA of another.
+static size_t whole_chunk(size_t bytes)
+{
+    const size_t c = (bytes + hype_solver::MAX_BANDS - 1) / hype_solver::MAX_BANDS;
+    return c < ((size_t)1 << 20) ? ((size_t)1 << 20) : c;
+}
+
+static int copy_in_whole(hype_solver *s, const double *U, size_t bytes)
+{
+    const HostIO io = host_io(s, U, nullptr);
+    if (!io.stage_in) {
+        CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, bytes, cudaMemcpyHostToDevice, s->stream));
+        return HYPE_OK;
+    }
+    const size_t chunk = whole_chunk(bytes);
+    for (size_t off = 0; off < bytes; off += chunk) {
+        const size_t n = bytes - off < chunk ? bytes - off : chunk;
+        host_copy((char *)s->hStageIn + off, (const char *)U + off, n);
+        CUDA_TRY(s, cudaMemcpyAsync((char *)s->dAosIn + off, (char *)s->hStageIn + off, n, cudaMemcpyHostToDevice, s->stream));
+    }
+    return HYPE_OK;
+}
+
+static int copy_out_whole(hype_solver *s, double *U, size_t bytes)
+{
+    const HostIO io = host_io(s, nullptr, U);
+    if (!io.stage_out) {
+        CUDA_TRY(s, cudaMemcpyAsync(U, s->dAosOut, bytes, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+        return HYPE_OK;
+    }
+    const size_t chunk = whole_chunk(bytes);
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += chunk, ++k) {
+        const size_t n = bytes - off < chunk ? bytes - off : chunk;
+        CUDA_TRY(s, cudaMemcpyAsync((char *)s->hStageOut + off, (char *)s->dAosOut + off, n, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, cudaEventRecord(s->ev_dl[k], s->stream));
+    }
+    k = 0;
+    for (size_t off = 0; off < bytes; off += chunk, ++k) {
+        const size_t n = bytes - off < chunk ? bytes - off : chunk;
+        CUDA_TRY(s, cudaEventSynchronize(s->ev_dl[k]));
+        host_copy((char *)U + off, (const char *)s->hStageOut + off, n);
+    }
+    return HYPE_OK;
+}
+
 int hype_set_state(hype_solver *s, const double *U)
 {
     if (!s || !U) return fail(s, HYPE_ERR_INVALID, "null argument");
     if (s->row_off) return fail(s, HYPE_ERR_INVALID, "a slab solver has no time loop of its own (hype_group runs slabs)");
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
-    CUDA_TRY(s, cudaMemcpyAsync(s->dAosIn, U, aos_bytes, cudaMemcpyHostToDevice, s->stream));
+    int rc;
+    if ((rc = copy_in_whole(s, U, aos_bytes))) return rc;
     CUDA_TRY(s, load_state(s, s->dAosIn, 0));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return HYPE_OK;
@@ -1041,9 +1091,7 @@ int hype_get_state(hype_solver *s, double *U)
     CUDA_TRY(s, cudaSetDevice(s->cfg.device));
     const size_t aos_bytes = sizeof(double) * (size_t)s->cfg.nx * s->cfg.ny * s->nv;
     CUDA_TRY(s, store_state(s, 0, s->dAosOut));
-    CUDA_TRY(s, cudaMemcpyAsync(U, s->dAosOut, aos_bytes, cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    return HYPE_OK;
+    return copy_out_whole(s, U, aos_bytes);
 }
 
 // One SSP-RK step (begin_step, the stages, end_step) captured once as a CUDA

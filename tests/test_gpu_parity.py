@@ -388,3 +388,12 @@ def test_host_calls_pinned_and_pageable_agree(hp):
         dtd, _ = s.rhs_function_prim_device(0.0, dU.data_ptr(), dR.data_ptr())
     assert dtp == dtq == dtd
     assert Rp.tobytes() == Rpin.tobytes() == dR.cpu().numpy().tobytes()
+    # whole-state copies (set_state / get_state), staged in chunks from pageable arrays
+    with hp.Solver(c) as s:
+        Upin = torch.from_numpy(U.copy()).pin_memory().numpy()
+        Gpin = torch.empty(U.shape, dtype=torch.float64).pin_memory().numpy()
+        s.set_state(Upin)
+        s.get_state(Gpin)
+        s.set_state(U)
+        Gpage = s.get_state()
+    assert Gpin.tobytes() == U.tobytes() and Gpage.tobytes() == U.tobytes()
