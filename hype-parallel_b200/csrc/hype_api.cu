@@ -508,12 +508,15 @@ static HostIO host_io(hype_solver *s, const void *in, const void *out)
     HostIO io;
     const bool want_in = in && host_is_pageable(in), want_out = out && host_is_pageable(out);
     if ((want_in || want_out) && !s->hStageIn) {   // first use; without pinned memory the copies stay direct
-        if (cudaHostAlloc(&s->hStageIn, s->aos_bytes, cudaHostAllocDefault) != cudaSuccess ||
-            cudaHostAlloc(&s->hStageOut, s->aos_bytes, cudaHostAllocDefault) != cudaSuccess) {
-            cudaGetLastError();
-            if (s->hStageIn) cudaFreeHost(s->hStageIn);
-            s->hStageIn = nullptr;
-            s->hStageOut = nullptr;
+        void *a = nullptr, *o = nullptr;
+        const bool ok_a = cudaHostAlloc(&a, s->aos_bytes, cudaHostAllocDefault) == cudaSuccess;
+        const bool ok_o = ok_a && cudaHostAlloc(&o, s->aos_bytes, cudaHostAllocDefault) == cudaSuccess;
+        if (ok_a && ok_o) {
+            s->hStageIn = (double *)a;
+            s->hStageOut = (double *)o;
+        } else {
+            cudaGetLastError();   // the failed allocation's error is not the call's
+            if (ok_a) cudaFreeHost(a);
         }
     }
     io.stage_in = want_in && s->hStageIn;
