@@ -34,7 +34,11 @@ struct MixedKernel {
     static constexpr int F_REGION = (F_ROW_BYTES + 127) / 128 * 128;
     static constexpr int D_REGION = (D_ROW_BYTES + 127) / 128 * 128;
     static constexpr int SLOT_BYTES = F_REGION + D_REGION;
-    static constexpr int COEF_FLOATS = 5 * NV * CELLS;   // [k-1][c][cell]; later 7 FP64 flux values per cell
+    // reconstruction coefficients: k = 1..4 as one float4 per (cell, variable), cells 7
+    // float4 apart (quarter-warp float4 loads fall on disjoint banks), then k = 5 as
+    // [c][cell]; later 7 FP64 flux values per cell
+    static constexpr int CV_STRIDE = 7;
+    static constexpr int COEF_FLOATS = 4 * CV_STRIDE * CELLS + NV * CELLS;
     static constexpr int YTF_FLOATS = 2 * 4 * CELLS;     // top-face rho1 rho2 u v, by Gauss point
     static constexpr int YTD_DOUBLES = 2 * 2 * CELLS;    // top-face p, a1
     static constexpr int CARRY_DOUBLES = 14 * CELLS;     // t1[6], G below[6], E5 below, ncp5
@@ -209,7 +213,18 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
     auto slot_of = [&](int row) { return (row - row_lo) % SLOTS; };
     auto rowf = [&](int row) { return reinterpret_cast<float *>(rows + (size_t)slot_of(row) * K::SLOT_BYTES); };
     auto rowd = [&](int row) { return reinterpret_cast<double *>(rows + (size_t)slot_of(row) * K::SLOT_BYTES + K::F_REGION); };
-    auto cf_at = [&](int k1, int c, int cell) -> float & { return coef_f[(k1 * NV + c) * CELLS + cell]; };
+    float4 *coef_v = reinterpret_cast<float4 *>(coef_f);                   // [cell][c] k = 1..4
+    float *coef_5 = coef_f + 4 * K::CV_STRIDE * CELLS;                      // [c][cell] k = 5
+    auto cf_store = [&](int c, int cell, const float *cf) {
+        coef_v[cell * K::CV_STRIDE + c] = make_float4(cf[0], cf[1], cf[2], cf[3]);
+        coef_5[c * CELLS + cell] = cf[4];
+    };
+    // the five coefficients of (cell, c) as an accessor for pair_poly (k1 = 0..4)
+    auto cf_of = [&](int c, int cell) {
+        const float4 v = coef_v[cell * K::CV_STRIDE + c];
+        const float *p5 = &coef_5[c * CELLS + cell];
+        return [v, p5](int k1) -> float { return k1 == 0 ? v.x : k1 == 1 ? v.y : k1 == 2 ? v.z : k1 == 3 ? v.w : *p5; };
+    };
 
     float smax_loc = 0.0f;
     bool bad = false;
@@ -343,7 +358,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 float cf[5];
                 weno3_f(d, cf);
 #pragma unroll
-                for (int k = 0; k < 5; ++k) cf_at(k, c, m) = cf[k];
+                cf_store(c, m, cf);
             }
         }
         __syncwarp();
@@ -353,7 +368,7 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
             using B1 = decltype(b1);
             float pv[NV];
 #pragma unroll
-            for (int c = 0; c < NV; ++c) pv[c] = pair_poly<B0, B1>([&](int k1) { return cf_at(k1, c, cell); }, h);
+            for (int c = 0; c < NV; ++c) pv[c] = pair_poly<B0, B1>(cf_of(c, cell), h);
             PrimM V;
             V.r1 = center(0, cell) + pv[0];
             V.r2 = center(1, cell) + pv[1];
@@ -391,9 +406,8 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                     const double w0 = d_0[o];
                     dxp = (float)(d_0[o + 1] - w0); dxm = (float)(w0 - d_0[o - 1]); dyp = (float)(d_p1[o] - w0); dym = (float)(w0 - d_m1[o]);
                 }
-                cf_at(0, c, m) = minmod_f(dxp, dxm);
-                cf_at(1, c, m) = minmod_f(dyp, dym);
-                cf_at(2, c, m) = 0.0f; cf_at(3, c, m) = 0.0f; cf_at(4, c, m) = 0.0f;
+                const float cf[5] = {minmod_f(dxp, dxm), minmod_f(dyp, dym), 0.0f, 0.0f, 0.0f};
+                cf_store(c, m, cf);
             }
         }
         __syncwarp();
@@ -488,10 +502,11 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                     using GX1 = DPhiVolX<2, qb>;
                     using GY0 = DPhiVolY<2, qa>;
                     using GY1 = DPhiVolY<2, qb>;
-                    float ux = pair_poly<GX0, GX1>([&](int k1) { return cf_at(k1, 2, m); }, h);
-                    float vy = pair_poly<GY0, GY1>([&](int k1) { return cf_at(k1, 3, m); }, h);
-                    float ax = pair_poly<GX0, GX1>([&](int k1) { return cf_at(k1, 5, m); }, h);
-                    float ay = pair_poly<GY0, GY1>([&](int k1) { return cf_at(k1, 5, m); }, h);
+                    const auto c2 = cf_of(2, m), c3 = cf_of(3, m), c5 = cf_of(5, m);
+                    float ux = pair_poly<GX0, GX1>(c2, h);
+                    float vy = pair_poly<GY0, GY1>(c3, h);
+                    float ax = pair_poly<GX0, GX1>(c5, h);
+                    float ay = pair_poly<GY0, GY1>(c5, h);
                     const float r1hf = (float)r1_h;
                     ux *= r1hf; vy *= r1hf; ax *= r1hf; ay *= r1hf;
                     const float K = kapila_K(e, V.r1, V.r2, V.p, V.a);
