@@ -10,32 +10,46 @@ namespace hype {
 
 __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
-// One direction of WENO3 (reconstruction.c:157-178) on deviations from the
-// cell value, weights gamma_k / (IS_k + eps)^4 scaled by min_k (IS_k + eps)^4.
-__device__ __forceinline__ void weno3_1d_f(float dm2, float dm1, float dp1, float dp2, float &slope, float &curv)
+// One direction of WENO3 (reconstruction.c:157-178) on deviations from the cell
+// value, weights gamma_k / (IS_k + eps)^4 scaled by min_k (IS_k + eps)^4: slope and
+// curvature from the deviations at -2, -1, +1, +2.  The x and the y direction run at
+// once as the two lanes of packed FP32 operations (sm_100 f32x2: lane .x the x
+// direction, lane .y the y direction), half the FP32 instructions of two scalar
+// passes; minima and the fast reciprocals stay per lane.
+__device__ __forceinline__ void weno3_xy_f2(float2 dm2, float2 dm1, float2 dp1, float2 dp2, float2 &slope, float2 &curv)
 {
-    const float ux0 = -2.0f * dm1 + 0.5f * dm2, uxx0 = 0.5f * (dm2 - 2.0f * dm1);
-    const float ux1 = 0.5f * (dp1 - dm1), uxx1 = 0.5f * (dm1 + dp1);
-    const float ux2 = 2.0f * dp1 - 0.5f * dp2, uxx2 = 0.5f * (dp2 - 2.0f * dp1);
-    const float r13 = 13.0f / 3.0f, eps = 1.0e-12f;
-    const float a0 = ux0 * ux0 + r13 * uxx0 * uxx0 + eps;
-    const float a1 = ux1 * ux1 + r13 * uxx1 * uxx1 + eps;
-    const float a2 = ux2 * ux2 + r13 * uxx2 * uxx2 + eps;
-    const float mn = fminf(a0, fminf(a1, a2));
-    float q0 = fdiv(mn, a0), q1 = fdiv(mn, a1), q2 = fdiv(mn, a2);
-    q0 *= q0; q1 *= q1; q2 *= q2;
-    const float w0 = q0 * q0, w1 = 100.0f * (q1 * q1), w2 = q2 * q2;
-    const float inv = fdiv(1.0f, w0 + w1 + w2);
-    slope = (w0 * ux0 + w1 * ux1 + w2 * ux2) * inv;
-    curv = (w0 * uxx0 + w1 * uxx1 + w2 * uxx2) * inv;
+    const float2 k2 = make_float2(2.0f, 2.0f), km2 = make_float2(-2.0f, -2.0f), kh = make_float2(0.5f, 0.5f);
+    const float2 kmh = make_float2(-0.5f, -0.5f), k13 = make_float2(13.0f / 3.0f, 13.0f / 3.0f);
+    const float2 keps = make_float2(1.0e-12f, 1.0e-12f), k100 = make_float2(100.0f, 100.0f);
+    const float2 ux0 = __ffma2_rn(km2, dm1, __fmul2_rn(kh, dm2));
+    const float2 uxx0 = __fmul2_rn(kh, __ffma2_rn(km2, dm1, dm2));
+    const float2 ux1 = __fmul2_rn(kh, __ffma2_rn(make_float2(-1.0f, -1.0f), dm1, dp1));
+    const float2 uxx1 = __fmul2_rn(kh, __fadd2_rn(dm1, dp1));
+    const float2 ux2 = __ffma2_rn(k2, dp1, __fmul2_rn(kmh, dp2));
+    const float2 uxx2 = __fmul2_rn(kh, __ffma2_rn(km2, dp1, dp2));
+    const float2 a0 = __ffma2_rn(ux0, ux0, __ffma2_rn(__fmul2_rn(k13, uxx0), uxx0, keps));
+    const float2 a1 = __ffma2_rn(ux1, ux1, __ffma2_rn(__fmul2_rn(k13, uxx1), uxx1, keps));
+    const float2 a2 = __ffma2_rn(ux2, ux2, __ffma2_rn(__fmul2_rn(k13, uxx2), uxx2, keps));
+    const float2 mn = make_float2(fminf(a0.x, fminf(a1.x, a2.x)), fminf(a0.y, fminf(a1.y, a2.y)));
+    auto rcp2 = [](float2 v) { return make_float2(__fdividef(1.0f, v.x), __fdividef(1.0f, v.y)); };   // fast reciprocals
+    float2 q0 = __fmul2_rn(mn, rcp2(a0));
+    float2 q1 = __fmul2_rn(mn, rcp2(a1));
+    float2 q2 = __fmul2_rn(mn, rcp2(a2));
+    q0 = __fmul2_rn(q0, q0); q1 = __fmul2_rn(q1, q1); q2 = __fmul2_rn(q2, q2);
+    const float2 w0 = __fmul2_rn(q0, q0), w1 = __fmul2_rn(k100, __fmul2_rn(q1, q1)), w2 = __fmul2_rn(q2, q2);
+    const float2 sum = __fadd2_rn(__fadd2_rn(w0, w1), w2);
+    const float2 inv = rcp2(sum);
+    slope = __fmul2_rn(__ffma2_rn(w2, ux2, __ffma2_rn(w1, ux1, __fmul2_rn(w0, ux0))), inv);
+    curv = __fmul2_rn(__ffma2_rn(w2, uxx2, __ffma2_rn(w1, uxx1, __fmul2_rn(w0, uxx0))), inv);
 }
 
 // reconstruction.c:144-221 on deviations (u_0 = 0): coefficients k = 1..5
 __device__ __forceinline__ void weno3_f(const float *d, float *c)
 {
     // d: xm2 xm1 xp1 xp2 ym2 ym1 yp1 yp2 pp pm mp mm
-    weno3_1d_f(d[0], d[1], d[2], d[3], c[0], c[2]);
-    weno3_1d_f(d[4], d[5], d[6], d[7], c[1], c[3]);
+    float2 sl, cu;
+    weno3_xy_f2(make_float2(d[0], d[4]), make_float2(d[1], d[5]), make_float2(d[2], d[6]), make_float2(d[3], d[7]), sl, cu);
+    c[0] = sl.x; c[1] = sl.y; c[2] = cu.x; c[3] = cu.y;
     const float c1 = c[0], c2 = c[1], c3 = c[2], c4 = c[3];
     const float x0 = d[8] - c1 - c2 - c3 - c4;
     const float x1 = -d[9] + c1 - c2 + c3 + c4;
