@@ -357,7 +357,6 @@ __device__ __forceinline__ void mixed_tile(const MixedParams &p, const MixedMaps
                 }
                 float cf[5];
                 weno3_f(d, cf);
-#pragma unroll
                 cf_store(c, m, cf);
             }
         }
