@@ -153,25 +153,31 @@ template <> struct System<SYS_KAPILA> {
     static constexpr int NV = 6;
     static constexpr int RX0 = 2, RX1 = -1, RY0 = 3, RY1 = -1;   // rhs_function_prim.c:124-125, 253-254
     static constexpr int RXV = 3, RYV = 2;                         // tangential, VISCOUS only: :126-127, :255-256
-    // kapila_5eqn.c:14-35
-    __device__ __forceinline__ static void cons2prim(const Eos &e, const double *Q, double *V)
+    // kapila_5eqn.c:14-35; dv(a, b) = a / b (cons2prim_dv: the bit-exact tile's row staging
+    // passes the branch-free correctly rounded division, so the independent divisions overlap)
+    template <class Dv>
+    __device__ __forceinline__ static void cons2prim_dv(const Eos &e, const double *Q, double *V, Dv dv)
     {
         double alpha_1 = Q[5];
         double alpha_2 = 1.0 - alpha_1;
         double rho = Q[0] + Q[1];
-        double u = Q[2] / rho;
-        double v = Q[3] / rho;
+        double u = dv(Q[2], rho);
+        double v = dv(Q[3], rho);
         double E = Q[4];
         double ei = E - 0.5 * rho * (u * u + v * v);
         double G1m1 = e.g1 - 1.0;
         double G2m1 = e.g2 - 1.0;
-        double p = (ei * G1m1 * G2m1 - alpha_1 * e.g1 * e.pi1 * G2m1 - alpha_2 * e.g2 * e.pi2 * G1m1) / (alpha_1 * G2m1 + alpha_2 * G1m1);
-        V[0] = Q[0] / alpha_1;
-        V[1] = Q[1] / alpha_2;
+        double p = dv(ei * G1m1 * G2m1 - alpha_1 * e.g1 * e.pi1 * G2m1 - alpha_2 * e.g2 * e.pi2 * G1m1, alpha_1 * G2m1 + alpha_2 * G1m1);
+        V[0] = dv(Q[0], alpha_1);
+        V[1] = dv(Q[1], alpha_2);
         V[2] = u;
         V[3] = v;
         V[4] = p;
         V[5] = alpha_1;
+    }
+    __device__ __forceinline__ static void cons2prim(const Eos &e, const double *Q, double *V)
+    {
+        cons2prim_dv(e, Q, V, [](double a, double b) { return a / b; });
     }
     // kapila_5eqn.c:41-61
     __device__ __forceinline__ static void prim2cons(const Eos &e, const double *V, double *Q)
@@ -392,17 +398,22 @@ template <> struct System<SYS_KAPILA> {
 template <> struct System<SYS_BN> {
     static constexpr int NV = 9;
     static constexpr int RX0 = 1, RX1 = 5, RY0 = 2, RY1 = 6;   // rhs_function_prim.c:115-117, 244-246
-    // baer_nunziato.c:14-41
+    // baer_nunziato.c:14-41; dv(a, b) = a / b (cons2prim_dv as for the Kapila system)
     __device__ __forceinline__ static void cons2prim(const Eos &e, const double *Q, double *V)
+    {
+        cons2prim_dv(e, Q, V, [](double a, double b) { return a / b; });
+    }
+    template <class Dv>
+    __device__ __forceinline__ static void cons2prim_dv(const Eos &e, const double *Q, double *V, Dv dv)
     {
         double phi_1 = Q[8];
         double phi_2 = 1.0 - Q[8];
-        double rho_1 = Q[0] / phi_1;
-        double rho_2 = Q[4] / phi_2;
-        double u_1 = Q[1] / Q[0], v_1 = Q[2] / Q[0];
-        double u_2 = Q[5] / Q[4], v_2 = Q[6] / Q[4];
-        double E_1 = Q[3] / phi_1;
-        double E_2 = Q[7] / phi_2;
+        double rho_1 = dv(Q[0], phi_1);
+        double rho_2 = dv(Q[4], phi_2);
+        double u_1 = dv(Q[1], Q[0]), v_1 = dv(Q[2], Q[0]);
+        double u_2 = dv(Q[5], Q[4]), v_2 = dv(Q[6], Q[4]);
+        double E_1 = dv(Q[3], phi_1);
+        double E_2 = dv(Q[7], phi_2);
         double p_1 = (e.g1 - 1.0) * (E_1 - 0.5 * rho_1 * (u_1 * u_1 + v_1 * v_1)) - e.g1 * e.pi1;
         double p_2 = (e.g2 - 1.0) * (E_2 - 0.5 * rho_2 * (u_2 * u_2 + v_2 * v_2)) - e.g2 * e.pi2;
         V[0] = rho_1; V[1] = u_1; V[2] = v_1; V[3] = p_1;

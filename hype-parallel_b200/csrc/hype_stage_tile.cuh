@@ -320,6 +320,15 @@ __device__ __forceinline__ void stage_tile(const StageParams &p, const CUtensorM
                 if constexpr (CONS) {
 #pragma unroll
                     for (int c = 0; c < NV; ++c) V[c] = Q[c];
+                } else if constexpr (!FAST && ((SYS == SYS_BN && (N == 1 || N == 2)) || (SYS == SYS_KAPILA && N <= 1))) {
+                    // branch-free correctly rounded divisions (hype_div.cuh): the cell's
+                    // independent divisions overlap instead of each waiting on the last
+                    // one's slow-path branch; the compiler's division where an operand is
+                    // outside their range.  Only in the tiles where it measured faster
+                    // (Kapila N = 2, 3 lose to the extra registers)
+                    bool special = false;
+                    S::cons2prim_dv(eos, Q, V, [&special](double a, double b) { return cr_div(a, b, special); });
+                    if (special) S::cons2prim(eos, Q, V);
                 } else {
                     S::cons2prim(eos, Q, V);
                 }
