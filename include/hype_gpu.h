@@ -133,8 +133,11 @@ HYPE_API const char *hype_last_error(const hype_solver *s);
  * launch, band of rows by band of rows.  Pinned (page-locked) U and RHS go to the
  * copy engines directly; pageable ones (PETSc's Vec arrays) are staged through
  * two pinned buffers of the state's size that the solver allocates on first use
- * (direct copies if that allocation fails).  The same holds for
- * hype_rhs_prim_slab and hype_advance_host.
+ * (direct copies if that allocation fails), copied by the calling thread and a
+ * pool of three host threads that the library starts on the first such copy (one
+ * pool per process; the threads idle between copies and end with the process).
+ * The same holds for hype_rhs_prim_slab, hype_advance_host, hype_set_state and
+ * hype_get_state.
  */
 HYPE_API int hype_rhs_prim(hype_solver *s, double t, const double *U, double *RHS, double *dt);
 
